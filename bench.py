@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Headline benchmark: clover solves/s to a 1e-10 FP64 true residual.
+
+Workload (one step = one batched solve): even-odd preconditioned Wilson-clover
+operator on a 16^3x32 lattice, kappa = 0.1360 (bare mass 1/(2 kappa) - 4),
+c_sw = 1.0, links exp(i 0.3 H) with H drawn from the Gaussian unitary
+ensemble (stored 12-real), antiperiodic in t.  The solver is QPhiX's
+InvRichardsonMultiPrec: FP64 outer defect correction to a 1e-10 relative
+true residual, inner BiCGStab on FP16-storage (per-site norm) / FP32-compute
+fields, `--batch` right-hand sides solved together.  The plain FP64 BiCGStab
+solve of the same system is timed beside it.
+
+value  = solves/s with the right-hand sides resident in HBM
+e2e    = solves/s through the C ABI with host buffers: pinned host -> device
+         upload of the sources, solve, device -> host download of x per step
+roofline: the dominant kernel (the FP16 clover Dslash of the inner solve),
+         timed alone on the same lattice with L2 flushed before every launch.
+cpu_baseline: the CPU oracle (FP64 clover BiCGStab iterations) on the host
+         cores, scaled to a full solve by the FP64 iteration count.
+
+N > 1 GPUs: independent replicas (the path does not shard across GPUs here);
+value = all ranks' solves / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+KAPPA = 0.1360
+CSW = 1.0
+EPS = 0.3
+DIMS = (16, 16, 16, 32)
+RSD = 1e-10
+DELTA = 0.1
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--inner", default="f16", choices=["f16", "bf16", "f32"])
+    ap.add_argument("--no-fp64", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def make_inputs(dims, batch, seed=2024):
+    from qphix_b200 import fields as F
+    g = F.make_gauge(dims, seed, "exp", eps=EPS)
+    mass = F.kappa_to_mass(KAPPA)
+    cl = F.make_clover(dims, g, mass, CSW)
+    inv_even = F.invert_clover(cl[0])
+    rhs = np.stack([F.gaussian_spinor(dims, seed + 100 + i) for i in range(batch)])
+    return dict(gauge=g, clov_odd=cl[1], invclov_even=inv_even, rhs=rhs, mass=mass)
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        out, _ = self.p.communicate(timeout=10)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-site DRAM traffic of the profiled kernels (profiles/traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ---------------------------------------------------------------------------
+def cpu_oracle_sample(inputs, dims, n_iter_fp64, max_sample_iters=3):
+    """FP64 clover BiCGStab on the host cores (the CPU oracle), a bounded
+    number of iterations, scaled to a full solve by the FP64 iteration count."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    L = O.make_lattice(dims, -1.0)
+    op = O.OracleOp("clover", L, inputs["gauge"], clov=inputs["clov_odd"],
+                    invclov=inputs["invclov_even"])
+    b = inputs["rhs"][0]
+    t0 = time.perf_counter()
+    _, info = O.bicgstab(op, b, 1e-30, max_sample_iters)
+    dt = time.perf_counter() - t0
+    per_iter = dt / max(1, max_sample_iters)
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    solve_s = per_iter * max(1, n_iter_fp64)
+    return {"value": 1.0 / solve_s, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"{max_sample_iters} FP64 clover BiCGStab iterations on {'x'.join(map(str, dims))} "
+                      f"({dt:.1f} s), scaled to a {n_iter_fp64}-iteration solve"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU implementation of the path on the host cores."""
+    if rank != 0:
+        return
+    inputs = make_inputs(DIMS, 1)
+    n_fp64 = int(os.environ.get("QPHIX_BENCH_FP64_ITERS", "110"))
+    vals = []
+    for _ in range(args.warmup):
+        cpu_oracle_sample(inputs, DIMS, n_fp64, 1)
+    for _ in range(args.steps):
+        vals.append(cpu_oracle_sample(inputs, DIMS, n_fp64, 2))
+    v = statistics.median([x["value"] for x in vals])
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "data": "synthetic", "config": config_dict(1, "f64"),
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": vals[-1]["cores"], "kind": "port",
+                             "sample": vals[-1]["sample"]},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "Clover solves/s @1e-10 mixed vs FP64 plain, 1 B200; Dslash HBM GB/s; p99 ms"
+
+
+def config_dict(batch, inner):
+    return {"workload": ("clover even-odd 16^3x32, kappa=0.1360, csw=1.0, links exp(i 0.3 H) "
+                         "(H GUE) 12-real, antiperiodic t; InvRichardsonMultiPrec FP64 outer to 1e-10 "
+                         f"true residual, inner BiCGStab {inner}-storage/FP32-compute"),
+            "rhs_per_step": batch, "lattice": list(DIMS), "kappa": KAPPA, "csw": CSW,
+            "l2": "flushed (256 MiB write) before every step"}
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    from qphix_b200 import _lib
+    from qphix_b200 import api
+
+    B = args.batch
+    inputs = make_inputs(DIMS, B, seed=2024 + 17 * rank)
+    lat = api.Lattice(DIMS, device=local)
+    stream = torch.cuda.Stream()
+    lat.set_stream(stream.cuda_stream)
+    # FP64 outer operator, inner operator on 16-bit storage
+    u64 = lat.gauge("f64", 12).upload(inputs["gauge"])
+    A64 = lat.clover("f64").upload(inputs["clov_odd"])
+    Ai64 = lat.clover("f64").upload(inputs["invclov_even"])
+    M64 = api.EvenOddCloverOperator(u64, A64, Ai64)
+    ui = lat.gauge(args.inner, 12).upload(inputs["gauge"])
+    Ai = lat.clover(args.inner).upload(inputs["clov_odd"])
+    Aii = lat.clover(args.inner).upload(inputs["invclov_even"])
+    Mi = api.EvenOddCloverOperator(ui, Ai, Aii)
+    solver = api.InvRichardsonMultiPrec(M64, Mi, "bicgstab", delta=DELTA, max_iters=100,
+                                        inner_max_iters=5000)
+    b_res = lat.spinor("f64", B).upload(inputs["rhs"])    # resident sources
+    b = lat.spinor("f64", B)
+    x = lat.spinor("f64", B)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step_resident():
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        api.copy(b, b_res)
+        api.zero(x)
+        return solver(x, b, RSD)
+
+    # host buffers for the end-to-end path (pinned)
+    h_rhs = torch.from_numpy(np.ascontiguousarray(
+        np.stack([inputs["rhs"].real, inputs["rhs"].imag], axis=-1))).pin_memory()
+    h_x = torch.empty_like(h_rhs).pin_memory()
+    layout = api._canon_layout()
+    import ctypes as C
+
+    def step_e2e():
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        _lib.check(_lib._lib.qphix_gpu_field_upload(b.h, C.c_void_p(h_rhs.data_ptr()), C.byref(layout), -1, -1))
+        api.zero(x)
+        inf = solver(x, b, RSD)
+        _lib.check(_lib._lib.qphix_gpu_field_download(x.h, C.c_void_p(h_x.data_ptr()), C.byref(layout), -1))
+        return inf
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def launches():
+        n = C.c_ulonglong(0)
+        _lib._lib.qphix_gpu_launch_count(C.byref(n))
+        return n.value
+
+    for _ in range(args.warmup):
+        infos = step_resident()
+    # ---- timed: resident inputs ------------------------------------------------
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    l0 = launches()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    all_infos = []
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        all_infos.append(step_resident())
+        ev[i][1].record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    n_launch = launches() - l0
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(bb) for a, bb in ev]
+    total_s = sum(step_ms) / 1e3
+    if dist is not None:
+        t = torch.tensor([total_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_s = float(t.item())
+    value = world * B * args.steps / total_s
+    worst_resid = max(i["true_rel_resid"] for inf in all_infos for i in inf)
+    converged = all(i["status"] == 0 for inf in all_infos for i in inf)
+    outer_iters = all_infos[-1][0]["n_iters"]
+    mv_apps = all_infos[-1][0]["mv_apps"]
+
+    # ---- e2e through the C ABI with host buffers -------------------------------
+    step_e2e()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_ms = []
+    for _ in range(args.steps):
+        t1 = time.perf_counter()
+        step_e2e()
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t1) * 1e3)
+    e2e_total = sum(e2e_ms) / 1e3
+    if dist is not None:
+        t = torch.tensor([e2e_total], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * B * args.steps / e2e_total
+    bytes_io = int(h_rhs.numel() * 8)
+
+    # ---- plain FP64 BiCGStab beside it ------------------------------------------
+    fp64 = None
+    if not args.no_fp64:
+        b1 = lat.spinor("f64", 1).upload(inputs["rhs"][0])
+        x1 = lat.spinor("f64", 1)
+        bic = api.InvBiCGStab(M64, 5000)
+        api.zero(x1)
+        inf = bic(x1, b1, RSD)[0]
+        ts = []
+        for _ in range(max(2, min(args.steps, 5))):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            api.zero(x1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            inf = bic(x1, b1, RSD)[0]
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        fp64 = {"solves_per_s": 1e3 / statistics.median(ts), "ms_per_solve": statistics.median(ts),
+                "iters": inf["n_iters"], "true_rel_resid": inf["true_rel_resid"],
+                "status": inf["status"]}
+
+    # ---- roofline: the FP16 clover Dslash kernel (inner solve), L2 flushed ------
+    def dslash_roofline(dims, prec, n=20):
+        from qphix_b200 import fields as F
+        lat2 = lat if dims == DIMS else api.Lattice(dims, device=local)
+        if dims != DIMS:
+            lat2.set_stream(stream.cuda_stream)
+        # a larger lattice for the roofline: the C2 links tiled (link values do not change timing)
+        g = inputs["gauge"] if dims == DIMS else np.tile(inputs["gauge"], (1, 1, F.vh(dims) // F.vh(DIMS), 1, 1))
+        u = lat2.gauge(prec, 12).upload(g)
+        cl = lat2.clover(prec).upload(inputs["invclov_even"] if dims == DIMS else
+                                      np.tile(inputs["invclov_even"][:1], (F.vh(dims), 1, 1)))
+        psi = lat2.spinor(prec).upload(F.gaussian_spinor(dims, 3))
+        out = lat2.spinor(prec)
+        D = api.ClovDslash(lat2, -1.0, 1.0, 1.0)
+        D.dslash(out, psi, u, cl, 1, 0)
+        durs = []
+        for _ in range(n):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            D.dslash(out, psi, u, cl, 1, 0)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            durs.append(e0.elapsed_time(e1) / 1e3)
+        vh = F.vh(dims)
+        esize = {"f16": 2, "bf16": 2, "f32": 4, "f64": 8}[prec]
+        norm = 4 if prec in ("f16", "bf16") else 0
+        per_site = 2 * (24 * esize + norm) + 8 * 12 * esize + 72 * esize
+        t = statistics.mean(durs)
+        return per_site, vh, t
+
+    peak, peak_kind = peaks()
+    per_site, vh, t = dslash_roofline(DIMS, args.inner)
+    achieved = per_site * vh / t / 1e9
+    traffic = profile_traffic().get(f"clover_dslash_{args.inner}_12")
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+            "traffic": (round(traffic * vh) if traffic else None),
+            "kernel": f"clover Dslash A^-1 D psi, {args.inner} storage, 12-real links",
+            "bytes_per_site": per_site, "sites": vh, "launch_us": round(t * 1e6, 2)}
+    big = (32, 32, 32, 64)
+    ps2, vh2, t2 = dslash_roofline(big, args.inner, n=10)
+    roof_big = {"lattice": list(big), "achieved": round(ps2 * vh2 / t2 / 1e9, 1),
+                "frac": round(ps2 * vh2 / t2 / 1e9 / peak, 4), "launch_us": round(t2 * 1e6, 1)}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        n_fp64 = fp64["iters"] if fp64 else 110
+        try:
+            cpu = cpu_oracle_sample(inputs, DIMS, n_fp64)
+        except Exception as e:  # pragma: no cover
+            cpu = {"value": None, "error": str(e)}
+
+    if rank == 0:
+        p = sorted(step_ms)
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(total_s * 1e3 / args.steps, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": f"mixed: f64 outer, f32 arithmetic on {args.inner} storage inner",
+            "data": "synthetic (seeded)", "config": config_dict(B, args.inner),
+            "e2e": {"value": round(e2e_value, 3), "unit": "solves/s", "h2d_bytes_per_step": bytes_io,
+                    "d2h_bytes_per_step": bytes_io},
+            "roofline": roof, "roofline_large_lattice": roof_big,
+            "cpu_baseline": cpu, "gpu_launches": int(n_launch),
+            "clocks": clk,
+            "p50_ms_per_step": round(p[len(p) // 2], 3), "p99_ms_per_step": round(p[min(len(p) - 1, int(0.99 * len(p)))], 3),
+            "fp64_plain": fp64,
+            "mixed_vs_fp64_solves_ratio": (round(value / world / fp64["solves_per_s"], 3) if fp64 else None),
+            "solver": {"outer_iters": outer_iters, "mv_apps": mv_apps, "worst_true_rel_resid": worst_resid,
+                       "all_converged": converged},
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

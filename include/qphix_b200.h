@@ -1,0 +1,208 @@
+/*
+ * qphix_b200 -- C ABI of the B200 (sm_100a) implementation of QPhiX's hot
+ * path: the Wilson / clover / twisted-mass (clover) Dslash, the even-odd
+ * preconditioned operators and the CG / BiCGStab / MR / multishift-CG /
+ * Richardson solvers.
+ *
+ * Plain C types only (opaque handles, pointers, sizes).  Every function
+ * returns 0 on success or a negative QPHIX_GPU_E* code; the message of the
+ * last failure on the calling thread is qphix_gpu_last_error().  Nothing in
+ * the library calls abort() or exit().  QPhiX's own interfaces abort on
+ * misuse (include/qphix/geometry.h:274-277, dslash_body.h:64-95,
+ * minvcg.h:92-96); here the same conditions come back as error codes and the
+ * C++ drop-in headers (include/qphix/) turn them into exceptions.
+ *
+ * Fields live in device memory in the library's own chunked layout; they are
+ * filled from and read back into host arrays in either the canonical
+ * site-major FP64 layout or QPhiX's blocked host layout (any veclen / soalen
+ * / padding / compress12 / FT the reference supports).
+ *
+ * Each lattice carries one CUDA stream (its own non-blocking stream unless
+ * the caller installs another); every call on objects of that lattice is
+ * ordered on it.  A lattice stays alive until it and all of its fields have
+ * been destroyed, in any order.  Objects are not
+ * thread-safe: one host thread per lattice (QPhiX objects are likewise not
+ * re-entrant, dslash_body.h:85-95).
+ */
+#ifndef QPHIX_B200_H
+#define QPHIX_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define QPHIX_GPU_OK 0
+#define QPHIX_GPU_EINVAL (-1)      /* bad argument / shape / combination     */
+#define QPHIX_GPU_ENOMEM (-2)      /* device or pinned allocation failed     */
+#define QPHIX_GPU_ECUDA (-3)       /* a CUDA runtime call failed             */
+#define QPHIX_GPU_ENOTCONV (-4)    /* solver hit its iteration limit         */
+#define QPHIX_GPU_EBREAKDOWN (-5)  /* solver breakdown (BiCGStab rho == 0 ...) */
+#define QPHIX_GPU_EUNSUPPORTED (-6)
+
+/* ---- enums ------------------------------------------------------------- */
+enum { QPHIX_GPU_F64 = 0, QPHIX_GPU_F32 = 1, QPHIX_GPU_F16 = 2, QPHIX_GPU_BF16 = 3 };
+enum { QPHIX_GPU_SPINOR = 0, QPHIX_GPU_GAUGE = 1, QPHIX_GPU_CLOVER = 2, QPHIX_GPU_FULLCLOVER = 3 };
+enum { QPHIX_GPU_WILSON = 0, QPHIX_GPU_CLOVER_OP = 1, QPHIX_GPU_TM = 2, QPHIX_GPU_TMCLOVER = 3 };
+enum { QPHIX_GPU_HOST_CANONICAL = 0, QPHIX_GPU_HOST_QPHIX = 1 };
+enum { QPHIX_GPU_HOST_F64 = 0, QPHIX_GPU_HOST_F32 = 1, QPHIX_GPU_HOST_F16 = 2 };
+enum { QPHIX_GPU_SOLVER_CG = 0, QPHIX_GPU_SOLVER_BICGSTAB = 1, QPHIX_GPU_SOLVER_MR = 2 };
+
+typedef struct qphix_gpu_lattice_s *qphix_gpu_lattice;
+typedef struct qphix_gpu_field_s *qphix_gpu_field;
+typedef struct qphix_gpu_eo_op_s *qphix_gpu_eo_op;
+
+/* Host array layout for upload / download.
+ * canonical: FP64 site-major (ft must be QPHIX_GPU_HOST_F64):
+ *   spinor [nrhs][Vh][4 spin][3 col][2], gauge [2 cb][4 mu][Vh][3][3][2]
+ *   (U_mu(x), x in cb), clover [Vh][2][36] (diag[6], offd[15] re/im),
+ *   full clover [Vh][2][6][6][2].
+ * qphix: the reference's Geometry<FT,V,S,compress12> arrays with padding
+ *   pad_xy / pad_xyz (include/qphix/geometry.h:130-175); spinor pointers are
+ *   the ones allocCBFourSpinor returns (block 0 = first site), gauge arrays
+ *   are one checkerboard each (8 links per site, stored transposed). */
+typedef struct {
+  int kind;        /* QPHIX_GPU_HOST_CANONICAL / _QPHIX                 */
+  int ft;          /* QPHIX_GPU_HOST_F64 / _F32 / _F16                  */
+  int veclen;      /* qphix only                                         */
+  int soalen;
+  int compress12;
+  int pad_xy;
+  int pad_xyz;
+} qphix_gpu_host_layout;
+
+/* Operator parameters: the constructor arguments of Dslash / ClovDslash /
+ * TMDslash / TMClovDslash and the EvenOdd*Operator classes. */
+typedef struct {
+  int kind;                 /* QPHIX_GPU_WILSON ... _TMCLOVER                 */
+  double t_boundary;        /* +1 / -1                                       */
+  double aniso_s, aniso_t;  /* hop coefficients                              */
+  int use_tbc[4];           /* twisted boundary phase per dimension          */
+  double tbc_phases[4][2];
+  double mass;              /* Wilson / TM bare mass (alpha = 4 + mass)      */
+  double twisted_mass;      /* TM mu                                         */
+  double prec_mass_rho;     /* clover / TM clover i rho gamma_5 term         */
+} qphix_gpu_op_params;
+
+typedef struct {
+  int n_iters;              /* as the reference solver reports it            */
+  double rsd_sq_final;      /* as the reference solver reports it            */
+  unsigned long site_flops; /* reference flop accounting                     */
+  unsigned long mv_apps;    /* operator applications                         */
+  int status;               /* 0 converged, 1 iteration limit, 2 breakdown   */
+  double true_rel_resid;    /* ||b - M x|| / ||b|| recomputed in FP64        */
+  double seconds;           /* device time of the solve                      */
+} qphix_gpu_solve_info;
+
+/* ---- library ------------------------------------------------------------ */
+int qphix_gpu_version(void);
+const char *qphix_gpu_last_error(void);
+/* Select the CUDA device for the calling thread. */
+int qphix_gpu_init(int device);
+/* Number of kernels this library has launched in this process; a CUDA-graph
+ * replay counts every kernel node it runs. */
+int qphix_gpu_launch_count(unsigned long long *out);
+
+/* ---- lattice (replaces Geometry<FT,V,S,c12>, include/qphix/geometry.h:130) */
+int qphix_gpu_lattice_create(const int latt_size[4], qphix_gpu_lattice *out);
+int qphix_gpu_lattice_destroy(qphix_gpu_lattice lat);
+int qphix_gpu_lattice_set_stream(qphix_gpu_lattice lat, void *cuda_stream);
+int qphix_gpu_lattice_sync(qphix_gpu_lattice lat);
+long qphix_gpu_lattice_volcb(qphix_gpu_lattice lat);
+
+/* ---- fields (replace Geometry::allocCB* / free, geometry.h:270-396) ---- */
+/* recon: 12 or 18 for gauge fields, ignored otherwise.  nrhs >= 1 for
+ * spinors (a block of right-hand sides), 1 otherwise.  Zero-filled. */
+int qphix_gpu_field_create(qphix_gpu_lattice lat, int kind, int prec, int recon, int nrhs,
+                           qphix_gpu_field *out);
+int qphix_gpu_field_destroy(qphix_gpu_field f);
+int qphix_gpu_field_bytes(qphix_gpu_field f, size_t *bytes);
+/* cb: gauge fields with a qphix layout carry one checkerboard per host array
+ * (pass 0 or 1); canonical gauge arrays carry both (pass -1).
+ * rhs: index of one right-hand side to transfer, or -1 for all. */
+int qphix_gpu_field_upload(qphix_gpu_field f, const void *host, const qphix_gpu_host_layout *layout,
+                           int cb, int rhs);
+int qphix_gpu_field_download(qphix_gpu_field f, void *host, const qphix_gpu_host_layout *layout, int rhs);
+/* Device-to-device copy with precision conversion: dst = scale * src. */
+int qphix_gpu_field_convert(qphix_gpu_field dst, qphix_gpu_field src, double scale);
+
+/* ---- Dslash family --------------------------------------------------------
+ * qphix_gpu_dslash replaces Dslash::dslash (include/qphix/dslash_def.h:35),
+ *   ClovDslash::dslash (clover_dslash_def.h:34, aux = A^-1),
+ *   TMDslash::dslash (tm_dslash_def.h:33) and TMClovDslash::dslash
+ *   (tm_clov_dslash_def.h:44, aux = invclov[0], aux2 = invclov[1]).
+ * qphix_gpu_dslash_achimbdpsi replaces the dslashAChiMinusBDPsi members
+ *   (dslash_def.h:42, clover_dslash_def.h:41, tm_dslash_def.h:39,
+ *   tm_clov_dslash_def.h:57; aux = the clover term A for clover kinds).
+ *   For Wilson res = alpha chi - beta D psi; clover kinds
+ *   res = A chi + i rho isign g5 chi - beta D psi (alpha ignored);
+ *   TM res = alpha (1 + i isign musign mu/(4+m) g5) chi - beta D psi.
+ * qphix_gpu_dslash_dir replaces Dslash::dslashDir (dslash_def.h:51).
+ * qphix_gpu_clover_apply replaces ClovDslash::clovMult (clover_dslash_def.h:50). */
+int qphix_gpu_dslash(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                     qphix_gpu_field gauge, qphix_gpu_field aux, qphix_gpu_field aux2, int isign, int cb);
+int qphix_gpu_dslash_achimbdpsi(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                                qphix_gpu_field chi, qphix_gpu_field gauge, qphix_gpu_field aux, double alpha,
+                                double beta, int isign, int cb, double musign);
+int qphix_gpu_dslash_dir(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                         qphix_gpu_field gauge, int cb, int dir);
+int qphix_gpu_clover_apply(qphix_gpu_field res, qphix_gpu_field chi, qphix_gpu_field clov);
+
+/* ---- even-odd operators ----------------------------------------------------
+ * Replace EvenOddWilsonOperator (include/qphix/wilson.h:20), EvenOddClover-
+ * Operator (clover.h:31), EvenOddTMWilsonOperator (twisted_mass.h:22) and
+ * EvenOddTMCloverOperator (twisted_mass_clover.h:29).  clov = A on the
+ * target (odd) checkerboard, invclov = A^-1 on the other (even) one;
+ * finv0/finv1 = (A_ee + i mu g5)^-1 / (A_ee - i mu g5)^-1 for TM clover.
+ * The operator holds non-owning references to the fields and owns one
+ * temporary spinor per right-hand side count it has been applied to. */
+int qphix_gpu_eo_op_create(const qphix_gpu_op_params *p, qphix_gpu_field gauge, qphix_gpu_field clov,
+                           qphix_gpu_field invclov, qphix_gpu_field finv0, qphix_gpu_field finv1,
+                           qphix_gpu_eo_op *out);
+int qphix_gpu_eo_op_destroy(qphix_gpu_eo_op op);
+/* operator()(res, in, isign, target_cb) (linearOp.h:21) */
+int qphix_gpu_eo_op_apply(qphix_gpu_eo_op op, qphix_gpu_field res, qphix_gpu_field in, int isign,
+                          int target_cb);
+
+/* ---- solvers ----------------------------------------------------------------
+ * x holds the initial guess and receives the solution; all right-hand sides
+ * of the block are solved together (info[nrhs]).  rsd_target is relative
+ * (ResiduumType RELATIVE, abs_solver.h:13).
+ *   cg       InvCG::operator() on M^dag M (invcg.h:88)
+ *   bicgstab InvBiCGStab::operator() (invbicgstab.h:80)
+ *   mr       InvMR::operator() with over-relaxation omega (invmr.h:62)
+ *   mshift   MInvCG::operator() (minvcg.h:77): x[n_shift] solve
+ *            (M^dag M + shifts[i]) x_i = rhs
+ *   richardson InvRichardsonMultiPrec::operator()
+ *            (inv_richardson_multiprec.h:42): outer operator / fields in
+ *            their precision, inner solver (CG / BiCGStab / MR) on
+ *            op_inner, whose fields carry the inner precision. */
+int qphix_gpu_solve_cg(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target,
+                       int max_iters, int isign, int cb, qphix_gpu_solve_info *info);
+int qphix_gpu_solve_bicgstab(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target,
+                             int max_iters, int isign, int cb, qphix_gpu_solve_info *info);
+int qphix_gpu_solve_mr(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target,
+                       int max_iters, double omega, int isign, int cb, qphix_gpu_solve_info *info);
+int qphix_gpu_solve_mshift_cg(qphix_gpu_eo_op op, qphix_gpu_field *x, qphix_gpu_field rhs, int n_shift,
+                              const double *shifts, const double *rsd_target, int max_iters, int isign,
+                              int cb, int *n_iters, double *rsd_sq_final, unsigned long *mv_apps);
+int qphix_gpu_solve_richardson(qphix_gpu_eo_op op_outer, qphix_gpu_eo_op op_inner, int inner_solver,
+                               qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target, double delta,
+                               int max_iters, int inner_max_iters, int isign, int cb,
+                               qphix_gpu_solve_info *info);
+
+/* ---- BLAS (include/qphix/blas_new_c.h) --------------------------------------
+ * Per right-hand side results are written to out[nrhs] (complex: out[2*nrhs]). */
+int qphix_gpu_blas_norm2(qphix_gpu_field x, double *out);                        /* :278 */
+int qphix_gpu_blas_inner_product(qphix_gpu_field x, qphix_gpu_field y, double *out); /* :520 */
+int qphix_gpu_blas_caxpby(const double a[2], qphix_gpu_field x, const double b[2], qphix_gpu_field y);
+                                                      /* y = a x + b y: axpy :214, axpby :247, aypx :139, caxpy :696 */
+int qphix_gpu_blas_copy(qphix_gpu_field dst, qphix_gpu_field src);               /* :18  */
+int qphix_gpu_blas_zero(qphix_gpu_field x);                                      /* :49  */
+
+#ifdef __cplusplus
+}
+#endif
+#endif

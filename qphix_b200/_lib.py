@@ -1,0 +1,114 @@
+"""ctypes declarations of the C ABI in include/qphix_b200.h.
+
+Loading fails loudly: there is no CPU fallback anywhere in the package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqphix_b200.so")
+
+OK, EINVAL, ENOMEM, ECUDA, ENOTCONV, EBREAKDOWN, EUNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
+F64, F32, F16, BF16 = 0, 1, 2, 3
+SPINOR, GAUGE, CLOVER, FULLCLOVER = 0, 1, 2, 3
+WILSON, CLOVER_OP, TM, TMCLOVER = 0, 1, 2, 3
+HOST_CANONICAL, HOST_QPHIX = 0, 1
+HOST_F64, HOST_F32, HOST_F16 = 0, 1, 2
+SOLVER_CG, SOLVER_BICGSTAB, SOLVER_MR = 0, 1, 2
+
+
+class HostLayout(C.Structure):
+    _fields_ = [("kind", C.c_int), ("ft", C.c_int), ("veclen", C.c_int), ("soalen", C.c_int),
+                ("compress12", C.c_int), ("pad_xy", C.c_int), ("pad_xyz", C.c_int)]
+
+
+class OpParams(C.Structure):
+    _fields_ = [("kind", C.c_int), ("t_boundary", C.c_double), ("aniso_s", C.c_double),
+                ("aniso_t", C.c_double), ("use_tbc", C.c_int * 4),
+                ("tbc_phases", (C.c_double * 2) * 4), ("mass", C.c_double),
+                ("twisted_mass", C.c_double), ("prec_mass_rho", C.c_double)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("n_iters", C.c_int), ("rsd_sq_final", C.c_double), ("site_flops", C.c_ulong),
+                ("mv_apps", C.c_ulong), ("status", C.c_int), ("true_rel_resid", C.c_double),
+                ("seconds", C.c_double)]
+
+
+P = C.c_void_p
+I_ = C.c_int
+D = C.c_double
+PP = C.POINTER(C.c_void_p)
+
+_SIGS = {
+    "qphix_gpu_version": ([], I_),
+    "qphix_gpu_last_error": ([], C.c_char_p),
+    "qphix_gpu_init": ([I_], I_),
+    "qphix_gpu_launch_count": ([C.POINTER(C.c_ulonglong)], I_),
+    "qphix_gpu_lattice_create": ([C.POINTER(C.c_int), PP], I_),
+    "qphix_gpu_lattice_destroy": ([P], I_),
+    "qphix_gpu_lattice_set_stream": ([P, P], I_),
+    "qphix_gpu_lattice_sync": ([P], I_),
+    "qphix_gpu_lattice_volcb": ([P], C.c_long),
+    "qphix_gpu_field_create": ([P, I_, I_, I_, I_, PP], I_),
+    "qphix_gpu_field_destroy": ([P], I_),
+    "qphix_gpu_field_bytes": ([P, C.POINTER(C.c_size_t)], I_),
+    "qphix_gpu_field_upload": ([P, P, C.POINTER(HostLayout), I_, I_], I_),
+    "qphix_gpu_field_download": ([P, P, C.POINTER(HostLayout), I_], I_),
+    "qphix_gpu_field_convert": ([P, P, D], I_),
+    "qphix_gpu_dslash": ([C.POINTER(OpParams), P, P, P, P, P, I_, I_], I_),
+    "qphix_gpu_dslash_achimbdpsi": ([C.POINTER(OpParams), P, P, P, P, P, D, D, I_, I_, D], I_),
+    "qphix_gpu_dslash_dir": ([C.POINTER(OpParams), P, P, P, I_, I_], I_),
+    "qphix_gpu_clover_apply": ([P, P, P], I_),
+    "qphix_gpu_eo_op_create": ([C.POINTER(OpParams), P, P, P, P, P, PP], I_),
+    "qphix_gpu_eo_op_destroy": ([P], I_),
+    "qphix_gpu_eo_op_apply": ([P, P, P, I_, I_], I_),
+    "qphix_gpu_solve_cg": ([P, P, P, D, I_, I_, I_, C.POINTER(SolveInfo)], I_),
+    "qphix_gpu_solve_bicgstab": ([P, P, P, D, I_, I_, I_, C.POINTER(SolveInfo)], I_),
+    "qphix_gpu_solve_mr": ([P, P, P, D, I_, D, I_, I_, C.POINTER(SolveInfo)], I_),
+    "qphix_gpu_solve_mshift_cg": ([P, PP, P, I_, P, P, I_, I_, I_, C.POINTER(C.c_int), P,
+                                   C.POINTER(C.c_ulong)], I_),
+    "qphix_gpu_solve_richardson": ([P, P, I_, P, P, D, D, I_, I_, I_, I_, C.POINTER(SolveInfo)], I_),
+    "qphix_gpu_blas_norm2": ([P, P], I_),
+    "qphix_gpu_blas_inner_product": ([P, P, P], I_),
+    "qphix_gpu_blas_caxpby": ([P, P, P, P], I_),
+    "qphix_gpu_blas_copy": ([P, P], I_),
+    "qphix_gpu_blas_zero": ([P], I_),
+}
+
+EXPORTED = sorted(_SIGS)
+
+_lib = None
+
+
+class QPhiXGPUError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def load(path: str | None = None):
+    """Load (once) and return the C library; raises if it is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `python -m qphix_b200.build` "
+                          "(there is no CPU fallback)")
+    lib = C.CDLL(path)
+    for name, (argt, rest) in _SIGS.items():
+        f = getattr(lib, name)
+        f.argtypes = argt
+        f.restype = rest
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    if rc != OK:
+        msg = _lib.qphix_gpu_last_error().decode() if _lib else "library not loaded"
+        raise QPhiXGPUError(rc, msg)
+    return rc

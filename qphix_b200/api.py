@@ -1,0 +1,466 @@
+"""Python mirror of QPhiX's host interface over the C ABI.
+
+Class and method names follow the reference (include/qphix/*.h) so that code
+written against QPhiX reads the same:
+
+  Geometry           -> Lattice (+ field allocators)      geometry.h:115
+  Dslash             -> Dslash.dslash / dslashAChiMinusBDPsi / dslashDir
+  ClovDslash         -> ClovDslash (+ clovMult)          clover_dslash_def.h:14
+  TMDslash           -> TMDslash                          tm_dslash_def.h:11
+  TMClovDslash       -> TMClovDslash                      tm_clov_dslash_def.h:11
+  EvenOdd*Operator   -> EvenOddWilsonOperator, EvenOddCloverOperator,
+                        EvenOddTMWilsonOperator, EvenOddTMCloverOperator
+  InvCG / InvBiCGStab / InvMR / InvRichardsonMultiPrec / MInvCG
+
+Fields are device-resident handles; `upload` / `download` move canonical
+numpy arrays (see qphix_b200.fields) or QPhiX blocked host arrays.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check
+
+PREC = {"f64": L.F64, "f32": L.F32, "f16": L.F16, "bf16": L.BF16,
+        "double": L.F64, "float": L.F32, "half": L.F16}
+
+
+def lib():
+    return L.load()
+
+
+def _canon_layout():
+    h = L.HostLayout()
+    h.kind = L.HOST_CANONICAL
+    h.ft = L.HOST_F64
+    return h
+
+
+def qphix_layout(veclen, soalen, compress12, ft="f64", pad_xy=0, pad_xyz=0):
+    h = L.HostLayout()
+    h.kind = L.HOST_QPHIX
+    h.ft = {"f64": L.HOST_F64, "f32": L.HOST_F32, "f16": L.HOST_F16}[ft]
+    h.veclen, h.soalen, h.compress12 = veclen, soalen, int(bool(compress12))
+    h.pad_xy, h.pad_xyz = pad_xy, pad_xyz
+    return h
+
+
+class Lattice:
+    """One lattice (Geometry) with its own CUDA stream and reduction workspace."""
+
+    def __init__(self, dims, device=0):
+        lib()
+        check(L._lib.qphix_gpu_init(device))
+        self.dims = tuple(int(d) for d in dims)
+        arr = (C.c_int * 4)(*self.dims)
+        h = C.c_void_p()
+        check(L._lib.qphix_gpu_lattice_create(arr, C.byref(h)))
+        self.h = h
+        self.vh = int(L._lib.qphix_gpu_lattice_volcb(h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            L._lib.qphix_gpu_lattice_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        check(L._lib.qphix_gpu_lattice_sync(self.h))
+
+    def set_stream(self, stream_handle: int):
+        check(L._lib.qphix_gpu_lattice_set_stream(self.h, C.c_void_p(stream_handle)))
+
+    # allocators (Geometry::allocCB*)
+    def spinor(self, prec="f64", nrhs=1):
+        return Field(self, L.SPINOR, PREC[prec], 0, nrhs)
+
+    def gauge(self, prec="f64", recon=18):
+        return Field(self, L.GAUGE, PREC[prec], recon, 1)
+
+    def clover(self, prec="f64"):
+        return Field(self, L.CLOVER, PREC[prec], 0, 1)
+
+    def full_clover(self, prec="f64"):
+        return Field(self, L.FULLCLOVER, PREC[prec], 0, 1)
+
+
+class Field:
+    def __init__(self, lat: Lattice, kind, prec, recon, nrhs):
+        self.lat, self.kind, self.prec, self.recon, self.nrhs = lat, kind, prec, recon, nrhs
+        h = C.c_void_p()
+        check(L._lib.qphix_gpu_field_create(lat.h, kind, prec, recon, nrhs, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            L._lib.qphix_gpu_field_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def nbytes(self):
+        n = C.c_size_t()
+        check(L._lib.qphix_gpu_field_bytes(self.h, C.byref(n)))
+        return n.value
+
+    # ---- canonical numpy arrays -------------------------------------------------
+    def upload(self, arr, rhs=-1):
+        """Fill from a canonical array (complex spinor [(nrhs,) Vh, 4, 3];
+        complex gauge [2, 4, Vh, 3, 3]; packed clover float [Vh, 2, 36];
+        complex full clover [Vh, 2, 6, 6])."""
+        a = np.asarray(arr)
+        if np.iscomplexobj(a):
+            a = np.stack([a.real, a.imag], axis=-1)
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        cb = -1
+        check(L._lib.qphix_gpu_field_upload(self.h, a.ctypes.data_as(C.c_void_p),
+                                            C.byref(_canon_layout()), cb, rhs))
+        return self
+
+    def download(self, rhs=-1):
+        if self.kind == L.SPINOR:
+            n = self.nrhs if rhs < 0 else 1
+            out = np.empty((n, self.lat.vh, 4, 3, 2))
+            check(L._lib.qphix_gpu_field_download(self.h, out.ctypes.data_as(C.c_void_p),
+                                                  C.byref(_canon_layout()), rhs))
+            c = out[..., 0] + 1j * out[..., 1]
+            return c[0] if (rhs >= 0 or self.nrhs == 1) else c
+        nr = 72 if self.kind == L.CLOVER else 144
+        out = np.empty((self.lat.vh, nr))
+        check(L._lib.qphix_gpu_field_download(self.h, out.ctypes.data_as(C.c_void_p),
+                                              C.byref(_canon_layout()), -1))
+        return out
+
+    # ---- QPhiX blocked host arrays (drop-in path) ------------------------------
+    def upload_qphix(self, arr, layout, cb=-1, rhs=-1):
+        a = np.ascontiguousarray(arr)
+        check(L._lib.qphix_gpu_field_upload(self.h, a.ctypes.data_as(C.c_void_p), C.byref(layout),
+                                            cb, rhs))
+        return self
+
+    def download_qphix(self, out, layout, rhs=-1):
+        assert out.flags["C_CONTIGUOUS"]
+        check(L._lib.qphix_gpu_field_download(self.h, out.ctypes.data_as(C.c_void_p),
+                                              C.byref(layout), rhs))
+        return out
+
+    def convert_from(self, src, scale=1.0):
+        check(L._lib.qphix_gpu_field_convert(self.h, src.h, scale))
+        return self
+
+
+# ---------------------------------------------------------------------------
+# operator parameters and the Dslash family
+# ---------------------------------------------------------------------------
+
+
+def op_params(kind, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0, use_tbc=None, tbc_phases=None,
+              mass=0.0, twisted_mass=0.0, prec_mass_rho=0.0):
+    p = L.OpParams()
+    p.kind = kind
+    p.t_boundary = t_boundary
+    p.aniso_s = aniso_s
+    p.aniso_t = aniso_t
+    for d in range(4):
+        p.tbc_phases[d][0] = 1.0
+        p.tbc_phases[d][1] = 0.0
+    if use_tbc is not None and tbc_phases is not None:
+        for d in range(4):
+            p.use_tbc[d] = int(bool(use_tbc[d]))
+            p.tbc_phases[d][0] = tbc_phases[d][0]
+            p.tbc_phases[d][1] = tbc_phases[d][1]
+    p.mass = mass
+    p.twisted_mass = twisted_mass
+    p.prec_mass_rho = prec_mass_rho
+    return p
+
+
+def _h(f):
+    return None if f is None else f.h
+
+
+class Dslash:
+    """include/qphix/dslash_def.h:27-58"""
+
+    kind = L.WILSON
+
+    def __init__(self, lat, t_boundary, aniso_s, aniso_t, use_tbc=None, tbc_phases=None, **kw):
+        self.lat = lat
+        self.p = op_params(self.kind, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases, **kw)
+
+    def dslash(self, res, psi, u, isign, cb):
+        check(L._lib.qphix_gpu_dslash(C.byref(self.p), res.h, psi.h, u.h, None, None, isign, cb))
+
+    def dslashAChiMinusBDPsi(self, res, psi, chi, u, alpha, beta, isign, cb):
+        check(L._lib.qphix_gpu_dslash_achimbdpsi(C.byref(self.p), res.h, psi.h, chi.h, u.h, None,
+                                                 alpha, beta, isign, cb, 1.0))
+
+    def dslashDir(self, res, psi, u, cb, d):
+        check(L._lib.qphix_gpu_dslash_dir(C.byref(self.p), res.h, psi.h, u.h, cb, d))
+
+
+class ClovDslash(Dslash):
+    """include/qphix/clover_dslash_def.h:24-53"""
+
+    kind = L.CLOVER_OP
+
+    def __init__(self, lat, t_boundary, aniso_s, aniso_t, use_tbc=None, tbc_phases=None,
+                 prec_mass_rho=0.0):
+        super().__init__(lat, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases,
+                         prec_mass_rho=prec_mass_rho)
+
+    def dslash(self, res, psi, u, invclov, isign, cb):
+        check(L._lib.qphix_gpu_dslash(C.byref(self.p), res.h, psi.h, u.h, invclov.h, None, isign, cb))
+
+    def dslashAChiMinusBDPsi(self, res, psi, chi, u, clov, beta, isign, cb):
+        check(L._lib.qphix_gpu_dslash_achimbdpsi(C.byref(self.p), res.h, psi.h, chi.h, u.h, clov.h,
+                                                 0.0, beta, isign, cb, 1.0))
+
+    def clovMult(self, res, chi, clov):
+        check(L._lib.qphix_gpu_clover_apply(res.h, chi.h, clov.h))
+
+
+class TMDslash(Dslash):
+    """include/qphix/tm_dslash_def.h:23-49"""
+
+    kind = L.TM
+
+    def __init__(self, lat, t_boundary, aniso_s, aniso_t, mass, twisted_mass, use_tbc=None,
+                 tbc_phases=None):
+        super().__init__(lat, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases, mass=mass,
+                         twisted_mass=twisted_mass)
+
+    def dslashAChiMinusBDPsi(self, res, psi, chi, u, alpha, beta, isign, cb, musign=1.0):
+        check(L._lib.qphix_gpu_dslash_achimbdpsi(C.byref(self.p), res.h, psi.h, chi.h, u.h, None,
+                                                 alpha, beta, isign, cb, musign))
+
+
+class TMClovDslash(Dslash):
+    """include/qphix/tm_clov_dslash_def.h:30-66"""
+
+    kind = L.TMCLOVER
+
+    def __init__(self, lat, t_boundary, aniso_s, aniso_t, use_tbc=None, tbc_phases=None,
+                 prec_mass_rho=0.0):
+        super().__init__(lat, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases,
+                         prec_mass_rho=prec_mass_rho)
+
+    def dslash(self, res, psi, u, invclov, isign, cb):
+        check(L._lib.qphix_gpu_dslash(C.byref(self.p), res.h, psi.h, u.h, invclov[0].h, invclov[1].h,
+                                      isign, cb))
+
+    def dslashAChiMinusBDPsi(self, res, psi, chi, u, clov, beta, isign, cb):
+        check(L._lib.qphix_gpu_dslash_achimbdpsi(C.byref(self.p), res.h, psi.h, chi.h, u.h, clov.h,
+                                                 0.0, beta, isign, cb, 1.0))
+
+
+# ---------------------------------------------------------------------------
+# even-odd operators
+# ---------------------------------------------------------------------------
+
+
+class EvenOddLinearOperator:
+    """include/qphix/linearOp.h:9-92: operator()(res, in, isign, target_cb=1)"""
+
+    def __init__(self, p, gauge, clov=None, invclov=None, finv=(None, None)):
+        self.p = p
+        self.fields = (gauge, clov, invclov, finv)
+        h = C.c_void_p()
+        check(L._lib.qphix_gpu_eo_op_create(C.byref(p), gauge.h, _h(clov), _h(invclov), _h(finv[0]),
+                                            _h(finv[1]), C.byref(h)))
+        self.h = h
+        self.lat = gauge.lat
+
+    def __call__(self, res, inp, isign=1, target_cb=1):
+        check(L._lib.qphix_gpu_eo_op_apply(self.h, res.h, inp.h, isign, target_cb))
+
+    def close(self):
+        if getattr(self, "h", None):
+            L._lib.qphix_gpu_eo_op_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class EvenOddWilsonOperator(EvenOddLinearOperator):
+    """include/qphix/wilson.h:20-40"""
+
+    def __init__(self, mass, u, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0, use_tbc=None,
+                 tbc_phases=None):
+        super().__init__(op_params(L.WILSON, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases,
+                                   mass=mass), u)
+
+
+class EvenOddCloverOperator(EvenOddLinearOperator):
+    """include/qphix/clover.h:31-102 (clov = A_oo, invclov = A_ee^-1)"""
+
+    def __init__(self, u, clov, invclov, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0, use_tbc=None,
+                 tbc_phases=None, prec_mass_rho=0.0):
+        super().__init__(op_params(L.CLOVER_OP, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases,
+                                   prec_mass_rho=prec_mass_rho), u, clov, invclov)
+
+
+class EvenOddTMWilsonOperator(EvenOddLinearOperator):
+    """include/qphix/twisted_mass.h:22-46"""
+
+    def __init__(self, mass, twisted_mass, u, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0,
+                 use_tbc=None, tbc_phases=None):
+        super().__init__(op_params(L.TM, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases,
+                                   mass=mass, twisted_mass=twisted_mass), u)
+
+
+class EvenOddTMCloverOperator(EvenOddLinearOperator):
+    """include/qphix/twisted_mass_clover.h:29-73 (invclov = [(A+i mu g5)^-1, (A-i mu g5)^-1])"""
+
+    def __init__(self, u, clov, invclov, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0, use_tbc=None,
+                 tbc_phases=None, prec_mass_rho=0.0):
+        super().__init__(op_params(L.TMCLOVER, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases,
+                                   prec_mass_rho=prec_mass_rho), u, clov, None, tuple(invclov))
+
+
+# ---------------------------------------------------------------------------
+# solvers
+# ---------------------------------------------------------------------------
+
+
+def _infos(n):
+    return (L.SolveInfo * n)()
+
+
+def _as_dicts(infos):
+    return [dict(n_iters=i.n_iters, rsd_sq_final=i.rsd_sq_final, site_flops=i.site_flops,
+                 mv_apps=i.mv_apps, status=i.status, true_rel_resid=i.true_rel_resid,
+                 seconds=i.seconds) for i in infos]
+
+
+def _solve_rc(rc):
+    # non-convergence and breakdown are reported through info, like the reference
+    if rc not in (L.OK, L.ENOTCONV, L.EBREAKDOWN):
+        check(rc)
+
+
+class InvCG:
+    """include/qphix/invcg.h:31-88"""
+
+    def __init__(self, M, max_iters):
+        self.M, self.max_iters = M, max_iters
+
+    def __call__(self, x, rhs, rsd_target, isign=1, cb=1):
+        inf = _infos(x.nrhs)
+        _solve_rc(L._lib.qphix_gpu_solve_cg(self.M.h, x.h, rhs.h, rsd_target, self.max_iters, isign,
+                                            cb, inf))
+        return _as_dicts(inf)
+
+
+class InvBiCGStab(InvCG):
+    """include/qphix/invbicgstab.h:24-80"""
+
+    def __call__(self, x, rhs, rsd_target, isign=1, cb=1):
+        inf = _infos(x.nrhs)
+        _solve_rc(L._lib.qphix_gpu_solve_bicgstab(self.M.h, x.h, rhs.h, rsd_target, self.max_iters,
+                                                  isign, cb, inf))
+        return _as_dicts(inf)
+
+
+class InvMR:
+    """include/qphix/invmr.h:249-300"""
+
+    def __init__(self, M, max_iters, omega=1.0):
+        self.M, self.max_iters, self.omega = M, max_iters, omega
+
+    def __call__(self, x, rhs, rsd_target, isign=1, cb=1):
+        inf = _infos(x.nrhs)
+        _solve_rc(L._lib.qphix_gpu_solve_mr(self.M.h, x.h, rhs.h, rsd_target, self.max_iters,
+                                            self.omega, isign, cb, inf))
+        return _as_dicts(inf)
+
+
+class InvRichardsonMultiPrec:
+    """include/qphix/inv_richardson_multiprec.h:22-42 (inner solver on op_inner)"""
+
+    INNER = {"cg": L.SOLVER_CG, "bicgstab": L.SOLVER_BICGSTAB, "mr": L.SOLVER_MR}
+
+    def __init__(self, M_outer, M_inner, inner="bicgstab", delta=0.1, max_iters=100,
+                 inner_max_iters=5000):
+        self.Mo, self.Mi = M_outer, M_inner
+        self.inner = self.INNER[inner]
+        self.delta, self.max_iters, self.inner_max = delta, max_iters, inner_max_iters
+
+    def __call__(self, x, rhs, rsd_target, isign=1, cb=1):
+        inf = _infos(x.nrhs)
+        _solve_rc(L._lib.qphix_gpu_solve_richardson(self.Mo.h, self.Mi.h, self.inner, x.h, rhs.h,
+                                                    rsd_target, self.delta, self.max_iters,
+                                                    self.inner_max, isign, cb, inf))
+        return _as_dicts(inf)
+
+
+class MInvCG:
+    """include/qphix/minvcg.h:23-77"""
+
+    def __init__(self, M, max_iters, max_shifts=32):
+        self.M, self.max_iters, self.max_shifts = M, max_iters, max_shifts
+
+    def __call__(self, xs, rhs, shifts, rsd_targets, isign=1, cb=1):
+        n = len(shifts)
+        if n > self.max_shifts:
+            raise ValueError("too many shifts")
+        xh = (C.c_void_p * n)(*[x.h.value for x in xs])
+        sh = np.ascontiguousarray(shifts, dtype=np.float64)
+        rs = np.ascontiguousarray(rsd_targets, dtype=np.float64)
+        fin = np.zeros(n)
+        it = C.c_int(0)
+        mv = C.c_ulong(0)
+        check(L._lib.qphix_gpu_solve_mshift_cg(self.M.h, C.cast(xh, L.PP), rhs.h, n,
+                                               sh.ctypes.data_as(C.c_void_p),
+                                               rs.ctypes.data_as(C.c_void_p), self.max_iters, isign,
+                                               cb, C.byref(it), fin.ctypes.data_as(C.c_void_p),
+                                               C.byref(mv)))
+        return it.value, fin, mv.value
+
+
+# ---------------------------------------------------------------------------
+# BLAS
+# ---------------------------------------------------------------------------
+
+
+def norm2(x):
+    out = np.zeros(x.nrhs)
+    check(L._lib.qphix_gpu_blas_norm2(x.h, out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+def inner_product(x, y):
+    out = np.zeros(2 * x.nrhs)
+    check(L._lib.qphix_gpu_blas_inner_product(x.h, y.h, out.ctypes.data_as(C.c_void_p)))
+    return out[0::2] + 1j * out[1::2]
+
+
+def caxpby(a, x, b, y):
+    av = (C.c_double * 2)(complex(a).real, complex(a).imag)
+    bv = (C.c_double * 2)(complex(b).real, complex(b).imag)
+    check(L._lib.qphix_gpu_blas_caxpby(av, x.h, bv, y.h))
+
+
+def copy(dst, src):
+    check(L._lib.qphix_gpu_blas_copy(dst.h, src.h))
+
+
+def zero(x):
+    check(L._lib.qphix_gpu_blas_zero(x.h))

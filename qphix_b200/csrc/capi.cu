@@ -1,0 +1,1516 @@
+// C ABI implementation: lattices, fields, the Dslash family, the even-odd
+// operators, BLAS and the Krylov solvers.  All device work of a lattice is
+// ordered on its stream.  Solver iterations keep every scalar on the device
+// (qpx_finalize.cuh) and are captured once per solve as a CUDA graph that is
+// replayed until the device-side `done` flag is raised; the host only polls
+// that flag every few iterations.
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "qpx_finalize.cuh"
+#include "qpx_host.h"
+
+using namespace qpx;
+
+static thread_local std::string g_last_error;
+
+template <typename F>
+static int guard(F &&f)
+{
+  try {
+    f();
+    return QPHIX_GPU_OK;
+  } catch (const Error &e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const std::exception &e) {
+    g_last_error = e.what();
+    return QPHIX_GPU_EINVAL;
+  }
+}
+
+static int nblocks_for(long long n) { return (int)((n + QPX_BLOCK - 1) / QPX_BLOCK); }
+
+static std::atomic<unsigned long long> g_launches{0};
+
+static void check_launch()
+{
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) throw Error(QPHIX_GPU_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  g_launches++;
+}
+
+extern "C" int qphix_gpu_launch_count(unsigned long long *out)
+{
+  if (!out) return QPHIX_GPU_EINVAL;
+  *out = g_launches.load();
+  return QPHIX_GPU_OK;
+}
+
+static void lattice_release(qphix_gpu_lattice_s *L);
+
+static bool env_flag(const char *name)
+{
+  const char *v = getenv(name);
+  return v && v[0] && v[0] != '0';
+}
+
+// ===========================================================================
+// lattice
+// ===========================================================================
+extern "C" int qphix_gpu_version(void) { return 100; }
+extern "C" const char *qphix_gpu_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int qphix_gpu_init(int device)
+{
+  return guard([&] {
+    int n = 0;
+    QPX_CUDA(cudaGetDeviceCount(&n));
+    QPX_REQUIRE(device >= 0 && device < n, "device index out of range");
+    QPX_CUDA(cudaSetDevice(device));
+  });
+}
+
+extern "C" int qphix_gpu_lattice_create(const int latt[4], qphix_gpu_lattice *out)
+{
+  return guard([&] {
+    QPX_REQUIRE(latt && out, "null argument");
+    for (int i = 0; i < 4; i++) QPX_REQUIRE(latt[i] >= 2, "every lattice extent must be >= 2");
+    QPX_REQUIRE(latt[0] % 2 == 0, "Nx must be even (checkerboarding)");
+    QPX_REQUIRE((latt[1] * latt[2] * latt[3]) % 2 == 0 || true, "");
+    auto *L = new qphix_gpu_lattice_s();
+    try {
+      for (int i = 0; i < 4; i++) L->dims[i] = latt[i];
+      L->nxh = latt[0] / 2;
+      L->vh = (long long)L->nxh * latt[1] * latt[2] * latt[3];
+      QPX_REQUIRE(L->vh < (1LL << 30), "lattice too large for 32-bit site indices");
+      L->stride = (L->vh + 63) / 64 * 64;
+      QPX_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
+      L->owns_stream = true;
+      L->partials_len = (size_t)nblocks_for(L->vh) * QPX_MAX_RHS * QPX_MAX_RED;
+      QPX_CUDA(cudaMalloc(&L->partials, L->partials_len * sizeof(double)));
+      QPX_CUDA(cudaMalloc(&L->ticket, 64 * sizeof(unsigned int)));
+      QPX_CUDA(cudaMemset(L->ticket, 0, 64 * sizeof(unsigned int)));
+      QPX_CUDA(cudaMalloc(&L->result, QPX_MAX_RHS * QPX_MAX_RED * sizeof(double)));
+      QPX_CUDA(cudaMallocHost(&L->h_result, QPX_MAX_RHS * QPX_MAX_RED * sizeof(double)));
+      QPX_CUDA(cudaMalloc(&L->state, sizeof(SolverState)));
+      QPX_CUDA(cudaMallocHost(&L->h_state, sizeof(SolverState)));
+      memset(L->h_state, 0, sizeof(SolverState));
+      QPX_CUDA(cudaMemset(L->state, 0, sizeof(SolverState)));
+    } catch (...) {
+      lattice_release(L);
+      throw;
+    }
+    *out = L;
+  });
+}
+
+static void lattice_release(qphix_gpu_lattice_s *L)
+{
+  if (!L) return;
+  if (--L->refs > 0) return;
+  if (L->stream) cudaStreamSynchronize(L->stream);
+  cudaFree(L->partials);
+  cudaFree(L->ticket);
+  cudaFree(L->result);
+  cudaFreeHost(L->h_result);
+  cudaFree(L->state);
+  cudaFreeHost(L->h_state);
+  cudaFree(L->staging);
+  if (L->stream && L->owns_stream) cudaStreamDestroy(L->stream);
+  delete L;
+}
+
+// The lattice stays alive until its last field is destroyed as well.
+extern "C" int qphix_gpu_lattice_destroy(qphix_gpu_lattice L)
+{
+  return guard([&] { lattice_release(L); });
+}
+
+extern "C" int qphix_gpu_lattice_set_stream(qphix_gpu_lattice L, void *stream)
+{
+  return guard([&] {
+    QPX_REQUIRE(L, "null lattice");
+    QPX_REQUIRE(stream, "a non-default stream is required (iterations are graph-captured)");
+    QPX_CUDA(cudaStreamSynchronize(L->stream));
+    if (L->owns_stream) QPX_CUDA(cudaStreamDestroy(L->stream));
+    L->stream = (cudaStream_t)stream;
+    L->owns_stream = false;
+  });
+}
+
+extern "C" int qphix_gpu_lattice_sync(qphix_gpu_lattice L)
+{
+  return guard([&] {
+    QPX_REQUIRE(L, "null lattice");
+    QPX_CUDA(cudaStreamSynchronize(L->stream));
+  });
+}
+
+extern "C" long qphix_gpu_lattice_volcb(qphix_gpu_lattice L) { return L ? (long)L->vh : -1; }
+
+static void *staging(qphix_gpu_lattice_s *L, size_t bytes)
+{
+  if (bytes > L->staging_bytes) {
+    QPX_CUDA(cudaStreamSynchronize(L->stream));
+    cudaFree(L->staging);
+    L->staging = nullptr;
+    L->staging_bytes = 0;
+    QPX_CUDA(cudaMalloc(&L->staging, bytes));
+    L->staging_bytes = bytes;
+  }
+  return L->staging;
+}
+
+// ===========================================================================
+// fields
+// ===========================================================================
+extern "C" int qphix_gpu_field_create(qphix_gpu_lattice L, int kind, int prec, int recon, int nrhs,
+                                      qphix_gpu_field *out)
+{
+  return guard([&] {
+    QPX_REQUIRE(L && out, "null argument");
+    QPX_REQUIRE(prec >= PREC_F64 && prec <= PREC_BF16, "bad precision");
+    auto *f = new qphix_gpu_field_s();
+    f->lat = L;
+    L->refs++;
+    f->kind = kind;
+    f->prec = prec;
+    f->recon = 0;
+    f->nrhs = 1;
+    size_t rows = 0;
+    switch (kind) {
+    case QPHIX_GPU_SPINOR:
+      QPX_REQUIRE(nrhs >= 1 && nrhs <= QPX_MAX_RHS, "nrhs must be in [1, 32]");
+      f->nrhs = nrhs;
+      f->spec = spinor_spec(prec);
+      rows = (size_t)nrhs;
+      break;
+    case QPHIX_GPU_GAUGE:
+      QPX_REQUIRE(recon == 12 || recon == 18, "gauge recon must be 12 or 18");
+      f->recon = recon;
+      f->spec = gauge_spec(prec, recon);
+      rows = 8;  // [cb][mu]
+      break;
+    case QPHIX_GPU_CLOVER:
+      f->spec = clover_spec(prec, 72);
+      rows = 1;
+      break;
+    case QPHIX_GPU_FULLCLOVER:
+      f->spec = clover_spec(prec, 144);
+      rows = 1;
+      break;
+    default:
+      L->refs--;
+      delete f;
+      throw Error(QPHIX_GPU_EINVAL, "bad field kind");
+    }
+    f->bytes = rows * f->spec.nchunk * (size_t)f->spec.chunk_bytes * L->stride;
+    cudaError_t e = cudaMalloc(&f->data, f->bytes);
+    if (e != cudaSuccess) {
+      L->refs--;
+      delete f;
+      throw Error(QPHIX_GPU_ENOMEM, std::string("field allocation: ") + cudaGetErrorString(e));
+    }
+    cudaMemsetAsync(f->data, 0, f->bytes, L->stream);
+    if (kind == QPHIX_GPU_SPINOR && prec >= PREC_F16) {
+      e = cudaMalloc(&f->norm, sizeof(float) * L->stride * f->nrhs);
+      if (e != cudaSuccess) {
+        cudaFree(f->data);
+        L->refs--;
+        delete f;
+        throw Error(QPHIX_GPU_ENOMEM, std::string("norm allocation: ") + cudaGetErrorString(e));
+      }
+      cudaMemsetAsync(f->norm, 0, sizeof(float) * L->stride * f->nrhs, L->stream);
+      f->bytes += sizeof(float) * L->stride * f->nrhs;
+    }
+    *out = f;
+  });
+}
+
+extern "C" int qphix_gpu_field_destroy(qphix_gpu_field f)
+{
+  return guard([&] {
+    if (!f) return;
+    cudaStreamSynchronize(f->lat->stream);
+    cudaFree(f->data);
+    cudaFree(f->norm);
+    qphix_gpu_lattice_s *L = f->lat;
+    delete f;
+    lattice_release(L);
+  });
+}
+
+extern "C" int qphix_gpu_field_bytes(qphix_gpu_field f, size_t *bytes)
+{
+  return guard([&] {
+    QPX_REQUIRE(f && bytes, "null argument");
+    *bytes = f->bytes;
+  });
+}
+
+static HostLayout make_layout(const qphix_gpu_field_s *f, const qphix_gpu_host_layout *hl)
+{
+  HostLayout L{};
+  QPX_REQUIRE(hl, "null host layout");
+  L.kind = hl->kind;
+  L.ft = hl->ft;
+  QPX_REQUIRE(L.ft >= 0 && L.ft <= 2, "bad host element type");
+  if (L.kind == HOST_CANONICAL) {
+    QPX_REQUIRE(L.ft == HFT_F64, "canonical host arrays are FP64");
+    return L;
+  }
+  QPX_REQUIRE(L.kind == HOST_QPHIX, "bad host layout kind");
+  const auto *lat = f->lat;
+  L.V = hl->veclen;
+  L.S = hl->soalen;
+  L.c12 = hl->compress12 ? 1 : 0;
+  QPX_REQUIRE(L.V > 0 && L.S > 0 && L.V % L.S == 0, "soalen must divide veclen");
+  QPX_REQUIRE(lat->nxh % L.S == 0, "Nx/2 must be divisible by soalen");
+  L.nvecs = lat->nxh / L.S;
+  L.ngy = L.V / L.S;
+  QPX_REQUIRE(lat->dims[1] % L.ngy == 0, "Ny must be divisible by veclen/soalen");
+  L.pxy = L.nvecs * lat->dims[1] + hl->pad_xy;
+  L.pxyz = L.pxy * lat->dims[2] + hl->pad_xyz;
+  return L;
+}
+
+static size_t host_elem_bytes(int ft) { return ft == HFT_F64 ? 8 : (ft == HFT_F32 ? 4 : 2); }
+
+// number of host elements of a field transfer
+static size_t host_elems(const qphix_gpu_field_s *f, const HostLayout &L, int nrhs)
+{
+  const auto *lat = f->lat;
+  size_t vh = lat->vh;
+  if (L.kind == HOST_CANONICAL) {
+    switch (f->kind) {
+    case QPHIX_GPU_SPINOR: return (size_t)nrhs * vh * 24;
+    case QPHIX_GPU_GAUGE: return 2 * 4 * vh * 18;
+    case QPHIX_GPU_CLOVER: return vh * 72;
+    default: return vh * 144;
+    }
+  }
+  size_t nt = lat->dims[3];
+  switch (f->kind) {
+  case QPHIX_GPU_SPINOR: return (size_t)nrhs * L.pxyz * nt * 24 * L.S;
+  case QPHIX_GPU_GAUGE: return (size_t)L.pxyz * nt * L.S / L.V * 8 * (L.c12 ? 2 : 3) * 3 * 2 * L.V;
+  case QPHIX_GPU_CLOVER: return (size_t)L.pxyz * nt * L.S / L.V * 72 * L.V;
+  default: return (size_t)L.pxyz * nt * L.S / L.V * 144 * L.V;
+  }
+}
+
+static SpinorArg rhs_view(const qphix_gpu_field_s *f, int rhs)
+{
+  SpinorArg a = f->sarg();
+  if (rhs > 0) {
+    a.data = (char *)a.data + (size_t)rhs * a.rhs_stride_chunks * f->spec.chunk_bytes;
+    if (a.norm) a.norm += (size_t)rhs * f->lat->stride;
+  }
+  return a;
+}
+
+extern "C" int qphix_gpu_field_upload(qphix_gpu_field f, const void *host, const qphix_gpu_host_layout *hl, int cb,
+                                      int rhs)
+{
+  return guard([&] {
+    QPX_REQUIRE(f && host, "null argument");
+    auto *lat = f->lat;
+    HostLayout L = make_layout(f, hl);
+    Geom g = lat->geom();
+    int nr = (f->kind == QPHIX_GPU_SPINOR) ? ((rhs < 0) ? f->nrhs : 1) : 1;
+    QPX_REQUIRE(rhs < f->nrhs, "rhs index out of range");
+    size_t bytes = host_elems(f, L, nr) * host_elem_bytes(L.ft);
+    void *st = staging(lat, bytes);
+    QPX_CUDA(cudaMemcpyAsync(st, host, bytes, cudaMemcpyHostToDevice, lat->stream));
+    switch (f->kind) {
+    case QPHIX_GPU_SPINOR: {
+      SpinorArg a = rhs_view(f, rhs < 0 ? 0 : rhs);
+      launch_spinor_in(f->prec, g, L, st, a, nr, dim3(nblocks_for(lat->vh), nr), lat->stream);
+      break;
+    }
+    case QPHIX_GPU_GAUGE: {
+      long long slab = (long long)f->spec.nchunk * f->spec.chunk_bytes * lat->stride;
+      if (L.kind == HOST_CANONICAL) {
+        QPX_REQUIRE(cb == -1, "canonical gauge arrays hold both checkerboards (cb = -1)");
+        for (int c = 0; c < 2; c++)
+          launch_gauge_in(f->prec, g, L, st, f->data, lat->stride, slab, f->spec.vpc, f->recon, c,
+                          dim3(nblocks_for(lat->vh), 4), lat->stream);
+      } else {
+        QPX_REQUIRE(cb == 0 || cb == 1, "qphix gauge arrays hold one checkerboard (cb = 0 or 1)");
+        launch_gauge_in(f->prec, g, L, st, f->data, lat->stride, slab, f->spec.vpc, f->recon, cb,
+                        dim3(nblocks_for(lat->vh), 4), lat->stream);
+      }
+      break;
+    }
+    case QPHIX_GPU_CLOVER:
+    case QPHIX_GPU_FULLCLOVER:
+      launch_clover_in(f->prec, g, L, st, f->data, lat->stride, f->spec.vpc,
+                       f->kind == QPHIX_GPU_CLOVER ? 72 : 144, dim3(nblocks_for(lat->vh)), lat->stream);
+      break;
+    }
+    check_launch();
+  });
+}
+
+extern "C" int qphix_gpu_field_download(qphix_gpu_field f, void *host, const qphix_gpu_host_layout *hl, int rhs)
+{
+  return guard([&] {
+    QPX_REQUIRE(f && host, "null argument");
+    auto *lat = f->lat;
+    HostLayout L = make_layout(f, hl);
+    Geom g = lat->geom();
+    QPX_REQUIRE(rhs < f->nrhs, "rhs index out of range");
+    int nr = (f->kind == QPHIX_GPU_SPINOR) ? ((rhs < 0) ? f->nrhs : 1) : 1;
+    size_t bytes = host_elems(f, L, nr) * host_elem_bytes(L.ft);
+    void *st = staging(lat, bytes);
+    if (f->kind == QPHIX_GPU_SPINOR) {
+      if (L.kind == HOST_QPHIX) QPX_CUDA(cudaMemsetAsync(st, 0, bytes, lat->stream));
+      SpinorArg a = rhs_view(f, rhs < 0 ? 0 : rhs);
+      launch_spinor_out(f->prec, g, L, st, a, nr, dim3(nblocks_for(lat->vh), nr), lat->stream);
+    } else if (f->kind == QPHIX_GPU_CLOVER || f->kind == QPHIX_GPU_FULLCLOVER) {
+      QPX_REQUIRE(L.kind == HOST_CANONICAL, "clover download supports the canonical layout only");
+      launch_clover_out(f->prec, g, st, f->data, lat->stride, f->spec.vpc, f->kind == QPHIX_GPU_CLOVER ? 72 : 144,
+                        dim3(nblocks_for(lat->vh)), lat->stream);
+    } else {
+      throw Error(QPHIX_GPU_EUNSUPPORTED, "gauge download is not supported");
+    }
+    check_launch();
+    QPX_CUDA(cudaMemcpyAsync(host, st, bytes, cudaMemcpyDeviceToHost, lat->stream));
+    QPX_CUDA(cudaStreamSynchronize(lat->stream));
+  });
+}
+
+static void convert_field(qphix_gpu_field_s *dst, qphix_gpu_field_s *src, Coef scale, SolverState *state)
+{
+  auto *lat = src->lat;
+  launch_convert(dst->prec, src->prec, (int)lat->vh, src->sarg(), dst->sarg(), scale, state,
+                 dim3(nblocks_for(lat->vh), src->nrhs), lat->stream);
+  check_launch();
+}
+
+extern "C" int qphix_gpu_field_convert(qphix_gpu_field dst, qphix_gpu_field src, double scale)
+{
+  return guard([&] {
+    QPX_REQUIRE(dst && src, "null argument");
+    QPX_REQUIRE(dst->kind == QPHIX_GPU_SPINOR && src->kind == QPHIX_GPU_SPINOR, "convert works on spinors");
+    QPX_REQUIRE(dst->nrhs == src->nrhs && dst->lat == src->lat, "shape mismatch");
+    Coef c{scale, 0, nullptr, nullptr};
+    convert_field(dst, src, c, nullptr);
+  });
+}
+
+// ===========================================================================
+// Dslash launch plumbing
+// ===========================================================================
+static DslashArgs base_args(const qphix_gpu_op_params &p, qphix_gpu_lattice_s *lat, int isign, int cb, int nrhs)
+{
+  DslashArgs a;
+  memset(&a, 0, sizeof(a));
+  a.geom = lat->geom();
+  a.cb = cb;
+  a.isign = isign;
+  a.nrhs = nrhs;
+  a.dir_mask = 0xFFu;
+  a.coeff_s = p.aniso_s;
+  a.coeff_t = p.aniso_t;
+  a.coeff_t_edge = p.aniso_t * p.t_boundary;
+  a.tbc_mask = 0;
+  for (int d = 0; d < 4; d++) {
+    a.tbc[d][0] = 1.0;
+    a.tbc[d][1] = 0.0;
+    if (p.use_tbc[d]) {
+      a.tbc_mask |= 1 << d;
+      a.tbc[d][0] = p.tbc_phases[d][0];
+      a.tbc[d][1] = p.tbc_phases[d][1];
+    }
+  }
+  a.post = POST_STORE;
+  return a;
+}
+
+static int pick_tile(int prec, int nrhs)
+{
+  const char *force = getenv("QPHIX_GPU_RHS_TILE");
+  if (force) {
+    int R = atoi(force);
+    if (R > 0 && nrhs % R == 0 && dslash_tile_ok(prec, R)) return R;
+  }
+  for (int R : {4, 2, 1})
+    if (nrhs % R == 0 && dslash_tile_ok(prec, R)) return R;
+  return 1;
+}
+
+static void set_reduce(DslashArgs &a, qphix_gpu_lattice_s *lat, int mask, int fin, SolverState *st)
+{
+  a.red.mask = mask;
+  a.red.nval = red_nval(mask);
+  a.red.fin = fin;
+  a.red.partials = lat->partials;
+  a.red.ticket = lat->ticket;
+  a.red.result = lat->result;
+  a.state = st;
+}
+
+static void dslash_launch(qphix_gpu_lattice_s *lat, int prec, int recon, int epi, int achi, DslashArgs &a)
+{
+  int R = pick_tile(prec, a.nrhs);
+  if (a.red.mask) {
+    a.red.partials = lat->partials;
+    a.red.ticket = lat->ticket;
+    a.red.result = lat->result;
+    a.red.nval = red_nval(a.red.mask);
+  }
+  dim3 grid(nblocks_for(lat->vh), a.nrhs / R);
+  launch_dslash(prec, recon, epi, achi, R, a, grid, lat->stream);
+  check_launch();
+}
+
+static void require_spinor(const qphix_gpu_field_s *f, const char *what)
+{
+  if (!f || f->kind != QPHIX_GPU_SPINOR) throw Error(QPHIX_GPU_EINVAL, std::string(what) + " must be a spinor field");
+}
+
+static void require_same(const qphix_gpu_field_s *a, const qphix_gpu_field_s *b)
+{
+  if (a->lat != b->lat) throw Error(QPHIX_GPU_EINVAL, "fields belong to different lattices");
+  if (a->prec != b->prec) throw Error(QPHIX_GPU_EINVAL, "fields have different precisions");
+}
+
+static void tm_derived(const qphix_gpu_op_params &p, double &dmu, double &dmu_inv)
+{
+  // include/qphix/tm_dslash_body.h:32-34
+  double alpha = 4.0 + p.mass;
+  dmu = p.twisted_mass / alpha;
+  dmu_inv = alpha / (p.twisted_mass * p.twisted_mass + alpha * alpha);
+}
+
+// res = EPI(D psi) on checkerboard cb
+static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphix_gpu_field_s *psi,
+                        qphix_gpu_field_s *gauge, qphix_gpu_field_s *aux, qphix_gpu_field_s *aux2, int isign,
+                        int cb, unsigned dir_mask = 0xFFu)
+{
+  require_spinor(res, "res");
+  require_spinor(psi, "psi");
+  QPX_REQUIRE(gauge && gauge->kind == QPHIX_GPU_GAUGE, "gauge must be a gauge field");
+  require_same(res, psi);
+  require_same(res, gauge);
+  QPX_REQUIRE(res->nrhs == psi->nrhs, "rhs count mismatch");
+  QPX_REQUIRE(res != psi, "res and psi must be different fields");
+  QPX_REQUIRE(isign == 1 || isign == -1, "isign must be +1 or -1");
+  QPX_REQUIRE(cb == 0 || cb == 1, "cb must be 0 or 1");
+  auto *lat = res->lat;
+  DslashArgs a = base_args(p, lat, isign, cb, res->nrhs);
+  a.dir_mask = dir_mask;
+  a.out = res->sarg();
+  a.in = psi->sarg();
+  a.gauge = gauge->garg();
+  int epi = EPI_NONE;
+  switch (p.kind) {
+  case QPHIX_GPU_WILSON:
+    break;
+  case QPHIX_GPU_CLOVER_OP:
+    QPX_REQUIRE(aux && aux->kind == QPHIX_GPU_CLOVER, "clover dslash needs A^-1 (clover field)");
+    require_same(res, aux);
+    a.clov = aux->carg();
+    epi = EPI_CLOV;
+    break;
+  case QPHIX_GPU_TM:
+    tm_derived(p, a.mu, a.mu_inv);
+    epi = EPI_TMINV;
+    break;
+  case QPHIX_GPU_TMCLOVER: {
+    qphix_gpu_field_s *f = (isign == 1) ? aux : aux2;  // tm_clov_dslash_body.h:352
+    QPX_REQUIRE(f && f->kind == QPHIX_GPU_FULLCLOVER, "tm clover dslash needs the two full inverses");
+    require_same(res, f);
+    a.clov = f->carg();
+    epi = EPI_FCLOV;
+    break;
+  }
+  default:
+    throw Error(QPHIX_GPU_EINVAL, "bad operator kind");
+  }
+  dslash_launch(lat, res->prec, gauge->recon, epi, ACHI_NONE, a);
+}
+
+// options for the second (achimbdpsi) kernel of an operator application
+struct ApplyOpts {
+  int post = POST_STORE;
+  int red_mask = 0;
+  int fin = FIN_NONE;
+  SolverState *state = nullptr;
+  const qphix_gpu_field_s *w = nullptr, *r = nullptr, *x = nullptr, *p = nullptr;
+};
+
+static void achi_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphix_gpu_field_s *psi,
+                      qphix_gpu_field_s *chi, qphix_gpu_field_s *gauge, qphix_gpu_field_s *aux, double alpha,
+                      double beta, int isign, int cb, double musign, const ApplyOpts &o)
+{
+  require_spinor(res, "res");
+  require_spinor(psi, "psi");
+  require_spinor(chi, "chi");
+  QPX_REQUIRE(gauge && gauge->kind == QPHIX_GPU_GAUGE, "gauge must be a gauge field");
+  require_same(res, psi);
+  require_same(res, chi);
+  require_same(res, gauge);
+  QPX_REQUIRE(res->nrhs == psi->nrhs && res->nrhs == chi->nrhs, "rhs count mismatch");
+  QPX_REQUIRE(res != psi, "res and psi must be different fields");
+  QPX_REQUIRE(isign == 1 || isign == -1, "isign must be +1 or -1");
+  QPX_REQUIRE(cb == 0 || cb == 1, "cb must be 0 or 1");
+  auto *lat = res->lat;
+  DslashArgs a = base_args(p, lat, isign, cb, res->nrhs);
+  a.out = res->sarg();
+  a.in = psi->sarg();
+  a.chi = chi->sarg();
+  a.gauge = gauge->garg();
+  a.alpha = alpha;
+  a.beta = beta;
+  int achi = ACHI_ALPHA;
+  switch (p.kind) {
+  case QPHIX_GPU_WILSON:
+    break;
+  case QPHIX_GPU_CLOVER_OP:
+  case QPHIX_GPU_TMCLOVER:
+    QPX_REQUIRE(aux && aux->kind == QPHIX_GPU_CLOVER, "clover achimbdpsi needs the clover term A");
+    require_same(res, aux);
+    a.clov = aux->carg();
+    a.rho = p.prec_mass_rho;
+    achi = ACHI_CLOV;
+    break;
+  case QPHIX_GPU_TM: {
+    double dmu, dmu_inv;
+    tm_derived(p, dmu, dmu_inv);
+    a.mu = musign * dmu;
+    achi = ACHI_TM;
+    break;
+  }
+  default:
+    throw Error(QPHIX_GPU_EINVAL, "bad operator kind");
+  }
+  a.post = o.post;
+  if (o.w) a.w = o.w->sarg();
+  if (o.r) a.r = o.r->sarg();
+  if (o.x) a.x = o.x->sarg();
+  if (o.p) a.p = o.p->sarg();
+  a.state = o.state;
+  if (o.red_mask) set_reduce(a, lat, o.red_mask, o.fin, o.state);
+  dslash_launch(lat, res->prec, gauge->recon, EPI_NONE, achi, a);
+}
+
+static qphix_gpu_op_params wilson_params_of(const qphix_gpu_op_params &p)
+{
+  qphix_gpu_op_params q = p;
+  q.kind = QPHIX_GPU_WILSON;
+  return q;
+}
+
+extern "C" int qphix_gpu_dslash(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                                qphix_gpu_field gauge, qphix_gpu_field aux, qphix_gpu_field aux2, int isign, int cb)
+{
+  return guard([&] {
+    QPX_REQUIRE(p, "null params");
+    dslash_core(*p, res, psi, gauge, aux, aux2, isign, cb);
+  });
+}
+
+extern "C" int qphix_gpu_dslash_achimbdpsi(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                                           qphix_gpu_field chi, qphix_gpu_field gauge, qphix_gpu_field aux,
+                                           double alpha, double beta, int isign, int cb, double musign)
+{
+  return guard([&] {
+    QPX_REQUIRE(p, "null params");
+    achi_core(*p, res, psi, chi, gauge, aux, alpha, beta, isign, cb, musign, ApplyOpts());
+  });
+}
+
+extern "C" int qphix_gpu_dslash_dir(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                                    qphix_gpu_field gauge, int cb, int dir)
+{
+  return guard([&] {
+    QPX_REQUIRE(p, "null params");
+    QPX_REQUIRE(dir >= 0 && dir < 8, "dir must be in [0, 8)");
+    // include/qphix/dslash_body.h:1075-1157: isign +1; dir = 2 mu (+0) takes
+    // the forward-neighbour hop, 2 mu + 1 the backward one
+    int mu = dir / 2;
+    unsigned bit = (dir % 2 == 0) ? (1u << (2 * mu + 1)) : (1u << (2 * mu));
+    dslash_core(wilson_params_of(*p), res, psi, gauge, nullptr, nullptr, 1, cb, bit);
+  });
+}
+
+extern "C" int qphix_gpu_clover_apply(qphix_gpu_field res, qphix_gpu_field chi, qphix_gpu_field clov)
+{
+  return guard([&] {
+    require_spinor(res, "res");
+    require_spinor(chi, "chi");
+    QPX_REQUIRE(clov && clov->kind == QPHIX_GPU_CLOVER, "clov must be a clover field");
+    require_same(res, chi);
+    require_same(res, clov);
+    QPX_REQUIRE(res->nrhs == chi->nrhs, "rhs count mismatch");
+    // A chi = the clover achimbdpsi kernel with beta = 0, rho = 0 and no hops
+    auto *lat = res->lat;
+    qphix_gpu_op_params p{};
+    p.kind = QPHIX_GPU_CLOVER_OP;
+    p.aniso_s = p.aniso_t = 1.0;
+    p.t_boundary = 1.0;
+    DslashArgs a = base_args(p, lat, 1, 0, res->nrhs);
+    a.dir_mask = 0;
+    a.out = res->sarg();
+    a.in = chi->sarg();
+    a.chi = chi->sarg();
+    a.clov = clov->carg();
+    a.beta = 0.0;
+    a.rho = 0.0;
+    // dir_mask = 0 means no gauge access: any recon is fine
+    a.gauge.data = nullptr;
+    dslash_launch(lat, res->prec, 18, EPI_NONE, ACHI_CLOV, a);
+  });
+}
+
+// ===========================================================================
+// even-odd operators
+// ===========================================================================
+extern "C" int qphix_gpu_eo_op_create(const qphix_gpu_op_params *p, qphix_gpu_field gauge, qphix_gpu_field clov,
+                                      qphix_gpu_field invclov, qphix_gpu_field finv0, qphix_gpu_field finv1,
+                                      qphix_gpu_eo_op *out)
+{
+  return guard([&] {
+    QPX_REQUIRE(p && out, "null argument");
+    QPX_REQUIRE(gauge && gauge->kind == QPHIX_GPU_GAUGE, "gauge must be a gauge field");
+    if (p->kind == QPHIX_GPU_CLOVER_OP) QPX_REQUIRE(clov && invclov, "clover operator needs clov and invclov");
+    if (p->kind == QPHIX_GPU_TMCLOVER) QPX_REQUIRE(clov && finv0 && finv1, "tm clover operator needs clov, finv0/1");
+    auto *op = new qphix_gpu_eo_op_s();
+    op->p = *p;
+    op->gauge = gauge;
+    op->clov = clov;
+    op->invclov = invclov;
+    op->finv0 = finv0;
+    op->finv1 = finv1;
+    *out = op;
+  });
+}
+
+extern "C" int qphix_gpu_eo_op_destroy(qphix_gpu_eo_op op)
+{
+  return guard([&] {
+    if (!op) return;
+    for (auto &kv : op->tmp) qphix_gpu_field_destroy(kv.second);
+    delete op;
+  });
+}
+
+static qphix_gpu_field_s *op_tmp(qphix_gpu_eo_op_s *op, int nrhs)
+{
+  auto it = op->tmp.find(nrhs);
+  if (it != op->tmp.end()) return it->second;
+  qphix_gpu_field f = nullptr;
+  int rc = qphix_gpu_field_create(op->gauge->lat, QPHIX_GPU_SPINOR, op->gauge->prec, 0, nrhs, &f);
+  if (rc) throw Error(rc, g_last_error);
+  op->tmp[nrhs] = f;
+  return f;
+}
+
+// M_oo in = [diag] in - beta D_{target,other} [inv-diag] D_{other,target} in
+static void eo_apply(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *res, qphix_gpu_field_s *in, int isign, int target_cb,
+                     const ApplyOpts &o)
+{
+  require_spinor(in, "in");
+  qphix_gpu_field_s *tmp = op_tmp(op, in->nrhs);
+  const auto &p = op->p;
+  int other = 1 - target_cb;
+  switch (p.kind) {
+  case QPHIX_GPU_WILSON: {  // include/qphix/wilson.h:49-65
+    double alpha = 4.0 + p.mass, beta = 0.25 / alpha;
+    dslash_core(p, tmp, in, op->gauge, nullptr, nullptr, isign, other);
+    achi_core(p, res, tmp, in, op->gauge, nullptr, alpha, beta, isign, target_cb, 1.0, o);
+    break;
+  }
+  case QPHIX_GPU_CLOVER_OP:  // include/qphix/clover.h:162-172
+    dslash_core(p, tmp, in, op->gauge, op->invclov, nullptr, isign, other);
+    achi_core(p, res, tmp, in, op->gauge, op->clov, 0.0, 0.25, isign, target_cb, 1.0, o);
+    break;
+  case QPHIX_GPU_TM: {  // include/qphix/twisted_mass.h:62-77
+    double alpha = 4.0 + p.mass;
+    dslash_core(p, tmp, in, op->gauge, nullptr, nullptr, isign, other);
+    achi_core(p, res, tmp, in, op->gauge, nullptr, alpha, 0.25, isign, target_cb, 1.0, o);
+    break;
+  }
+  case QPHIX_GPU_TMCLOVER:  // include/qphix/twisted_mass_clover.h:92-102
+    dslash_core(p, tmp, in, op->gauge, op->finv0, op->finv1, isign, other);
+    achi_core(p, res, tmp, in, op->gauge, op->clov, 0.0, 0.25, isign, target_cb, 1.0, o);
+    break;
+  default:
+    throw Error(QPHIX_GPU_EINVAL, "bad operator kind");
+  }
+}
+
+extern "C" int qphix_gpu_eo_op_apply(qphix_gpu_eo_op op, qphix_gpu_field res, qphix_gpu_field in, int isign,
+                                     int target_cb)
+{
+  return guard([&] {
+    QPX_REQUIRE(op, "null operator");
+    eo_apply(op, res, in, isign, target_cb, ApplyOpts());
+  });
+}
+
+// ===========================================================================
+// BLAS
+// ===========================================================================
+static Coef cval(double re, double im = 0.0) { return Coef{re, im, nullptr, nullptr}; }
+static Coef cslot(SolverState *st, int slot_re, int slot_im = -1)
+{
+  return Coef{0, 0, st->v[slot_re], slot_im >= 0 ? st->v[slot_im] : nullptr};
+}
+
+struct BlasCall {
+  int op;
+  const qphix_gpu_field_s *x = nullptr, *y = nullptr, *z = nullptr, *w = nullptr, *v = nullptr;
+  Coef a{0, 0, nullptr, nullptr}, b{0, 0, nullptr, nullptr};
+  int slots = 0;  // reduction slot set
+  int fin = FIN_NONE;
+  SolverState *state = nullptr;
+};
+
+static void blas_launch(qphix_gpu_lattice_s *lat, int prec, int nrhs, const BlasCall &c)
+{
+  BlasArgs a;
+  memset(&a, 0, sizeof(a));
+  a.op = c.op;
+  a.vh = (int)lat->vh;
+  a.nrhs = nrhs;
+  if (c.x) a.x = c.x->sarg();
+  if (c.y) a.y = c.y->sarg();
+  if (c.z) a.z = c.z->sarg();
+  if (c.w) a.w = c.w->sarg();
+  if (c.v) a.v = c.v->sarg();
+  a.a = c.a;
+  a.b = c.b;
+  a.state = c.state;
+  if (c.slots) {
+    a.red.mask = c.slots;
+    a.red.nval = __builtin_popcount(c.slots);
+    a.red.fin = c.fin;
+    a.red.partials = lat->partials;
+    a.red.ticket = lat->ticket;
+    a.red.result = lat->result;
+  }
+  launch_blas(prec, a, dim3(nblocks_for(lat->vh), nrhs), lat->stream);
+  check_launch();
+}
+
+// fetch the last reduction result (nrhs x nval) to the host
+static const double *fetch_result(qphix_gpu_lattice_s *lat, int nrhs, int nval)
+{
+  QPX_CUDA(cudaMemcpyAsync(lat->h_result, lat->result, sizeof(double) * nrhs * nval, cudaMemcpyDeviceToHost,
+                           lat->stream));
+  QPX_CUDA(cudaStreamSynchronize(lat->stream));
+  return lat->h_result;
+}
+
+static std::vector<double> norm2_host(const qphix_gpu_field_s *x)
+{
+  BlasCall c;
+  c.op = B_NORM2;
+  c.x = x;
+  c.slots = 0x1;
+  c.fin = FIN_NONE;
+  blas_launch(x->lat, x->prec, x->nrhs, c);
+  const double *r = fetch_result(x->lat, x->nrhs, 1);
+  return std::vector<double>(r, r + x->nrhs);
+}
+
+extern "C" int qphix_gpu_blas_norm2(qphix_gpu_field x, double *out)
+{
+  return guard([&] {
+    require_spinor(x, "x");
+    QPX_REQUIRE(out, "null out");
+    auto v = norm2_host(x);
+    for (int r = 0; r < x->nrhs; r++) out[r] = v[r];
+  });
+}
+
+extern "C" int qphix_gpu_blas_inner_product(qphix_gpu_field x, qphix_gpu_field y, double *out)
+{
+  return guard([&] {
+    require_spinor(x, "x");
+    require_spinor(y, "y");
+    require_same(x, y);
+    QPX_REQUIRE(out, "null out");
+    BlasCall c;
+    c.op = B_DOT;
+    c.x = x;
+    c.y = y;
+    c.slots = 0x3;
+    blas_launch(x->lat, x->prec, x->nrhs, c);
+    const double *r = fetch_result(x->lat, x->nrhs, 2);
+    for (int i = 0; i < 2 * x->nrhs; i++) out[i] = r[i];
+  });
+}
+
+extern "C" int qphix_gpu_blas_caxpby(const double a[2], qphix_gpu_field x, const double b[2], qphix_gpu_field y)
+{
+  return guard([&] {
+    require_spinor(x, "x");
+    require_spinor(y, "y");
+    require_same(x, y);
+    QPX_REQUIRE(a && b, "null coefficient");
+    BlasCall c;
+    c.op = B_CAXPBY;
+    c.x = x;
+    c.y = y;
+    c.a = cval(a[0], a[1]);
+    c.b = cval(b[0], b[1]);
+    blas_launch(x->lat, x->prec, x->nrhs, c);
+  });
+}
+
+extern "C" int qphix_gpu_blas_copy(qphix_gpu_field dst, qphix_gpu_field src)
+{
+  return guard([&] {
+    require_spinor(dst, "dst");
+    require_spinor(src, "src");
+    QPX_REQUIRE(dst->nrhs == src->nrhs && dst->lat == src->lat, "shape mismatch");
+    if (dst->prec == src->prec) {
+      BlasCall c;
+      c.op = B_COPY;
+      c.x = src;
+      c.y = dst;
+      blas_launch(src->lat, src->prec, src->nrhs, c);
+    } else {
+      convert_field(dst, src, cval(1.0), nullptr);
+    }
+  });
+}
+
+extern "C" int qphix_gpu_blas_zero(qphix_gpu_field x)
+{
+  return guard([&] {
+    require_spinor(x, "x");
+    BlasCall c;
+    c.op = B_ZERO;
+    c.x = x;
+    blas_launch(x->lat, x->prec, x->nrhs, c);
+  });
+}
+
+// ===========================================================================
+// solvers
+// ===========================================================================
+namespace {
+
+struct Tmp {  // scoped temporary spinor
+  qphix_gpu_field f = nullptr;
+  Tmp(qphix_gpu_lattice_s *lat, int prec, int nrhs)
+  {
+    int rc = qphix_gpu_field_create(lat, QPHIX_GPU_SPINOR, prec, 0, nrhs, &f);
+    if (rc) throw Error(rc, g_last_error);
+  }
+  ~Tmp() { qphix_gpu_field_destroy(f); }
+  operator qphix_gpu_field_s *() const { return f; }
+};
+
+// push the host copy of the solver state to the device
+void state_upload(qphix_gpu_lattice_s *lat)
+{
+  QPX_CUDA(cudaMemcpyAsync(lat->state, lat->h_state, sizeof(SolverState), cudaMemcpyHostToDevice, lat->stream));
+  QPX_CUDA(cudaStreamSynchronize(lat->stream));
+}
+
+void state_download(qphix_gpu_lattice_s *lat)
+{
+  QPX_CUDA(cudaMemcpyAsync(lat->h_state, lat->state, sizeof(SolverState), cudaMemcpyDeviceToHost, lat->stream));
+  QPX_CUDA(cudaStreamSynchronize(lat->stream));
+}
+
+SolverState &state_reset(qphix_gpu_lattice_s *lat, int nrhs, int max_iter)
+{
+  SolverState &s = *lat->h_state;
+  memset(&s, 0, sizeof(SolverState));
+  s.nrhs = nrhs;
+  s.max_iter = max_iter;
+  return s;
+}
+
+// Replays `step` (one solver iteration, kernels only) until the device raises
+// state->done.  The step is captured once into a CUDA graph.
+template <typename Step>
+void run_iterations(qphix_gpu_lattice_s *lat, Step &&step, int max_iter)
+{
+  const int check = 8;
+  bool use_graph = !env_flag("QPHIX_GPU_NO_GRAPH");
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long nodes = 0;
+  if (use_graph) {
+    cudaGraph_t graph = nullptr;
+    unsigned long long before = g_launches.load();
+    QPX_CUDA(cudaStreamBeginCapture(lat->stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      step();
+    } catch (...) {
+      cudaStreamEndCapture(lat->stream, &graph);
+      if (graph) cudaGraphDestroy(graph);
+      throw;
+    }
+    QPX_CUDA(cudaStreamEndCapture(lat->stream, &graph));
+    nodes = g_launches.load() - before;  // captured, not run: counted per replay below
+    g_launches -= nodes;
+    cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) throw Error(QPHIX_GPU_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  int launched = 0;
+  try {
+    while (true) {
+      for (int i = 0; i < check; i++) {
+        if (use_graph) {
+          QPX_CUDA(cudaGraphLaunch(exec, lat->stream));
+          g_launches += nodes;
+        } else
+          step();
+        launched++;
+      }
+      QPX_CUDA(cudaMemcpyAsync(&lat->h_state->done, &lat->state->done, sizeof(int), cudaMemcpyDeviceToHost,
+                               lat->stream));
+      QPX_CUDA(cudaStreamSynchronize(lat->stream));
+      if (lat->h_state->done) break;
+      if (launched > max_iter + 2 * check) break;  // the device enforces max_iter; belt and braces
+    }
+  } catch (...) {
+    if (exec) cudaGraphExecDestroy(exec);
+    throw;
+  }
+  if (exec) QPX_CUDA(cudaGraphExecDestroy(exec));
+  state_download(lat);
+}
+
+double elapsed(cudaEvent_t a, cudaEvent_t b)
+{
+  float ms = 0;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms * 1e-3;
+}
+
+struct Timer {
+  cudaEvent_t t0, t1;
+  qphix_gpu_lattice_s *lat;
+  explicit Timer(qphix_gpu_lattice_s *l) : lat(l)
+  {
+    cudaEventCreate(&t0);
+    cudaEventCreate(&t1);
+    cudaEventRecord(t0, lat->stream);
+  }
+  double stop()
+  {
+    cudaEventRecord(t1, lat->stream);
+    cudaEventSynchronize(t1);
+    return elapsed(t0, t1);
+  }
+  ~Timer()
+  {
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+  }
+};
+
+void check_solver_fields(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs)
+{
+  QPX_REQUIRE(op, "null operator");
+  require_spinor(x, "x");
+  require_spinor(rhs, "rhs");
+  require_same(x, rhs);
+  require_same(x, op->gauge);
+  QPX_REQUIRE(x->nrhs == rhs->nrhs, "rhs count mismatch");
+}
+
+// true residual |b - M x|^2 per rhs (and relative), t: scratch
+void true_residual(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs, qphix_gpu_field_s *t,
+                   qphix_gpu_field_s *r, int isign, int cb, bool normal_eq, const std::vector<double> &bnorm,
+                   std::vector<double> &abs2, std::vector<double> &rel)
+{
+  if (normal_eq) {
+    eo_apply(op, r, x, isign, cb, ApplyOpts());
+    eo_apply(op, t, r, -isign, cb, ApplyOpts());
+  } else {
+    eo_apply(op, t, x, isign, cb, ApplyOpts());
+  }
+  BlasCall c;
+  c.op = B_XMY_NORM;
+  c.x = rhs;
+  c.y = t;
+  c.z = r;
+  c.slots = 0x1;
+  blas_launch(x->lat, x->prec, x->nrhs, c);
+  const double *h = fetch_result(x->lat, x->nrhs, 1);
+  abs2.assign(h, h + x->nrhs);
+  rel.resize(x->nrhs);
+  for (int i = 0; i < x->nrhs; i++) rel[i] = bnorm[i] > 0 ? std::sqrt(abs2[i] / bnorm[i]) : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// CG on M^dag M (include/qphix/invcg.h:88-456)
+void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs, const double *rsd,
+              int max_iters, int isign, int cb, qphix_gpu_solve_info *info)
+{
+  check_solver_fields(op, x, rhs);
+  auto *lat = x->lat;
+  const int nr = x->nrhs, prec = x->prec;
+  Timer timer(lat);
+  Tmp mp(lat, prec, nr), mmp(lat, prec, nr), r(lat, prec, nr), p(lat, prec, nr);
+  std::vector<double> chi = norm2_host(rhs);
+  eo_apply(op, mp, x, isign, cb, ApplyOpts());
+  eo_apply(op, mmp, mp, -isign, cb, ApplyOpts());
+  BlasCall c;
+  c.op = B_XMY_NORM;
+  c.x = rhs;
+  c.y = mmp;
+  c.z = r;
+  c.slots = 0x1;
+  blas_launch(lat, prec, nr, c);
+  const double *h = fetch_result(lat, nr, 1);
+  std::vector<double> cp(h, h + nr);
+  SolverState &S = state_reset(lat, nr, max_iters + 1);
+  bool all = true;
+  for (int i = 0; i < nr; i++) {
+    S.v[S_RSD][i] = rsd[i] * rsd[i] * chi[i];
+    S.v[S_C][i] = cp[i];
+    S.v[S_RNORM][i] = cp[i];
+    if (cp[i] <= S.v[S_RSD][i]) {
+      S.rhs_done[i] = 1;
+      S.rhs_iter[i] = 0;
+    }
+    all = all && S.rhs_done[i];
+  }
+  S.done = all ? 1 : 0;
+  state_upload(lat);
+  SolverState *ds = lat->state;
+  unsigned long mv = 2;
+  if (!all) {
+    BlasCall cpy;
+    cpy.op = B_COPY;
+    cpy.x = r;
+    cpy.y = p;
+    blas_launch(lat, prec, nr, cpy);
+    auto step = [&] {
+      ApplyOpts o1;
+      o1.red_mask = RED_NORM_OUT;
+      o1.fin = FIN_CG_A;
+      o1.state = ds;
+      eo_apply(op, mp, p, isign, cb, o1);
+      ApplyOpts o2;
+      o2.post = POST_CG;
+      o2.red_mask = RED_NORM_R;
+      o2.fin = FIN_CG_R;
+      o2.state = ds;
+      o2.r = r;
+      o2.x = x;
+      o2.p = p;
+      eo_apply(op, mmp, mp, -isign, cb, o2);
+      BlasCall pu;
+      pu.op = B_CG_P;
+      pu.x = r;
+      pu.y = p;
+      pu.a = cslot(ds, S_B);
+      pu.state = ds;
+      blas_launch(lat, prec, nr, pu);
+    };
+    run_iterations(lat, step, max_iters + 1);
+    mv += 2ul * lat->h_state->iter;
+  }
+  std::vector<double> abs2, rel;
+  true_residual(op, x, rhs, mmp, r, isign, cb, true, chi, abs2, rel);
+  mv += 2;
+  const SolverState &H = *lat->h_state;
+  double secs = timer.stop();
+  for (int i = 0; i < nr; i++) {
+    info[i].n_iters = H.rhs_done[i] ? H.rhs_iter[i] : max_iters;
+    info[i].rsd_sq_final = abs2[i];
+    info[i].mv_apps = mv;
+    info[i].site_flops = (unsigned long)(4 * 12 + 6 * 12 + H.iter * (4 * 12 + 12 * 12 + 4 * 12) + 6 * 12);
+    info[i].status = H.rhs_done[i] == 2 ? 2 : (H.rhs_done[i] ? 0 : 1);
+    info[i].true_rel_resid = rel[i];
+    info[i].seconds = secs;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// BiCGStab (include/qphix/invbicgstab.h:80-263)
+void solve_bicgstab(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs, const double *rsd,
+                    int max_iters, int isign, int cb, qphix_gpu_solve_info *info)
+{
+  check_solver_fields(op, x, rhs);
+  auto *lat = x->lat;
+  const int nr = x->nrhs, prec = x->prec;
+  Timer timer(lat);
+  Tmp r0(lat, prec, nr), r(lat, prec, nr), p(lat, prec, nr), v(lat, prec, nr), t(lat, prec, nr);
+  std::vector<double> bn = norm2_host(rhs);
+  eo_apply(op, r0, x, isign, cb, ApplyOpts());
+  BlasCall c;
+  c.op = B_XMY_NORM;
+  c.x = rhs;
+  c.y = r0;
+  c.z = r0;
+  c.slots = 0x1;
+  blas_launch(lat, prec, nr, c);
+  const double *h = fetch_result(lat, nr, 1);
+  std::vector<double> rn(h, h + nr);
+  SolverState &S = state_reset(lat, nr, max_iters);
+  bool all = true;
+  for (int i = 0; i < nr; i++) {
+    S.v[S_RSD][i] = rsd[i] * rsd[i] * bn[i];
+    S.v[S_RNORM][i] = rn[i];
+    S.v[S_RHO_RE][i] = rn[i];  // rho_1 = <r0, r> with r = r0
+    S.v[S_RHOP_RE][i] = 1.0;
+    S.v[S_ALPHA_RE][i] = 1.0;
+    S.v[S_OMEGA_RE][i] = 1.0;
+    S.v[S_BETA_RE][i] = rn[i];  // (rho / 1) (1 / 1)
+    if (rn[i] < S.v[S_RSD][i] || bn[i] == 0.0) {
+      S.rhs_done[i] = 1;
+      S.rhs_iter[i] = -1;  // reported as 0
+      S.v[S_BETA_RE][i] = 0;
+      S.v[S_ALPHA_RE][i] = 0;
+      S.v[S_OMEGA_RE][i] = 0;
+    }
+    all = all && S.rhs_done[i];
+  }
+  S.done = all ? 1 : 0;
+  state_upload(lat);
+  SolverState *ds = lat->state;
+  unsigned long mv = 1;
+  if (!all) {
+    BlasCall cpy;
+    cpy.op = B_COPY;
+    cpy.x = r0;
+    cpy.y = r;
+    blas_launch(lat, prec, nr, cpy);
+    BlasCall z;
+    z.op = B_ZERO;
+    z.x = p;
+    blas_launch(lat, prec, nr, z);
+    z.x = v;
+    blas_launch(lat, prec, nr, z);
+    auto step = [&] {
+      BlasCall pu;
+      pu.op = B_BICG_P;
+      pu.x = r;
+      pu.y = p;
+      pu.z = v;
+      pu.a = cslot(ds, S_BETA_RE, S_BETA_IM);
+      pu.b = cslot(ds, S_OMEGA_RE, S_OMEGA_IM);
+      pu.state = ds;
+      blas_launch(lat, prec, nr, pu);
+      ApplyOpts o1;
+      o1.red_mask = RED_DOT_W_OUT;
+      o1.fin = FIN_BICG_ALPHA;
+      o1.state = ds;
+      o1.w = r0;
+      eo_apply(op, v, p, isign, cb, o1);
+      BlasCall su;
+      su.op = B_BICG_S;
+      su.x = r;
+      su.y = v;
+      su.a = cslot(ds, S_ALPHA_RE, S_ALPHA_IM);
+      su.state = ds;
+      blas_launch(lat, prec, nr, su);
+      ApplyOpts o2;
+      o2.red_mask = RED_NORM_OUT | RED_DOT_OUT_CHI;
+      o2.fin = FIN_BICG_OMEGA;
+      o2.state = ds;
+      eo_apply(op, t, r, isign, cb, o2);
+      BlasCall rx;
+      rx.op = B_BICG_RX;
+      rx.x = x;
+      rx.y = r;
+      rx.z = t;
+      rx.v = p;
+      rx.w = r0;
+      rx.a = cslot(ds, S_OMEGA_RE, S_OMEGA_IM);
+      rx.b = cslot(ds, S_ALPHA_RE, S_ALPHA_IM);
+      rx.slots = 0x7;
+      rx.fin = FIN_BICG_RX;
+      rx.state = ds;
+      blas_launch(lat, prec, nr, rx);
+    };
+    run_iterations(lat, step, max_iters);
+    mv += 2ul * lat->h_state->iter;
+  }
+  std::vector<double> abs2, rel;
+  true_residual(op, x, rhs, t, r, isign, cb, false, bn, abs2, rel);
+  const SolverState &H = *lat->h_state;
+  double secs = timer.stop();
+  for (int i = 0; i < nr; i++) {
+    // the reference reports its loop counter after the final increment
+    info[i].n_iters = H.rhs_done[i] ? H.rhs_iter[i] + 1 : max_iters + 1;
+    if (H.rhs_done[i] == 2) info[i].n_iters = H.rhs_iter[i];
+    info[i].rsd_sq_final = H.v[S_RNORM][i];
+    info[i].mv_apps = mv;
+    info[i].site_flops = (unsigned long)(4 * 12 + 24 + H.iter * (8 * 12 + 16 * 12 + 8 * 12 + 8 * 12 + 4 * 12 +
+                                                                  8 * 12 + 28 * 12));
+    info[i].status = H.rhs_done[i] == 2 ? 2 : (H.rhs_done[i] ? 0 : 1);
+    info[i].true_rel_resid = rel[i];
+    info[i].seconds = secs;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// MR (include/qphix/invmr.h:62-210), terminating on the relative residual
+void solve_mr(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs, const double *rsd, int max_iters,
+              double omega, int isign, int cb, qphix_gpu_solve_info *info)
+{
+  check_solver_fields(op, x, rhs);
+  auto *lat = x->lat;
+  const int nr = x->nrhs, prec = x->prec;
+  Timer timer(lat);
+  if (max_iters == 0) {
+    for (int i = 0; i < nr; i++) {
+      info[i] = qphix_gpu_solve_info{};
+      info[i].rsd_sq_final = -1;
+    }
+    return;
+  }
+  Tmp r(lat, prec, nr), Mr(lat, prec, nr);
+  std::vector<double> bn = norm2_host(rhs);
+  eo_apply(op, r, x, isign, cb, ApplyOpts());
+  BlasCall c;
+  c.op = B_XMY_NORM;
+  c.x = rhs;
+  c.y = r;
+  c.z = r;
+  c.slots = 0x1;
+  blas_launch(lat, prec, nr, c);
+  const double *h = fetch_result(lat, nr, 1);
+  std::vector<double> cp(h, h + nr);
+  SolverState &S = state_reset(lat, nr, max_iters);
+  bool all = true;
+  for (int i = 0; i < nr; i++) {
+    S.v[S_RSD][i] = rsd[i] * rsd[i] * bn[i];
+    S.v[S_RNORM][i] = cp[i];
+    S.v[S_AUX0][i] = omega;
+    if (cp[i] < S.v[S_RSD][i] || bn[i] == 0.0) {
+      S.rhs_done[i] = 1;
+      S.rhs_iter[i] = 0;
+    }
+    all = all && S.rhs_done[i];
+  }
+  S.done = all ? 1 : 0;
+  state_upload(lat);
+  SolverState *ds = lat->state;
+  unsigned long mv = 1;
+  if (!all) {
+    auto step = [&] {
+      ApplyOpts o;
+      o.red_mask = RED_NORM_OUT | RED_DOT_OUT_CHI;
+      o.fin = FIN_MR_A;
+      o.state = ds;
+      eo_apply(op, Mr, r, isign, cb, o);
+      BlasCall u;
+      u.op = B_MR_RX;
+      u.x = x;
+      u.y = r;
+      u.z = Mr;
+      u.a = cslot(ds, S_ALPHA_RE, S_ALPHA_IM);
+      u.slots = 0x1;
+      u.fin = FIN_MR_R;
+      u.state = ds;
+      blas_launch(lat, prec, nr, u);
+    };
+    run_iterations(lat, step, max_iters);
+    mv += lat->h_state->iter;
+  }
+  std::vector<double> abs2, rel;
+  Tmp t(lat, prec, nr), rr(lat, prec, nr);
+  true_residual(op, x, rhs, t, rr, isign, cb, false, bn, abs2, rel);
+  const SolverState &H = *lat->h_state;
+  double secs = timer.stop();
+  for (int i = 0; i < nr; i++) {
+    info[i].n_iters = H.rhs_done[i] ? H.rhs_iter[i] : H.iter;
+    info[i].rsd_sq_final = H.v[S_RNORM][i] / bn[i];
+    info[i].mv_apps = mv;
+    info[i].site_flops = (unsigned long)(24 + 8 * 12 + H.iter * (12 * 12 + 2 * 8 * 12 + 4 * 12));
+    info[i].status = H.rhs_done[i] ? 0 : 1;
+    info[i].true_rel_resid = rel[i];
+    info[i].seconds = secs;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Richardson defect correction (include/qphix/inv_richardson_multiprec.h:42-239)
+void solve_richardson(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opi, int inner, qphix_gpu_field_s *x,
+                      qphix_gpu_field_s *rhs, double rsd, double delta, int max_iters, int inner_max, int isign,
+                      int cb, qphix_gpu_solve_info *info)
+{
+  check_solver_fields(op, x, rhs);
+  QPX_REQUIRE(opi && opi->gauge->lat == x->lat, "inner operator must live on the same lattice");
+  auto *lat = x->lat;
+  const int nr = x->nrhs, prec = x->prec, iprec = opi->gauge->prec;
+  Timer timer(lat);
+  Tmp r(lat, prec, nr), tmp(lat, prec, nr), dx(lat, prec, nr);
+  Tmp rin(lat, iprec, nr), dxin(lat, iprec, nr);
+  std::vector<double> bn = norm2_host(rhs);
+  std::vector<double> rsd_t(nr);
+  for (int i = 0; i < nr; i++) rsd_t[i] = rsd * rsd * bn[i];
+  eo_apply(op, tmp, x, isign, cb, ApplyOpts());
+  BlasCall c;
+  c.op = B_XMY_NORM;
+  c.x = rhs;
+  c.y = tmp;
+  c.z = r;
+  c.slots = 0x1;
+  blas_launch(lat, prec, nr, c);
+  const double *h = fetch_result(lat, nr, 1);
+  std::vector<double> rn(h, h + nr);
+  unsigned long mv_outer = 1, mv_inner = 0;
+  std::vector<int> done(nr, 0);
+  bool all = true;
+  for (int i = 0; i < nr; i++) {
+    done[i] = rn[i] < rsd_t[i] || bn[i] == 0.0;
+    all = all && done[i];
+  }
+  int iter = 0;
+  // per-rhs scale factors live in the state's AUX slots between inner solves
+  std::vector<double> scale_dn(nr), scale_up(nr), inner_rsd(nr);
+  double *d_scales = nullptr;
+  QPX_CUDA(cudaMalloc(&d_scales, sizeof(double) * 2 * QPX_MAX_RHS));
+  std::vector<qphix_gpu_solve_info> ii(nr);
+  try {
+    if (!all) {
+      for (iter = 1; iter < max_iters; iter++) {
+        for (int i = 0; i < nr; i++) {
+          double dfin = std::sqrt(rsd_t[i] / rn[i]);
+          inner_rsd[i] = done[i] ? 1.0 : (dfin > delta ? dfin : delta);
+          double rnorm = std::sqrt(rn[i]);
+          scale_dn[i] = done[i] ? 0.0 : 1.0 / rnorm;
+          scale_up[i] = done[i] ? 0.0 : rnorm;
+        }
+        std::vector<double> sc(2 * QPX_MAX_RHS, 0.0);
+        for (int i = 0; i < nr; i++) {
+          sc[i] = scale_dn[i];
+          sc[QPX_MAX_RHS + i] = scale_up[i];
+        }
+        QPX_CUDA(cudaMemcpyAsync(d_scales, sc.data(), sizeof(double) * 2 * QPX_MAX_RHS, cudaMemcpyHostToDevice,
+                                 lat->stream));
+        convert_field(rin, r, Coef{0, 0, d_scales, nullptr}, nullptr);
+        BlasCall z;
+        z.op = B_ZERO;
+        z.x = dxin;
+        blas_launch(lat, iprec, nr, z);
+        if (inner == QPHIX_GPU_SOLVER_BICGSTAB)
+          solve_bicgstab(opi, dxin, rin, inner_rsd.data(), inner_max, isign, cb, ii.data());
+        else if (inner == QPHIX_GPU_SOLVER_MR)
+          solve_mr(opi, dxin, rin, inner_rsd.data(), inner_max, 1.0, isign, cb, ii.data());
+        else
+          solve_cg(opi, dxin, rin, inner_rsd.data(), inner_max, isign, cb, ii.data());
+        mv_inner += ii[0].mv_apps;
+        convert_field(dx, dxin, Coef{0, 0, d_scales + QPX_MAX_RHS, nullptr}, nullptr);
+        eo_apply(op, tmp, dx, isign, cb, ApplyOpts());
+        mv_outer++;
+        BlasCall u;
+        u.op = B_RICH_RX;
+        u.x = x;
+        u.y = r;
+        u.z = dx;
+        u.w = tmp;
+        u.slots = 0x1;
+        blas_launch(lat, prec, nr, u);
+        h = fetch_result(lat, nr, 1);
+        all = true;
+        for (int i = 0; i < nr; i++) {
+          rn[i] = h[i];
+          if (!done[i] && rn[i] < rsd_t[i]) done[i] = 1;
+          all = all && done[i];
+        }
+        if (all) break;
+      }
+    }
+  } catch (...) {
+    cudaFree(d_scales);
+    throw;
+  }
+  cudaFree(d_scales);
+  std::vector<double> abs2, rel;
+  true_residual(op, x, rhs, tmp, r, isign, cb, false, bn, abs2, rel);
+  mv_outer++;
+  double secs = timer.stop();
+  for (int i = 0; i < nr; i++) {
+    info[i].n_iters = iter;
+    info[i].rsd_sq_final = bn[i] > 0 ? abs2[i] / bn[i] : 0.0;  // relative, as the reference reports
+    info[i].mv_apps = mv_outer + mv_inner;
+    info[i].site_flops = 0;
+    info[i].status = done[i] ? 0 : 1;
+    info[i].true_rel_resid = rel[i];
+    info[i].seconds = secs;
+  }
+}
+
+}  // namespace
+
+static int solve_status(const qphix_gpu_solve_info *info, int n)
+{
+  for (int i = 0; i < n; i++)
+    if (info[i].status == 2) return QPHIX_GPU_EBREAKDOWN;
+  for (int i = 0; i < n; i++)
+    if (info[i].status == 1) return QPHIX_GPU_ENOTCONV;
+  return QPHIX_GPU_OK;
+}
+
+#define QPX_SOLVE_ENTRY(body)                                               \
+  int rc = guard([&] { body; });                                            \
+  if (rc) return rc;                                                        \
+  int st_ = solve_status(info, x->nrhs);                                    \
+  if (st_) g_last_error = st_ == QPHIX_GPU_ENOTCONV ? "solver did not converge" : "solver breakdown"; \
+  return st_;
+
+extern "C" int qphix_gpu_solve_cg(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target,
+                                  int max_iters, int isign, int cb, qphix_gpu_solve_info *info)
+{
+  QPX_SOLVE_ENTRY({
+    QPX_REQUIRE(info && x, "null argument");
+    std::vector<double> rs(x->nrhs, rsd_target);
+    solve_cg(op, x, rhs, rs.data(), max_iters, isign, cb, info);
+  })
+}
+
+extern "C" int qphix_gpu_solve_bicgstab(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs,
+                                        double rsd_target, int max_iters, int isign, int cb,
+                                        qphix_gpu_solve_info *info)
+{
+  QPX_SOLVE_ENTRY({
+    QPX_REQUIRE(info && x, "null argument");
+    std::vector<double> rs(x->nrhs, rsd_target);
+    solve_bicgstab(op, x, rhs, rs.data(), max_iters, isign, cb, info);
+  })
+}
+
+extern "C" int qphix_gpu_solve_mr(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target,
+                                  int max_iters, double omega, int isign, int cb, qphix_gpu_solve_info *info)
+{
+  QPX_SOLVE_ENTRY({
+    QPX_REQUIRE(info && x, "null argument");
+    std::vector<double> rs(x->nrhs, rsd_target);
+    solve_mr(op, x, rhs, rs.data(), max_iters, omega, isign, cb, info);
+  })
+}
+
+extern "C" int qphix_gpu_solve_richardson(qphix_gpu_eo_op op_outer, qphix_gpu_eo_op op_inner, int inner_solver,
+                                          qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target, double delta,
+                                          int max_iters, int inner_max_iters, int isign, int cb,
+                                          qphix_gpu_solve_info *info)
+{
+  QPX_SOLVE_ENTRY({
+    QPX_REQUIRE(info && x, "null argument");
+    solve_richardson(op_outer, op_inner, inner_solver, x, rhs, rsd_target, delta, max_iters, inner_max_iters,
+                     isign, cb, info);
+  })
+}
+
+extern "C" int qphix_gpu_solve_mshift_cg(qphix_gpu_eo_op op, qphix_gpu_field *x, qphix_gpu_field rhs, int n_shift,
+                                         const double *shifts, const double *rsd_target, int max_iters, int isign,
+                                         int cb, int *n_iters, double *rsd_sq_final, unsigned long *mv_apps)
+{
+  (void)op; (void)x; (void)rhs; (void)n_shift; (void)shifts; (void)rsd_target; (void)max_iters; (void)isign;
+  (void)cb; (void)n_iters; (void)rsd_sq_final; (void)mv_apps;
+  g_last_error = "multishift CG is not built yet";
+  return QPHIX_GPU_EUNSUPPORTED;
+}

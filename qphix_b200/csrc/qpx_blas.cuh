@@ -1,0 +1,268 @@
+// Streaming BLAS over checkerboarded spinor fields, each fused the way the
+// reference fuses it (include/qphix/blas_new_c.h, real_functors.h,
+// complex_functors.h): one pass over the vectors, arithmetic in the field's
+// compute type, reductions accumulated in FP64 and folded deterministically
+// by reduce_epilogue.  Coefficients come either from the launch (host values)
+// or from a SolverState slot (device-resident Krylov scalars), per rhs.
+#pragma once
+
+#include "qpx_common.cuh"
+#include "qpx_reduce.cuh"
+
+namespace qpx {
+
+// complex coefficient: state slot pointers (per rhs) if set, else the value
+struct Coef {
+  double re, im;
+  const double *pre, *pim;
+  __device__ __forceinline__ double r(int rhs) const { return pre ? pre[rhs] : re; }
+  __device__ __forceinline__ double i(int rhs) const { return pim ? pim[rhs] : im; }
+};
+
+enum BlasOp : int {
+  B_NORM2 = 0,     // red: |x|^2
+  B_DOT,           // red: <x, y>
+  B_DOTNORM,       // red: <x, y>, |x|^2           (innerProductNorm)
+  B_COPY,          // y = x
+  B_ZERO,          // x = 0
+  B_CAXPBY,        // y = a x + b y                (ax, axy, axpy, axpby, aypx, caxpy)
+  B_CAXPBY_NORM,   // y = a x + b y, red |y|^2     (axpyNorm2)
+  B_XMY_NORM,      // z = x - y, red |z|^2          (xmyNorm2Spinor)
+  B_BICG_P,        // p = r + beta (p - omega v)    (bicgstab_p_update)
+  B_BICG_S,        // r = r - alpha v               (bicgstab_s_update)
+  B_BICG_RX,       // x += omega r + alpha p ; r -= omega t ; red |r|^2, <w, r>
+  B_CG_P,          // p = r + b p                   (aypx with device b)
+  B_MR_RX,         // x += a r ; r -= a Mr ; red |r|^2
+  B_RICH_RX,       // x += dx ; r -= t ; red |r|^2  (richardson_rxupdateNormR)
+  B_G5,            // y = gamma_5 x
+};
+
+// BLAS reductions use red.mask directly as the slot set: B_NORM2 / the
+// *_NORM ops fill slot 0, B_DOT slots 0-1, B_DOTNORM / B_BICG_RX slots 0-2.
+struct BlasArgs {
+  int op;
+  int vh;
+  int nrhs;
+  SpinorArg x, y, z, w, v;  // operand roles documented per op
+  Coef a, b, c;
+  ReduceArg red;
+  SolverState *state;
+};
+
+template <typename T>
+__device__ __forceinline__ void caxpy_(T *y, double ar, double ai, const T *x)
+{
+  const T r = (T)ar, i = (T)ai;
+#pragma unroll
+  for (int k = 0; k < 24; k += 2) {
+    T xr = x[k], xi = x[k + 1];
+    y[k] += r * xr - i * xi;
+    y[k + 1] += r * xi + i * xr;
+  }
+}
+
+template <typename P>
+__global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
+{
+  using T = typename P::real;
+  using IO = SpinorIO<P>;
+  if (a.state && a.state->done) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  double red[1][QPX_MAX_RED];
+#pragma unroll
+  for (int k = 0; k < QPX_MAX_RED; k++) red[0][k] = 0;
+  if (s < a.vh) {
+    T x[24], y[24];
+    switch (a.op) {
+    case B_NORM2: {
+      IO::load(a.x, rhs, s, x);
+      double n = 0;
+#pragma unroll
+      for (int k = 0; k < 24; k++) n += (double)x[k] * x[k];
+      red[0][0] = n;
+      break;
+    }
+    case B_DOT:
+    case B_DOTNORM: {
+      IO::load(a.x, rhs, s, x);
+      IO::load(a.y, rhs, s, y);
+      double re = 0, im = 0, n = 0;
+#pragma unroll
+      for (int k = 0; k < 24; k += 2) {
+        re += (double)x[k] * y[k] + (double)x[k + 1] * y[k + 1];
+        im += (double)x[k] * y[k + 1] - (double)x[k + 1] * y[k];
+        n += (double)x[k] * x[k] + (double)x[k + 1] * x[k + 1];
+      }
+      red[0][0] = re;
+      red[0][1] = im;
+      red[0][2] = n;
+      break;
+    }
+    case B_COPY:
+      IO::load(a.x, rhs, s, x);
+      IO::store(a.y, rhs, s, x);
+      break;
+    case B_ZERO:
+#pragma unroll
+      for (int k = 0; k < 24; k++) x[k] = 0;
+      IO::store(a.x, rhs, s, x);
+      break;
+    case B_CAXPBY:
+    case B_CAXPBY_NORM: {
+      IO::load(a.x, rhs, s, x);
+      IO::load(a.y, rhs, s, y);
+      const T ar = (T)a.a.r(rhs), ai = (T)a.a.i(rhs), br = (T)a.b.r(rhs), bi = (T)a.b.i(rhs);
+      double n = 0;
+#pragma unroll
+      for (int k = 0; k < 24; k += 2) {
+        T yr = ar * x[k] - ai * x[k + 1] + br * y[k] - bi * y[k + 1];
+        T yi = ar * x[k + 1] + ai * x[k] + br * y[k + 1] + bi * y[k];
+        y[k] = yr;
+        y[k + 1] = yi;
+        n += (double)yr * yr + (double)yi * yi;
+      }
+      IO::store(a.y, rhs, s, y);
+      red[0][0] = n;
+      break;
+    }
+    case B_XMY_NORM: {
+      IO::load(a.x, rhs, s, x);
+      IO::load(a.y, rhs, s, y);
+      double n = 0;
+#pragma unroll
+      for (int k = 0; k < 24; k++) {
+        x[k] -= y[k];
+        n += (double)x[k] * x[k];
+      }
+      IO::store(a.z, rhs, s, x);
+      red[0][0] = n;
+      break;
+    }
+    case B_BICG_P: {  // x = r, y = p, z = v ; a = beta, b = omega
+      T v[24];
+      IO::load(a.x, rhs, s, x);
+      IO::load(a.y, rhs, s, y);
+      IO::load(a.z, rhs, s, v);
+      const T br = (T)a.a.r(rhs), bi = (T)a.a.i(rhs), orr = (T)a.b.r(rhs), oi = (T)a.b.i(rhs);
+#pragma unroll
+      for (int k = 0; k < 24; k += 2) {
+        T tr = y[k] - (orr * v[k] - oi * v[k + 1]);
+        T ti = y[k + 1] - (orr * v[k + 1] + oi * v[k]);
+        y[k] = x[k] + br * tr - bi * ti;
+        y[k + 1] = x[k + 1] + br * ti + bi * tr;
+      }
+      IO::store(a.y, rhs, s, y);
+      break;
+    }
+    case B_BICG_S: {  // x = r (in/out), y = v ; a = alpha
+      IO::load(a.x, rhs, s, x);
+      IO::load(a.y, rhs, s, y);
+      caxpy_(x, -a.a.r(rhs), -a.a.i(rhs), y);
+      IO::store(a.x, rhs, s, x);
+      break;
+    }
+    case B_BICG_RX: {  // x = x, y = r, z = t, v = p, w = r0 ; a = omega, b = alpha
+      T t[24], p[24];
+      IO::load(a.x, rhs, s, x);
+      IO::load(a.y, rhs, s, y);
+      IO::load(a.z, rhs, s, t);
+      IO::load(a.v, rhs, s, p);
+      const double orr = a.a.r(rhs), oi = a.a.i(rhs);
+      caxpy_(x, orr, oi, y);
+      caxpy_(x, a.b.r(rhs), a.b.i(rhs), p);
+      caxpy_(y, -orr, -oi, t);
+      IO::store(a.x, rhs, s, x);
+      IO::store(a.y, rhs, s, y);
+      T w[24];
+      IO::load(a.w, rhs, s, w);
+      double n = 0, re = 0, im = 0;
+#pragma unroll
+      for (int k = 0; k < 24; k += 2) {
+        n += (double)y[k] * y[k] + (double)y[k + 1] * y[k + 1];
+        re += (double)w[k] * y[k] + (double)w[k + 1] * y[k + 1];
+        im += (double)w[k] * y[k + 1] - (double)w[k + 1] * y[k];
+      }
+      red[0][0] = n;
+      red[0][1] = re;
+      red[0][2] = im;
+      break;
+    }
+    case B_CG_P: {  // x = r, y = p ; a = b
+      IO::load(a.x, rhs, s, x);
+      IO::load(a.y, rhs, s, y);
+      const T b = (T)a.a.r(rhs);
+#pragma unroll
+      for (int k = 0; k < 24; k++) y[k] = x[k] + b * y[k];
+      IO::store(a.y, rhs, s, y);
+      break;
+    }
+    case B_MR_RX: {  // x = x, y = r, z = Mr ; a = a
+      T mr[24];
+      IO::load(a.x, rhs, s, x);
+      IO::load(a.y, rhs, s, y);
+      IO::load(a.z, rhs, s, mr);
+      const double ar = a.a.r(rhs), ai = a.a.i(rhs);
+      caxpy_(x, ar, ai, y);
+      caxpy_(y, -ar, -ai, mr);
+      IO::store(a.x, rhs, s, x);
+      IO::store(a.y, rhs, s, y);
+      double n = 0;
+#pragma unroll
+      for (int k = 0; k < 24; k++) n += (double)y[k] * y[k];
+      red[0][0] = n;
+      break;
+    }
+    case B_RICH_RX: {  // x = x, y = r, z = dx, w = t
+      T dx[24], t[24];
+      IO::load(a.x, rhs, s, x);
+      IO::load(a.y, rhs, s, y);
+      IO::load(a.z, rhs, s, dx);
+      IO::load(a.w, rhs, s, t);
+      double n = 0;
+#pragma unroll
+      for (int k = 0; k < 24; k++) {
+        x[k] += dx[k];
+        y[k] -= t[k];
+        n += (double)y[k] * y[k];
+      }
+      IO::store(a.x, rhs, s, x);
+      IO::store(a.y, rhs, s, y);
+      red[0][0] = n;
+      break;
+    }
+    case B_G5: {
+      IO::load(a.x, rhs, s, x);
+#pragma unroll
+      for (int k = 12; k < 24; k++) x[k] = -x[k];
+      IO::store(a.y, rhs, s, x);
+      break;
+    }
+    default:
+      break;
+    }
+  }
+  if (a.red.mask) reduce_epilogue<1>(a.red, a.state, a.nrhs, rhs, a.red.mask, red);
+}
+
+// y (precision Q) = scale * x (precision P): the precision conversion of
+// InvRichardsonMultiPrec (blas_new_c.h:852-960), scale = 1/|r| going down
+// and |r| coming back up.  `scale` may be a per-rhs device value.
+template <typename P, typename Q>
+__global__ void __launch_bounds__(QPX_BLOCK) convert_kernel(int vh, SpinorArg x, SpinorArg y, Coef scale,
+                                                            SolverState *state)
+{
+  if (state && state->done) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rhs = blockIdx.y;
+  if (s >= vh) return;
+  typename P::real xv[24];
+  typename Q::real yv[24];
+  SpinorIO<P>::load(x, rhs, s, xv);
+  const double sc = scale.r(rhs);
+#pragma unroll
+  for (int k = 0; k < 24; k++) yv[k] = (typename Q::real)((double)xv[k] * sc);
+  SpinorIO<Q>::store(y, rhs, s, yv);
+}
+
+}  // namespace qpx

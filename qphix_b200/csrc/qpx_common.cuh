@@ -1,0 +1,479 @@
+// Device-side building blocks shared by every kernel of the library:
+// precision traits, the chunked structure-of-arrays field layouts in HBM,
+// complex helpers and the lattice geometry passed to kernels.
+//
+// Layouts (one checkerboard of Vh sites, `stride` >= Vh, a multiple of 64):
+//   spinor  [rhs][chunk][stride] of Chunk, 24 reals per site ordered
+//           (spin, colour, re/im); FP64 12 x double2, FP32 6 x float4,
+//           half / bf16 3 x 16-byte chunks (8 values) + float norm[rhs][stride]
+//   gauge   [cb][mu][chunk][stride]: U_mu(x) for x in cb, row-major (row, col,
+//           re/im); 18 reals, or 12 (rows 0 and 1; row 2 = conj(row0 x row1))
+//   clover  [chunk][stride], 72 reals = 2 blocks x (diag[6], offd[15] re/im)
+//   full    [chunk][stride], 144 reals = 2 blocks x 6 x 6 complex, row-major
+// A warp therefore reads 32 consecutive sites x 16 (or 8) bytes per chunk.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace qpx {
+
+enum Prec : int { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2, PREC_BF16 = 3 };
+
+// ---------------------------------------------------------------------------
+// complex arithmetic on plain structs (kept in registers)
+// ---------------------------------------------------------------------------
+template <typename T>
+struct cx {
+  T re, im;
+};
+
+template <typename T>
+__device__ __forceinline__ cx<T> cmake(T r, T i) { return cx<T>{r, i}; }
+template <typename T>
+__device__ __forceinline__ cx<T> operator+(cx<T> a, cx<T> b) { return {a.re + b.re, a.im + b.im}; }
+template <typename T>
+__device__ __forceinline__ cx<T> operator-(cx<T> a, cx<T> b) { return {a.re - b.re, a.im - b.im}; }
+template <typename T>
+__device__ __forceinline__ cx<T> operator*(cx<T> a, cx<T> b)
+{
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+template <typename T>
+__device__ __forceinline__ cx<T> operator*(T s, cx<T> a) { return {s * a.re, s * a.im}; }
+template <typename T>
+__device__ __forceinline__ cx<T> conj(cx<T> a) { return {a.re, -a.im}; }
+// conj(a) * b
+template <typename T>
+__device__ __forceinline__ cx<T> cmulc(cx<T> a, cx<T> b)
+{
+  return {a.re * b.re + a.im * b.im, a.re * b.im - a.im * b.re};
+}
+// i * a
+template <typename T>
+__device__ __forceinline__ cx<T> itimes(cx<T> a) { return {-a.im, a.re}; }
+
+// ---------------------------------------------------------------------------
+// precision traits
+// ---------------------------------------------------------------------------
+struct F64 {
+  using real = double;       // arithmetic type
+  static constexpr int prec = PREC_F64;
+  static constexpr bool has_norm = false;
+};
+struct F32 {
+  using real = float;
+  static constexpr int prec = PREC_F32;
+  static constexpr bool has_norm = false;
+};
+struct F16 {
+  using real = float;
+  static constexpr int prec = PREC_F16;
+  static constexpr bool has_norm = true;
+};
+struct BF16 {
+  using real = float;
+  static constexpr int prec = PREC_BF16;
+  static constexpr bool has_norm = true;
+};
+
+// 16-bit conversions --------------------------------------------------------
+__device__ __forceinline__ void unpack8(const uint4 &v, float out[8], F16)
+{
+  const __half2 *h = reinterpret_cast<const __half2 *>(&v);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    float2 f = __half22float2(h[i]);
+    out[2 * i] = f.x;
+    out[2 * i + 1] = f.y;
+  }
+}
+__device__ __forceinline__ void unpack8(const uint4 &v, float out[8], BF16)
+{
+  const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    float2 f = __bfloat1622float2(h[i]);
+    out[2 * i] = f.x;
+    out[2 * i + 1] = f.y;
+  }
+}
+__device__ __forceinline__ uint4 pack8(const float in[8], F16)
+{
+  uint4 v;
+  __half2 *h = reinterpret_cast<__half2 *>(&v);
+#pragma unroll
+  for (int i = 0; i < 4; i++) h[i] = __floats2half2_rn(in[2 * i], in[2 * i + 1]);
+  return v;
+}
+__device__ __forceinline__ uint4 pack8(const float in[8], BF16)
+{
+  uint4 v;
+  __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&v);
+#pragma unroll
+  for (int i = 0; i < 4; i++) h[i] = __floats2bfloat162_rn(in[2 * i], in[2 * i + 1]);
+  return v;
+}
+__device__ __forceinline__ void unpack4(const uint2 &v, float out[4], F16)
+{
+  const __half2 *h = reinterpret_cast<const __half2 *>(&v);
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    float2 f = __half22float2(h[i]);
+    out[2 * i] = f.x;
+    out[2 * i + 1] = f.y;
+  }
+}
+__device__ __forceinline__ void unpack4(const uint2 &v, float out[4], BF16)
+{
+  const __nv_bfloat162 *h = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+  for (int i = 0; i < 2; i++) {
+    float2 f = __bfloat1622float2(h[i]);
+    out[2 * i] = f.x;
+    out[2 * i + 1] = f.y;
+  }
+}
+__device__ __forceinline__ uint2 pack4(const float in[4], F16)
+{
+  uint2 v;
+  __half2 *h = reinterpret_cast<__half2 *>(&v);
+  h[0] = __floats2half2_rn(in[0], in[1]);
+  h[1] = __floats2half2_rn(in[2], in[3]);
+  return v;
+}
+__device__ __forceinline__ uint2 pack4(const float in[4], BF16)
+{
+  uint2 v;
+  __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&v);
+  h[0] = __floats2bfloat162_rn(in[0], in[1]);
+  h[1] = __floats2bfloat162_rn(in[2], in[3]);
+  return v;
+}
+__device__ __forceinline__ void unpack2(const uint32_t &v, float out[2], F16)
+{
+  float2 f = __half22float2(*reinterpret_cast<const __half2 *>(&v));
+  out[0] = f.x;
+  out[1] = f.y;
+}
+__device__ __forceinline__ void unpack2(const uint32_t &v, float out[2], BF16)
+{
+  float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&v));
+  out[0] = f.x;
+  out[1] = f.y;
+}
+__device__ __forceinline__ uint32_t pack2(const float in[2], F16)
+{
+  __half2 h = __floats2half2_rn(in[0], in[1]);
+  return *reinterpret_cast<uint32_t *>(&h);
+}
+__device__ __forceinline__ uint32_t pack2(const float in[2], BF16)
+{
+  __nv_bfloat162 h = __floats2bfloat162_rn(in[0], in[1]);
+  return *reinterpret_cast<uint32_t *>(&h);
+}
+
+// ---------------------------------------------------------------------------
+// spinor fields
+// ---------------------------------------------------------------------------
+struct SpinorArg {
+  void *data;         // chunk array
+  float *norm;        // per-site norm (16-bit storage only)
+  long long stride;   // sites per chunk row
+  long long rhs_stride_chunks;  // chunk rows per right-hand side (= nchunk * stride)
+};
+
+template <typename P>
+struct SpinorIO;
+
+template <>
+struct SpinorIO<F64> {
+  static constexpr int nchunk = 12;
+  static constexpr size_t chunk_bytes = 16;
+  __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, long long s, double v[24])
+  {
+    const double2 *p = reinterpret_cast<const double2 *>(f.data) + rhs * f.rhs_stride_chunks + s;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      double2 d = __ldg(p + k * f.stride);
+      v[2 * k] = d.x;
+      v[2 * k + 1] = d.y;
+    }
+  }
+  __device__ __forceinline__ static void store(const SpinorArg &f, int rhs, long long s, const double v[24])
+  {
+    double2 *p = reinterpret_cast<double2 *>(f.data) + rhs * f.rhs_stride_chunks + s;
+#pragma unroll
+    for (int k = 0; k < 12; k++) p[k * f.stride] = make_double2(v[2 * k], v[2 * k + 1]);
+  }
+};
+
+template <>
+struct SpinorIO<F32> {
+  static constexpr int nchunk = 6;
+  static constexpr size_t chunk_bytes = 16;
+  __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, long long s, float v[24])
+  {
+    const float4 *p = reinterpret_cast<const float4 *>(f.data) + rhs * f.rhs_stride_chunks + s;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      float4 d = __ldg(p + k * f.stride);
+      v[4 * k] = d.x;
+      v[4 * k + 1] = d.y;
+      v[4 * k + 2] = d.z;
+      v[4 * k + 3] = d.w;
+    }
+  }
+  __device__ __forceinline__ static void store(const SpinorArg &f, int rhs, long long s, const float v[24])
+  {
+    float4 *p = reinterpret_cast<float4 *>(f.data) + rhs * f.rhs_stride_chunks + s;
+#pragma unroll
+    for (int k = 0; k < 6; k++) p[k * f.stride] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+  }
+};
+
+// 16-bit storage with a per-site scale: stored = value / norm, |stored| <= 1
+template <typename H>
+struct SpinorIO16 {
+  static constexpr int nchunk = 3;
+  static constexpr size_t chunk_bytes = 16;
+  __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, long long s, float v[24])
+  {
+    const uint4 *p = reinterpret_cast<const uint4 *>(f.data) + rhs * f.rhs_stride_chunks + s;
+    float nrm = __ldg(f.norm + rhs * f.stride + s);
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      uint4 d = __ldg(p + k * f.stride);
+      unpack8(d, v + 8 * k, H());
+    }
+#pragma unroll
+    for (int k = 0; k < 24; k++) v[k] *= nrm;
+  }
+  __device__ __forceinline__ static void store(const SpinorArg &f, int rhs, long long s, const float v[24])
+  {
+    float m = 0.f;
+#pragma unroll
+    for (int k = 0; k < 24; k++) m = fmaxf(m, fabsf(v[k]));
+    float inv = (m > 0.f) ? 1.0f / m : 0.f;
+    float w[24];
+#pragma unroll
+    for (int k = 0; k < 24; k++) w[k] = v[k] * inv;
+    uint4 *p = reinterpret_cast<uint4 *>(f.data) + rhs * f.rhs_stride_chunks + s;
+#pragma unroll
+    for (int k = 0; k < 3; k++) p[k * f.stride] = pack8(w + 8 * k, H());
+    f.norm[rhs * f.stride + s] = m;
+  }
+};
+template <>
+struct SpinorIO<F16> : SpinorIO16<F16> {};
+template <>
+struct SpinorIO<BF16> : SpinorIO16<BF16> {};
+
+// ---------------------------------------------------------------------------
+// gauge links
+// ---------------------------------------------------------------------------
+struct GaugeArg {
+  const void *data;
+  long long stride;     // sites per chunk row
+  long long mu_stride;  // chunk rows per (cb, mu) = nchunk * stride
+};
+
+// reconstruct row 2 = conj(row0 x row1)
+template <typename T>
+__device__ __forceinline__ void recon12(cx<T> u[3][3])
+{
+  u[2][0] = conj(u[0][1] * u[1][2] - u[0][2] * u[1][1]);
+  u[2][1] = conj(u[0][2] * u[1][0] - u[0][0] * u[1][2]);
+  u[2][2] = conj(u[0][0] * u[1][1] - u[0][1] * u[1][0]);
+}
+
+template <typename P, int RECON>
+struct GaugeIO;
+
+template <>
+struct GaugeIO<F64, 18> {
+  static constexpr int nchunk = 9;
+  static constexpr size_t chunk_bytes = 16;
+  __device__ __forceinline__ static void load(const GaugeArg &g, int cb, int mu, long long s, cx<double> u[3][3])
+  {
+    const double2 *p = reinterpret_cast<const double2 *>(g.data) + (cb * 4 + mu) * g.mu_stride + s;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      double2 d = __ldg(p + k * g.stride);
+      u[k / 3][k % 3] = {d.x, d.y};
+    }
+  }
+};
+template <>
+struct GaugeIO<F64, 12> {
+  static constexpr int nchunk = 6;
+  static constexpr size_t chunk_bytes = 16;
+  __device__ __forceinline__ static void load(const GaugeArg &g, int cb, int mu, long long s, cx<double> u[3][3])
+  {
+    const double2 *p = reinterpret_cast<const double2 *>(g.data) + (cb * 4 + mu) * g.mu_stride + s;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      double2 d = __ldg(p + k * g.stride);
+      u[k / 3][k % 3] = {d.x, d.y};
+    }
+    recon12(u);
+  }
+};
+template <>
+struct GaugeIO<F32, 18> {
+  static constexpr int nchunk = 9;
+  static constexpr size_t chunk_bytes = 8;
+  __device__ __forceinline__ static void load(const GaugeArg &g, int cb, int mu, long long s, cx<float> u[3][3])
+  {
+    const float2 *p = reinterpret_cast<const float2 *>(g.data) + (cb * 4 + mu) * g.mu_stride + s;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      float2 d = __ldg(p + k * g.stride);
+      u[k / 3][k % 3] = {d.x, d.y};
+    }
+  }
+};
+template <>
+struct GaugeIO<F32, 12> {
+  static constexpr int nchunk = 3;
+  static constexpr size_t chunk_bytes = 16;
+  __device__ __forceinline__ static void load(const GaugeArg &g, int cb, int mu, long long s, cx<float> u[3][3])
+  {
+    const float4 *p = reinterpret_cast<const float4 *>(g.data) + (cb * 4 + mu) * g.mu_stride + s;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      float4 d = __ldg(p + k * g.stride);
+      u[(2 * k) / 3][(2 * k) % 3] = {d.x, d.y};
+      u[(2 * k + 1) / 3][(2 * k + 1) % 3] = {d.z, d.w};
+    }
+    recon12(u);
+  }
+};
+template <typename H>
+struct GaugeIO16_18 {
+  static constexpr int nchunk = 9;
+  static constexpr size_t chunk_bytes = 4;
+  __device__ __forceinline__ static void load(const GaugeArg &g, int cb, int mu, long long s, cx<float> u[3][3])
+  {
+    const uint32_t *p = reinterpret_cast<const uint32_t *>(g.data) + (cb * 4 + mu) * g.mu_stride + s;
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      float f[2];
+      unpack2(__ldg(p + k * g.stride), f, H());
+      u[k / 3][k % 3] = {f[0], f[1]};
+    }
+  }
+};
+template <typename H>
+struct GaugeIO16_12 {
+  static constexpr int nchunk = 3;
+  static constexpr size_t chunk_bytes = 8;
+  __device__ __forceinline__ static void load(const GaugeArg &g, int cb, int mu, long long s, cx<float> u[3][3])
+  {
+    const uint2 *p = reinterpret_cast<const uint2 *>(g.data) + (cb * 4 + mu) * g.mu_stride + s;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      float f[4];
+      unpack4(__ldg(p + k * g.stride), f, H());
+      u[(2 * k) / 3][(2 * k) % 3] = {f[0], f[1]};
+      u[(2 * k + 1) / 3][(2 * k + 1) % 3] = {f[2], f[3]};
+    }
+    recon12(u);
+  }
+};
+template <>
+struct GaugeIO<F16, 18> : GaugeIO16_18<F16> {};
+template <>
+struct GaugeIO<F16, 12> : GaugeIO16_12<F16> {};
+template <>
+struct GaugeIO<BF16, 18> : GaugeIO16_18<BF16> {};
+template <>
+struct GaugeIO<BF16, 12> : GaugeIO16_12<BF16> {};
+
+// ---------------------------------------------------------------------------
+// clover fields (NR = 72 packed Hermitian, NR = 144 full blocks)
+// ---------------------------------------------------------------------------
+struct CloverArg {
+  const void *data;
+  long long stride;
+};
+
+template <typename P, int NR>
+struct CloverIO;
+
+template <int NR>
+struct CloverIO<F64, NR> {
+  static constexpr int nchunk = NR / 2;
+  static constexpr size_t chunk_bytes = 16;
+  // load reals [k0, k0+n) (n even, k0 even)
+  __device__ __forceinline__ static void load(const CloverArg &c, long long s, int k0, int n, double *v)
+  {
+    const double2 *p = reinterpret_cast<const double2 *>(c.data) + s;
+    for (int k = 0; k < n; k += 2) {
+      double2 d = __ldg(p + ((k0 + k) / 2) * c.stride);
+      v[k] = d.x;
+      v[k + 1] = d.y;
+    }
+  }
+};
+template <int NR>
+struct CloverIO<F32, NR> {
+  static constexpr int nchunk = NR / 4;
+  static constexpr size_t chunk_bytes = 16;
+  // k0, n multiples of 4
+  __device__ __forceinline__ static void load(const CloverArg &c, long long s, int k0, int n, float *v)
+  {
+    const float4 *p = reinterpret_cast<const float4 *>(c.data) + s;
+    for (int k = 0; k < n; k += 4) {
+      float4 d = __ldg(p + ((k0 + k) / 4) * c.stride);
+      v[k] = d.x;
+      v[k + 1] = d.y;
+      v[k + 2] = d.z;
+      v[k + 3] = d.w;
+    }
+  }
+};
+template <typename H, int NR>
+struct CloverIO16 {
+  static constexpr int nchunk = NR / 8;
+  static constexpr size_t chunk_bytes = 16;
+  // k0, n multiples of 4: loads whole 8-value chunks and picks the needed half
+  __device__ __forceinline__ static void load(const CloverArg &c, long long s, int k0, int n, float *v)
+  {
+    const uint4 *p = reinterpret_cast<const uint4 *>(c.data) + s;
+    for (int k = 0; k < n; k += 4) {
+      int q = k0 + k;
+      uint4 d = __ldg(p + (q / 8) * c.stride);
+      uint2 h = (q % 8 == 0) ? make_uint2(d.x, d.y) : make_uint2(d.z, d.w);
+      unpack4(h, v + k, H());
+    }
+  }
+};
+template <int NR>
+struct CloverIO<F16, NR> : CloverIO16<F16, NR> {};
+template <int NR>
+struct CloverIO<BF16, NR> : CloverIO16<BF16, NR> {};
+
+// ---------------------------------------------------------------------------
+// lattice geometry as seen by a kernel
+// ---------------------------------------------------------------------------
+struct Geom {
+  int nx, ny, nz, nt, nxh;
+  int vh;
+};
+
+__device__ __forceinline__ void site_coords(const Geom &g, int s, int cb, int &xh, int &y, int &z,
+                                            int &t, int &par)
+{
+  xh = s % g.nxh;
+  int r = s / g.nxh;
+  y = r % g.ny;
+  r /= g.ny;
+  z = r % g.nz;
+  t = r / g.nz;
+  par = (y + z + t + cb) & 1;  // x = 2 xh + par
+}
+
+}  // namespace qpx

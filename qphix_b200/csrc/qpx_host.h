@@ -1,0 +1,142 @@
+// Host-side internals of the C ABI: handle structs, error plumbing and the
+// kernel-dispatch entry points implemented by the per-precision .cu files.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/qphix_b200.h"
+#include "qpx_blas.cuh"
+#include "qpx_dslash.cuh"
+#include "qpx_layout.cuh"
+#include "qpx_reduce.cuh"
+
+namespace qpx {
+
+// error raised inside the library, mapped to a status code at the C boundary
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define QPX_CUDA(call)                                                                          \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      throw ::qpx::Error(e_ == cudaErrorMemoryAllocation ? QPHIX_GPU_ENOMEM : QPHIX_GPU_ECUDA, \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));                   \
+  } while (0)
+
+#define QPX_REQUIRE(cond, msg)                                   \
+  do {                                                           \
+    if (!(cond)) throw ::qpx::Error(QPHIX_GPU_EINVAL, (msg));    \
+  } while (0)
+
+// per-precision element geometry of the device layouts
+struct ChunkSpec {
+  int nchunk;
+  int chunk_bytes;
+  int vpc;  // values per chunk
+};
+ChunkSpec spinor_spec(int prec);
+ChunkSpec gauge_spec(int prec, int recon);
+ChunkSpec clover_spec(int prec, int nreal);
+
+}  // namespace qpx
+
+struct qphix_gpu_lattice_s {
+  int dims[4];
+  int nxh;
+  long long vh;
+  long long stride;  // vh rounded up to a multiple of 64
+  cudaStream_t stream = nullptr;
+  bool owns_stream = false;
+  int refs = 1;  // the creator's reference plus one per live field
+  // reduction workspace (one in-flight reduction per stream at a time)
+  double *partials = nullptr;
+  size_t partials_len = 0;
+  unsigned int *ticket = nullptr;
+  double *result = nullptr;       // device [QPX_MAX_RHS * QPX_MAX_RED]
+  double *h_result = nullptr;     // pinned mirror
+  qpx::SolverState *state = nullptr;   // device
+  qpx::SolverState *h_state = nullptr; // pinned mirror
+  void *staging = nullptr;
+  size_t staging_bytes = 0;
+  qpx::Geom geom() const
+  {
+    qpx::Geom g;
+    g.nx = dims[0];
+    g.ny = dims[1];
+    g.nz = dims[2];
+    g.nt = dims[3];
+    g.nxh = nxh;
+    g.vh = (int)vh;
+    return g;
+  }
+};
+
+struct qphix_gpu_field_s {
+  qphix_gpu_lattice_s *lat;
+  int kind, prec, recon, nrhs;
+  qpx::ChunkSpec spec;
+  void *data = nullptr;
+  float *norm = nullptr;
+  size_t bytes = 0;
+  qpx::SpinorArg sarg() const
+  {
+    qpx::SpinorArg a;
+    a.data = data;
+    a.norm = norm;
+    a.stride = lat->stride;
+    a.rhs_stride_chunks = (long long)spec.nchunk * lat->stride;
+    return a;
+  }
+  qpx::GaugeArg garg() const
+  {
+    qpx::GaugeArg a;
+    a.data = data;
+    a.stride = lat->stride;
+    a.mu_stride = (long long)spec.nchunk * lat->stride;
+    return a;
+  }
+  qpx::CloverArg carg() const
+  {
+    qpx::CloverArg a;
+    a.data = data;
+    a.stride = lat->stride;
+    return a;
+  }
+};
+
+struct qphix_gpu_eo_op_s {
+  qphix_gpu_op_params p;
+  qphix_gpu_field_s *gauge, *clov, *invclov, *finv0, *finv1;
+  std::map<int, qphix_gpu_field_s *> tmp;  // by nrhs
+};
+
+namespace qpx {
+
+// ---- dispatch (implemented per precision) ----------------------------------
+void launch_dslash(int prec, int recon, int epi, int achi, int R, const DslashArgs &a, dim3 grid,
+                   cudaStream_t st);
+void launch_blas(int prec, const BlasArgs &a, dim3 grid, cudaStream_t st);
+void launch_convert(int pdst, int psrc, int vh, SpinorArg src, SpinorArg dst, Coef scale, SolverState *state,
+                    dim3 grid, cudaStream_t st);
+void launch_spinor_in(int prec, Geom g, HostLayout L, const void *host, SpinorArg f, int nrhs, dim3 grid,
+                      cudaStream_t st);
+void launch_spinor_out(int prec, Geom g, HostLayout L, void *host, SpinorArg f, int nrhs, dim3 grid,
+                       cudaStream_t st);
+void launch_gauge_in(int prec, Geom g, HostLayout L, const void *host, void *dev, long long stride,
+                     long long slab_bytes, int vpc, int recon, int cb, dim3 grid, cudaStream_t st);
+void launch_clover_in(int prec, Geom g, HostLayout L, const void *host, void *dev, long long stride, int vpc,
+                      int nr, dim3 grid, cudaStream_t st);
+void launch_clover_out(int prec, Geom g, void *host, const void *dev, long long stride, int vpc, int nr,
+                       dim3 grid, cudaStream_t st);
+
+// tile sizes compiled for each precision
+bool dslash_tile_ok(int prec, int R);
+
+}  // namespace qpx

@@ -1,0 +1,146 @@
+// Deterministic global reductions fused into the epilogue of any kernel, and
+// the device-resident solver scalars they feed.
+//
+// Every reducing kernel computes up to QPX_MAX_RED doubles per right-hand
+// side per thread, reduces them over the block (warp shuffles, then a fixed
+// order over warps), writes one partial per (block, rhs, value), and the last
+// block to finish (atomic ticket) sums the partials in block order and runs a
+// finalize step on thread 0.  The order of every addition is fixed by the
+// launch shape, so results are bitwise reproducible run to run.
+//
+// The finalize step updates a SolverState in device memory (Krylov scalars
+// alpha, beta, omega, rho, residual norms, convergence flags) so that a
+// solver iteration is a fixed sequence of launches with no host round trip:
+// it can be captured once in a CUDA graph and replayed.
+#pragma once
+
+#include "qpx_common.cuh"
+
+namespace qpx {
+
+constexpr int QPX_MAX_RHS = 32;
+constexpr int QPX_MAX_RED = 6;
+constexpr int QPX_NSLOT = 24;
+constexpr int QPX_BLOCK = 128;
+
+// scalar slots (per rhs)
+enum Slot : int {
+  S_RHO_RE = 0, S_RHO_IM, S_RHOP_RE, S_RHOP_IM, S_ALPHA_RE, S_ALPHA_IM,
+  S_OMEGA_RE, S_OMEGA_IM, S_BETA_RE, S_BETA_IM, S_RNORM, S_TNORM,
+  S_A, S_B, S_C, S_D, S_RSD, S_AUX0, S_AUX1, S_AUX2, S_AUX3, S_AUX4, S_AUX5, S_AUX6
+};
+
+struct SolverState {
+  int done;       // 1: stop issuing work (all rhs converged, broke down or hit max)
+  int iter;       // completed iterations
+  int max_iter;
+  int status;     // 0 converged / running, 1 max iterations, 2 breakdown
+  int nrhs;
+  int pad[3];
+  int rhs_done[QPX_MAX_RHS];
+  int rhs_iter[QPX_MAX_RHS];
+  double v[QPX_NSLOT][QPX_MAX_RHS];
+};
+
+// finalize operations (solver-specific scalar recurrences)
+enum FinOp : int {
+  FIN_NONE = 0,
+  FIN_CG_A,        // d = |Mp|^2 ; a = c / d
+  FIN_CG_R,        // cp = |r|^2 ; converged? ; b = cp / c ; c = cp
+  FIN_BICG_ALPHA,  // <r0,v> -> alpha = rho / <r0,v>, rho_prev = rho
+  FIN_BICG_OMEGA,  // |t|^2, <t,s> -> omega
+  FIN_BICG_RX,     // |r|^2, <r0,r> -> converged? ; rho ; beta
+  FIN_MR_A,        // |Mr|^2, <Mr,r> -> a = Omega <Mr,r>/|Mr|^2
+  FIN_MR_R,        // |r|^2 -> converged?
+  FIN_STORE,       // plain reduction: result only
+  FIN_MCG_D,       // multishift CG: d = |Mp|^2, b = -cp/d
+  FIN_MCG_R,       // multishift CG: c = |r|^2, zeta/beta per shift, convergence
+};
+
+struct ReduceArg {
+  int mask;            // which values (bit order fixed by the producing kernel)
+  int nval;            // number of doubles per rhs
+  int fin;             // FinOp
+  double *partials;    // [nblocks][nrhs][nval]
+  unsigned int *ticket;
+  double *result;      // [nrhs][nval]
+};
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum `val` over the block; result valid in thread 0.  All threads must call.
+__device__ __forceinline__ double block_sum(double val, double *smem)
+{
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int nw = (blockDim.x + 31) >> 5;
+  val = warp_sum(val);
+  __syncthreads();
+  if (lane == 0) smem[wid] = val;
+  __syncthreads();
+  double r = 0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < nw; w++) r += smem[w];
+  return r;
+}
+
+__device__ inline void finalize(int fin, SolverState *st, const double *res, int nrhs, int nval);
+
+// Called by every thread of every block after the block's per-thread values
+// are final.  Values live in fixed slots val[r][k] (k < QPX_MAX_RED, compile-
+// time indices so they stay in registers); `slots` (ReduceArg::mask of the
+// producing kernel, translated by it into a slot bit set) says which slots
+// are live, and they are packed in slot order into nval doubles per rhs.
+// rhs0 = first rhs of the block's tile.  The last block runs the finalize.
+template <int R>
+__device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, SolverState *st, int nrhs, int rhs0,
+                                                int slots, const double val[R][QPX_MAX_RED])
+{
+  __shared__ double smem[32];
+  __shared__ bool am_last;
+  const long long nblocks = (long long)gridDim.x * gridDim.y;
+  const long long bid = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    int o = 0;
+#pragma unroll
+    for (int k = 0; k < QPX_MAX_RED; k++) {
+      if (slots & (1 << k)) {
+        double s = block_sum(val[r][k], smem);
+        if (threadIdx.x == 0 && rhs0 + r < nrhs)
+          ra.partials[((long long)blockIdx.x * nrhs + rhs0 + r) * ra.nval + o] = s;
+        o++;
+      }
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int t = atomicAdd(ra.ticket, 1u);
+    am_last = (t == (unsigned int)(nblocks - 1));
+  }
+  __syncthreads();
+  (void)bid;
+  if (!am_last) return;
+  __threadfence();
+  // last block: fold the partials of every x-block, in block order
+  const int gx = gridDim.x;
+  for (int idx = 0; idx < nrhs * ra.nval; idx++) {
+    double acc = 0;
+    for (int b = threadIdx.x; b < gx; b += blockDim.x)
+      acc += __ldcg(ra.partials + (long long)b * nrhs * ra.nval + idx);
+    double s = block_sum(acc, smem);
+    if (threadIdx.x == 0) ra.result[idx] = s;
+  }
+  if (threadIdx.x == 0) {
+    *ra.ticket = 0u;
+    __threadfence();
+    if (ra.fin != FIN_NONE && st) finalize(ra.fin, st, ra.result, nrhs, ra.nval);
+  }
+}
+
+}  // namespace qpx

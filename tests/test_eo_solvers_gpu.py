@@ -1,0 +1,173 @@
+"""Even-odd operators and solvers through the C ABI against the CPU oracle.
+
+Operators: relative L2 <= 1e-13 (FP64) / 1e-6 (FP32) for every kind, isign
+and target checkerboard, plus the gamma_5 hermiticity identity
+|<y, M x> - <M^dag y, x>| / (|y| |M x|) <= 1e-14 in FP64
+(the idea of include/qphix/inv_dummy_hermtest.h).
+Solvers: the true residual |b - M x| / |b| is recomputed in FP64 for every
+solve and must meet the target; FP64 iteration counts equal the oracle's
+(same recurrences as include/qphix/invcg.h, invbicgstab.h, invmr.h).
+"""
+import numpy as np
+import pytest
+
+from helpers import TOL, make_setup, rel_l2
+from qphix_b200 import fields as F
+
+pytestmark = pytest.mark.gpu
+
+KINDS = ["wilson", "clover", "tm", "tmclover"]
+
+
+@pytest.fixture(scope="module")
+def api():
+    from qphix_b200 import api
+    return api
+
+
+@pytest.fixture(scope="module")
+def setup():
+    return make_setup((4, 4, 4, 8), seed=21, gauge_kind="weak", mass=0.1, mu=0.1)
+
+
+def build_ops(api, oracle, s, kind, prec="f64", recon=12, target_cb=1):
+    dims = s["dims"]
+    lat = api.Lattice(dims)
+    u = lat.gauge(prec, recon).upload(s["gauge"])
+    L = oracle.make_lattice(dims, -1.0, 1.0, 1.0)
+    other = 1 - target_cb
+    keep = [u]
+    if kind == "wilson":
+        M = api.EvenOddWilsonOperator(s["mass"], u)
+        O = oracle.OracleOp("wilson", L, s["gauge"], mass=s["mass"])
+    elif kind == "tm":
+        M = api.EvenOddTMWilsonOperator(s["mass"], s["mu"], u)
+        O = oracle.OracleOp("tm", L, s["gauge"], mass=s["mass"], twisted_mass=s["mu"])
+    elif kind == "clover":
+        A = lat.clover(prec).upload(s["clov"][target_cb])
+        Ai = lat.clover(prec).upload(s["invclov"][other])
+        keep += [A, Ai]
+        M = api.EvenOddCloverOperator(u, A, Ai, prec_mass_rho=0.0)
+        O = oracle.OracleOp("clover", L, s["gauge"], clov=s["clov"][target_cb],
+                            invclov=s["invclov"][other])
+    else:
+        A = lat.clover(prec).upload(s["clov"][target_cb])
+        f0 = lat.full_clover(prec).upload(s["finv"][other][0])
+        f1 = lat.full_clover(prec).upload(s["finv"][other][1])
+        keep += [A, f0, f1]
+        M = api.EvenOddTMCloverOperator(u, A, (f0, f1), prec_mass_rho=s["mu"])
+        O = oracle.OracleOp("tmclover", L, s["gauge"], clov=s["clov"][target_cb],
+                            finv=s["finv"][other], rho=s["mu"])
+    M._keep = keep
+    return lat, M, O
+
+
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_eo_operator(api, oracle, setup, kind, prec):
+    for target_cb in (1, 0):
+        lat, M, O = build_ops(api, oracle, setup, kind, prec, target_cb=target_cb)
+        x = F.gaussian_spinor(setup["dims"], 31)
+        gx = lat.spinor(prec).upload(x)
+        gr = lat.spinor(prec)
+        for isign in (1, -1):
+            M(gr, gx, isign, target_cb)
+            ref = O.apply(x, isign, target_cb)
+            assert rel_l2(gr.download(), ref) < TOL[prec], (kind, target_cb, isign)
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_hermiticity(api, oracle, setup, kind):
+    lat, M, O = build_ops(api, oracle, setup, kind)
+    x = F.gaussian_spinor(setup["dims"], 32)
+    y = F.gaussian_spinor(setup["dims"], 33)
+    gx, gy = lat.spinor().upload(x), lat.spinor().upload(y)
+    mx, mdy = lat.spinor(), lat.spinor()
+    M(mx, gx, 1)
+    M(mdy, gy, -1)
+    a = np.vdot(y, mx.download())
+    b = np.vdot(mdy.download(), x)
+    assert abs(a - b) / (np.linalg.norm(y) * np.linalg.norm(mx.download())) < 1e-14
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_cg(api, oracle, setup, kind):
+    lat, M, O = build_ops(api, oracle, setup, kind)
+    b = F.gaussian_spinor(setup["dims"], 41)
+    gx, gb = lat.spinor(), lat.spinor().upload(b)
+    info = api.InvCG(M, 500)(gx, gb, 1e-10)[0]
+    xo, io = oracle.cg(O, b, 1e-10, 500)
+    x = gx.download()
+    r = b - O.apply(O.apply(x, 1), -1)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10 * 1.5
+    assert info["status"] == 0 and info["true_rel_resid"] < 1.5e-10
+    assert info["n_iters"] == io.n_iters
+    assert rel_l2(x, xo) < 1e-8
+
+
+@pytest.mark.parametrize("kind", KINDS)
+def test_bicgstab(api, oracle, setup, kind):
+    lat, M, O = build_ops(api, oracle, setup, kind)
+    b = F.gaussian_spinor(setup["dims"], 42)
+    gx, gb = lat.spinor(), lat.spinor().upload(b)
+    info = api.InvBiCGStab(M, 500)(gx, gb, 1e-10)[0]
+    xo, io = oracle.bicgstab(O, b, 1e-10, 500)
+    x = gx.download()
+    r = b - O.apply(x, 1)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 2e-10
+    assert info["status"] == 0
+    assert abs(info["n_iters"] - io.n_iters) <= 1
+    assert rel_l2(x, xo) < 1e-8
+
+
+def test_mr(api, oracle, setup):
+    lat, M, O = build_ops(api, oracle, setup, "clover")
+    b = F.gaussian_spinor(setup["dims"], 43)
+    gx, gb = lat.spinor(), lat.spinor().upload(b)
+    info = api.InvMR(M, 2000, 1.0)(gx, gb, 1e-10)[0]
+    xo, io = oracle.mr(O, b, 1e-10, 2000, 1.0)
+    x = gx.download()
+    r = b - O.apply(x, 1)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 2e-10
+    assert info["n_iters"] == io.n_iters
+
+
+@pytest.mark.parametrize("inner_prec", ["f32", "f16", "bf16"])
+def test_richardson_mixed(api, oracle, setup, inner_prec):
+    s = setup
+    lat, M, O = build_ops(api, oracle, s, "clover")
+    u_in = lat.gauge(inner_prec, 12).upload(s["gauge"])
+    A = lat.clover(inner_prec).upload(s["clov"][1])
+    Ai = lat.clover(inner_prec).upload(s["invclov"][0])
+    Mi = api.EvenOddCloverOperator(u_in, A, Ai)
+    b = F.gaussian_spinor(s["dims"], 44)
+    gx, gb = lat.spinor(), lat.spinor().upload(b)
+    solver = api.InvRichardsonMultiPrec(M, Mi, "bicgstab", delta=0.1, max_iters=50)
+    info = solver(gx, gb, 1e-10)[0]
+    x = gx.download()
+    r = b - O.apply(x, 1)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10
+    assert info["status"] == 0
+
+
+def test_multi_rhs_block_matches_single(api, oracle, setup):
+    """A block of right-hand sides gives, rhs by rhs, the single-rhs result."""
+    s = setup
+    dims = s["dims"]
+    for prec in ("f64", "f32"):
+        lat, M, O = build_ops(api, oracle, s, "clover", prec)
+        nr = 4
+        bs = [F.gaussian_spinor(dims, 50 + i) for i in range(nr)]
+        gb = lat.spinor(prec, nr).upload(np.stack(bs))
+        gr = lat.spinor(prec, nr)
+        M(gr, gb, 1)
+        out = gr.download()
+        for i in range(nr):
+            assert rel_l2(out[i], O.apply(bs[i], 1)) < TOL[prec]
+        gx = lat.spinor(prec, nr)
+        infos = api.InvBiCGStab(M, 500)(gx, gb, 1e-5 if prec == "f32" else 1e-10)
+        xs = gx.download()
+        for i in range(nr):
+            r = bs[i] - O.apply(xs[i], 1)
+            assert np.linalg.norm(r) / np.linalg.norm(bs[i]) < (2e-5 if prec == "f32" else 2e-10)
+            assert infos[i]["status"] == 0
