@@ -485,9 +485,11 @@ void or_cg(const or_operator *op, double *x, const double *rhs, double rsd,
     }
     if (cp < rsd_sq) {
       info->n_iters = k;
+      /* true residual; the reference's own recompute sits under an #ifdef
+         that is never defined (include/qphix/invcg.h:342-403), so it counts
+         no operator applications for it and leaves rsd_sq_final unset */
       or_eo_apply(op, mp, x, isign, cb);
       or_eo_apply(op, mmp, mp, -isign, cb);
-      mv += 2;
       for (long i = 0; i < n; i++) r[i] = rhs[i] - mmp[i];
       info->rsd_sq_final = or_norm2(n, r);
       info->mv_apps = mv;

@@ -1,0 +1,170 @@
+"""Pins the CPU oracle to the reference (CPU only).
+
+1. Against tests/golden/reference_pin.npz, produced by the reference's own
+   clover product, BLAS and Krylov solvers (tests/golden/make_golden.py):
+   clover products bit-exact, BLAS to rounding, solver iteration counts equal
+   and solutions to 1e-12.
+2. When the reference sources are present (oracle/_ref built), the same
+   comparisons live, for every operator kind.
+3. The oracle's Dslash against the analytic free-field result: on unit links
+   a plane wave e^{i p.x} u is an eigenvector,
+       D psi = sum_mu c_mu [2 cos p_mu - 2 i isign sin p_mu gamma_mu] psi,
+   with p_t an odd multiple of pi/Nt for antiperiodic time boundaries
+   (tests/dslashm_w.cc:20-34 with the DeGrand-Rossi gammas of
+   codegen/dslash_common.cc:848-866).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import make_setup
+from qphix_b200 import fields as F
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLD = os.path.join(HERE, "golden", "reference_pin.npz")
+DIMS = (4, 4, 4, 4)
+SHIFTS = [0.01, 0.1, 0.5]
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return dict(np.load(GOLD))
+
+
+@pytest.fixture(scope="module")
+def inp():
+    s = make_setup(DIMS, seed=3, gauge_kind="weak", mass=0.1, mu=0.1)
+    return s, F.gaussian_spinor(DIMS, 1), F.gaussian_spinor(DIMS, 2), F.gaussian_spinor(DIMS, 5)
+
+
+def test_clover_products_bit_exact(oracle, gold, inp):
+    s, x, y, b = inp
+    assert np.array_equal(oracle.clover_apply(x, s["clov"][0]), gold["clover_packed"])
+    assert np.array_equal(oracle.fullclover_apply(x, s["finv"][0][0]), gold["clover_full"])
+
+
+def test_blas(gold, inp):
+    s, x, y, b = inp
+    assert abs(np.vdot(x, x).real - gold["blas_norm2"][0]) < 1e-12 * gold["blas_norm2"][0]
+    ip = np.vdot(x, y)
+    assert abs(ip - (gold["blas_inner"][0] + 1j * gold["blas_inner"][1])) < 1e-12 * abs(ip) + 1e-12
+    assert np.allclose(0.3 * x + y, gold["blas_axpy"], atol=1e-14)
+    assert np.allclose((0.3 - 0.7j) * x + y, gold["blas_caxpy"], atol=1e-14)
+    assert np.allclose(0.3 * x - 1.1 * y, gold["blas_axpby"], atol=1e-14)
+    assert np.allclose(x + 0.45 * y, gold["blas_aypx"], atol=1e-14)
+    assert np.allclose(x - y, gold["blas_xmynorm2"], atol=1e-14)
+    assert abs(np.vdot(x - y, x - y).real - gold["blas_xmynorm2_n"]) < 1e-10
+
+
+def _clover_op(oracle, s):
+    L = oracle.make_lattice(DIMS, -1.0)
+    return oracle.OracleOp("clover", L, s["gauge"], clov=s["clov"][1], invclov=s["invclov"][0])
+
+
+@pytest.mark.parametrize("kind", ["cg", "bicgstab", "mr"])
+def test_solvers_against_reference(oracle, gold, inp, kind):
+    s, x, y, b = inp
+    op = _clover_op(oracle, s)
+    xo, info = getattr(oracle, kind)(op, b, 1e-10, 1000)
+    assert info.n_iters == gold[f"{kind}_iters"]
+    assert info.mv_apps == gold[f"{kind}_mv"]
+    assert np.abs(xo - gold[f"{kind}_x"]).max() < 1e-12
+    if kind != "cg":  # the reference leaves CG's rsd_sq_final unset
+        assert abs(info.rsd_sq_final - gold[f"{kind}_rsd"]) <= 1e-6 * gold[f"{kind}_rsd"]
+
+
+def test_richardson_against_reference(oracle, gold, inp):
+    s, x, y, b = inp
+    op = _clover_op(oracle, s)
+    xo, info = oracle.richardson_bicgstab(op, b, 1e-10, 0.1)
+    assert info.n_iters == gold["rich_iters"] and info.mv_apps == gold["rich_mv"]
+    assert np.abs(xo - gold["rich_x"]).max() < 1e-12
+
+
+def test_minvcg_against_reference(oracle, gold, inp):
+    s, x, y, b = inp
+    op = _clover_op(oracle, s)
+    xs, it, fin, mv = oracle.minvcg(op, b, SHIFTS, [1e-9] * 3)
+    assert it == gold["minv_iters"] and mv == gold["minv_mv"]
+    assert np.abs(np.stack(xs) - gold["minv_x"]).max() < 1e-12
+    assert np.allclose(fin, gold["minv_rsd"], rtol=1e-6)
+
+
+def _ref():
+    import ref_oracle as R
+    if not R.available():
+        pytest.skip("reference harness not built (no reference sources here)")
+    return R
+
+
+@pytest.mark.parametrize("kind", ["wilson", "clover", "tm", "tmclover"])
+def test_live_reference_solvers_every_operator(oracle, kind):
+    R = _ref()
+    s = make_setup(DIMS, seed=8, gauge_kind="gaussian" if kind == "wilson" else "weak", mass=0.15, mu=0.07)
+    L = oracle.make_lattice(DIMS, -1.0, 0.9, 1.1)
+    kw = {"wilson": dict(mass=s["mass"]), "tm": dict(mass=s["mass"], twisted_mass=s["mu"]),
+          "clover": dict(clov=s["clov"][1], invclov=s["invclov"][0], rho=0.02),
+          "tmclover": dict(clov=s["clov"][1], finv=s["finv"][0], rho=s["mu"])}[kind]
+    op = oracle.OracleOp(kind, L, s["gauge"], **kw)
+    b = F.gaussian_spinor(DIMS, 9)
+    for solver in ("cg", "bicgstab", "mr"):
+        for isign in (1, -1):
+            xr, it, fin, mv = R.solve(op, solver, b, 1e-9, 2000, isign=isign)
+            xo, info = getattr(oracle, solver)(op, b, 1e-9, 2000, isign=isign)
+            assert it == info.n_iters and mv == info.mv_apps, (solver, isign)
+            assert np.abs(xr - xo).max() < 1e-11
+
+
+def test_live_reference_clover_products(oracle):
+    R = _ref()
+    for seed in (1, 2):
+        s = make_setup((8, 4, 4, 4), seed=seed, mu=0.2)
+        x = F.gaussian_spinor((8, 4, 4, 4), seed + 10)
+        for cb in (0, 1):
+            assert np.array_equal(R.clover_apply((8, 4, 4, 4), x, s["invclov"][cb]),
+                                  oracle.clover_apply(x, s["invclov"][cb]))
+            f = s["finv"][cb][1]
+            assert np.array_equal(R.clover_apply((8, 4, 4, 4), x, F.full_clover_to_real(f), True),
+                                  oracle.fullclover_apply(x, f))
+
+
+# DeGrand-Rossi gammas
+G = np.zeros((4, 4, 4), dtype=complex)
+G[0][0, 3], G[0][1, 2], G[0][2, 1], G[0][3, 0] = 1j, 1j, -1j, -1j
+G[1][0, 3], G[1][1, 2], G[1][2, 1], G[1][3, 0] = -1, 1, 1, -1
+G[2][0, 2], G[2][1, 3], G[2][2, 0], G[2][3, 1] = 1j, -1j, -1j, 1j
+G[3][0, 2], G[3][1, 3], G[3][2, 0], G[3][3, 1] = 1, 1, 1, 1
+
+
+@pytest.mark.parametrize("isign", [1, -1])
+@pytest.mark.parametrize("t_bc", [1.0, -1.0])
+def test_dslash_free_field_plane_wave(oracle, isign, t_bc):
+    dims = (8, 4, 6, 8)
+    g = F.make_gauge(dims, 0, "unit")
+    rng = np.random.default_rng(4)
+    n = [1, 1, 2, 3]
+    p = [2 * np.pi * n[m] / dims[m] for m in range(3)]
+    p.append((2 * n[3] + (1 if t_bc < 0 else 0)) * np.pi / dims[3])
+    u = rng.standard_normal((4, 3)) + 1j * rng.standard_normal((4, 3))
+    aniso_s, aniso_t = 0.8, 1.3
+    L = oracle.make_lattice(dims, t_bc, aniso_s, aniso_t)
+    for cb in (0, 1):
+        src_cb = 1 - cb
+        xs = F.cb_coords(dims, src_cb)
+        ph = np.exp(1j * sum(p[m] * xs[m] for m in range(4)))
+        psi = ph[:, None, None] * u[None]
+        out = oracle.dslash(L, psi, g, isign, cb)
+        K = np.zeros((4, 4), dtype=complex)
+        for m in range(4):
+            c = aniso_t if m == 3 else aniso_s
+            K += c * (2 * np.cos(p[m]) * np.eye(4) - 2j * isign * np.sin(p[m]) * G[m])
+        xt = F.cb_coords(dims, cb)
+        pht = np.exp(1j * sum(p[m] * xt[m] for m in range(4)))
+        expect = pht[:, None, None] * np.einsum("ij,jc->ic", K, u)[None]
+        assert np.abs(out - expect).max() < 1e-12
+
+
+def test_gamma5_is_product_of_gammas():
+    g5 = G[0] @ G[1] @ G[2] @ G[3]
+    assert np.allclose(g5, np.diag([1, 1, -1, -1]))
