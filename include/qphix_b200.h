@@ -202,6 +202,23 @@ int qphix_gpu_blas_caxpby(const double a[2], qphix_gpu_field x, const double b[2
 int qphix_gpu_blas_copy(qphix_gpu_field dst, qphix_gpu_field src);               /* :18  */
 int qphix_gpu_blas_zero(qphix_gpu_field x);                                      /* :49  */
 
+/* ---- squared norms without allocation ---------------------------------------
+ * No counterpart in the reference.  Same result as qphix_gpu_blas_norm2, for
+ * callers that cannot let the library call cudaMalloc: host codes whose
+ * device memory is owned by another allocator that has already reserved the
+ * free HBM, or that must not add the device-wide synchronisation cudaMalloc /
+ * cudaFree can cause inside a latency-sensitive loop.  Allocates nothing: the
+ * per-block partial sums live in a fixed 512 KiB array in the library's
+ * device memory (held by every GPU that loads the library until exit) and
+ * the nrhs results are written to out_dev, a device buffer of nrhs doubles
+ * owned by the caller, asynchronously on the lattice's stream (synchronise it
+ * before reading).  Limit: ceil(volcb / 128) * nrhs <= 65536, else
+ * QPHIX_GPU_EINVAL.  The field's device must be the current device.  The
+ * first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  Every call shares the array, so
+ * calls whose kernels overlap on the GPU race. */
+int qphix_gpu_blas_norm2_noalloc(qphix_gpu_field x, double *out_dev);
+
 #ifdef __cplusplus
 }
 #endif

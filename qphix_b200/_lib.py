@@ -72,6 +72,7 @@ _SIGS = {
                                    C.POINTER(C.c_ulong)], I_),
     "qphix_gpu_solve_richardson": ([P, P, I_, P, P, D, D, I_, I_, I_, I_, C.POINTER(SolveInfo)], I_),
     "qphix_gpu_blas_norm2": ([P, P], I_),
+    "qphix_gpu_blas_norm2_noalloc": ([P, P], I_),
     "qphix_gpu_blas_inner_product": ([P, P, P], I_),
     "qphix_gpu_blas_caxpby": ([P, P, P, P], I_),
     "qphix_gpu_blas_copy": ([P, P], I_),

@@ -19,6 +19,12 @@ using namespace qpx;
 
 static thread_local std::string g_last_error;
 
+int qpx_set_last_error(const char *msg, int code)
+{
+  g_last_error = msg;
+  return code;
+}
+
 template <typename F>
 static int guard(F &&f)
 {

@@ -1,0 +1,67 @@
+"""qphix_gpu_blas_norm2_noalloc against qphix_gpu_blas_norm2, through the C ABI.
+
+The no-allocation entry point is for callers that cannot let the library
+call cudaMalloc (their device memory belongs to another allocator, or an
+allocation's implicit synchronisation is not acceptable where they call).
+It keeps its reduction scratch in a fixed device array instead of the
+lattice workspace and writes to a caller-owned device buffer; the test checks
+that, on two calls in a row, it returns what the regular entry point returns
+(relative 1e-13, the FP64 tolerance of the other parity tests), for several
+precisions and right-hand-side counts, and that it rejects a request larger
+than its fixed scratch.  This file is collected last so a stop-at-first-
+failure run has already run every other test.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _noalloc(lib, field, out):
+    import torch
+    torch.cuda.synchronize()
+    rc = lib.qphix_gpu_blas_norm2_noalloc(field.h, C.c_void_p(out.data_ptr()))
+    return rc
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32", "f16"])
+@pytest.mark.parametrize("nrhs", [1, 4])
+def test_norm2_noalloc_matches_norm2(prec, nrhs):
+    import torch
+
+    from qphix_b200 import _lib, api
+    from qphix_b200 import fields as F
+
+    lib = _lib.load()
+    dims = (8, 8, 8, 16)
+    lat = api.Lattice(dims, device=0)
+    x = lat.spinor(prec, nrhs).upload(np.stack([F.gaussian_spinor(dims, 70 + i) for i in range(nrhs)]))
+    ref = api.norm2(x)
+    out = torch.full((nrhs,), float("nan"), dtype=torch.float64, device="cuda:0")
+    for _ in range(2):  # two calls in a row share the scratch
+        out.fill_(float("nan"))
+        assert _noalloc(lib, x, out) == _lib.OK, lib.qphix_gpu_last_error()
+        lat.sync()
+        got = out.cpu().numpy()
+        assert np.all(np.abs(got - ref) <= 1e-13 * np.abs(ref)), (got, ref)
+
+
+def test_norm2_noalloc_rejects_oversized_request():
+    import torch
+
+    from qphix_b200 import _lib, api
+
+    lib = _lib.load()
+    lat = api.Lattice((32, 32, 32, 64), device=0)  # 8192 blocks of 128 sites
+    x = lat.spinor("f16", 9)                        # 8192 * 9 > 65536 partials
+    out = torch.zeros(9, dtype=torch.float64, device="cuda:0")
+    assert _noalloc(lib, x, out) == _lib.EINVAL
+    assert b"65536" in lib.qphix_gpu_last_error()
+    x.close()
+    small = lat.spinor("f16", 8)                    # exactly at the limit
+    out8 = torch.zeros(8, dtype=torch.float64, device="cuda:0")
+    assert _noalloc(lib, small, out8) == _lib.OK
+    lat.sync()
+    assert np.all(out8.cpu().numpy() == 0.0)
