@@ -4,11 +4,12 @@
 Workload (one step = one batched solve): even-odd preconditioned Wilson-clover
 operator on a 16^3x32 lattice, kappa = 0.1360 (bare mass 1/(2 kappa) - 4),
 c_sw = 1.0, links exp(i 0.3 H) with H drawn from the Gaussian unitary
-ensemble (stored 12-real), antiperiodic in t.  The solver is QPhiX's
-InvRichardsonMultiPrec: FP64 outer defect correction to a 1e-10 relative
-true residual, inner BiCGStab on FP16-storage (per-site norm) / FP32-compute
-fields, `--batch` right-hand sides solved together.  The plain FP64 BiCGStab
-solve of the same system is timed beside it.
+ensemble (stored 12-real), antiperiodic in t.  `--batch` right-hand sides are
+solved together to a 1e-10 relative true (FP64) residual by BiCGStab with
+reliable updates (iterations on FP16-storage / FP32-arithmetic fields, FP64
+solution and true residual; `--solver richardson` selects QPhiX's
+InvRichardsonMultiPrec instead, and the other one is timed beside it).  The
+plain FP64 BiCGStab solve of the same system is timed as well.
 
 value  = solves/s with the right-hand sides resident in HBM
 e2e    = solves/s through the C ABI with host buffers: pinned host -> device
@@ -53,6 +54,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--inner", default="f16", choices=["f16", "bf16", "f32"])
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--solver", default="ru", choices=["ru", "richardson"],
+                    help="ru: BiCGStab with reliable updates; richardson: InvRichardsonMultiPrec")
+    ap.add_argument("--delta", type=float, default=0.1)
     return ap.parse_args()
 
 
@@ -172,10 +176,12 @@ def run_reference(args, rank, world):
 METRIC = "Clover solves/s @1e-10 mixed vs FP64 plain, 1 B200; Dslash HBM GB/s; p99 ms"
 
 
-def config_dict(batch, inner):
+def config_dict(batch, inner, solver="ru"):
+    how = ("BiCGStab with reliable updates (FP64 true residual / solution, iterations in "
+           f"{inner} storage + FP32 arithmetic)" if solver == "ru" else
+           f"InvRichardsonMultiPrec (FP64 outer, BiCGStab inner in {inner} storage + FP32 arithmetic)")
     return {"workload": ("clover even-odd 16^3x32, kappa=0.1360, csw=1.0, links exp(i 0.3 H) "
-                         "(H GUE) 12-real, antiperiodic t; InvRichardsonMultiPrec FP64 outer to 1e-10 "
-                         f"true residual, inner BiCGStab {inner}-storage/FP32-compute"),
+                         f"(H GUE) 12-real, antiperiodic t; {how} to 1e-10 true residual"),
             "rhs_per_step": batch, "lattice": list(DIMS), "kappa": KAPPA, "csw": CSW,
             "l2": "flushed (256 MiB write) before every step"}
 
@@ -216,8 +222,10 @@ def main():
     Ai = lat.clover(args.inner).upload(inputs["clov_odd"])
     Aii = lat.clover(args.inner).upload(inputs["invclov_even"])
     Mi = api.EvenOddCloverOperator(ui, Ai, Aii)
-    solver = api.InvRichardsonMultiPrec(M64, Mi, "bicgstab", delta=DELTA, max_iters=100,
-                                        inner_max_iters=5000)
+    rich = api.InvRichardsonMultiPrec(M64, Mi, "bicgstab", delta=args.delta, max_iters=100,
+                                      inner_max_iters=5000)
+    ru = api.InvBiCGStabMixed(M64, Mi, delta=args.delta, max_iters=20000)
+    solver = ru if args.solver == "ru" else rich
     b_res = lat.spinor("f64", B).upload(inputs["rhs"])    # resident sources
     b = lat.spinor("f64", B)
     x = lat.spinor("f64", B)
@@ -305,6 +313,25 @@ def main():
     e2e_value = world * B * args.steps / e2e_total
     bytes_io = int(h_rhs.numel() * 8)
 
+    # ---- the other mixed solver, for comparison --------------------------------
+    other = rich if args.solver == "ru" else ru
+    ots = []
+    for _ in range(2):
+        with torch.cuda.stream(stream):
+            flush.fill_(1)
+        api.copy(b, b_res)
+        api.zero(x)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        oinf = other(x, b, RSD)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ots.append(e0.elapsed_time(e1))
+    other_line = {"solver": "richardson" if args.solver == "ru" else "ru",
+                  "solves_per_s": round(B * 1e3 / min(ots), 3),
+                  "worst_true_rel_resid": max(i["true_rel_resid"] for i in oinf),
+                  "iters": oinf[0]["n_iters"], "mv_apps": oinf[0]["mv_apps"]}
+
     # ---- plain FP64 BiCGStab beside it ------------------------------------------
     fp64 = None
     if not args.no_fp64:
@@ -390,7 +417,7 @@ def main():
             "ms_per_step": round(total_s * 1e3 / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": f"mixed: f64 outer, f32 arithmetic on {args.inner} storage inner",
-            "data": "synthetic (seeded)", "config": config_dict(B, args.inner),
+            "data": "synthetic (seeded)", "config": config_dict(B, args.inner, args.solver),
             "e2e": {"value": round(e2e_value, 3), "unit": "solves/s", "h2d_bytes_per_step": bytes_io,
                     "d2h_bytes_per_step": bytes_io},
             "roofline": roof, "roofline_large_lattice": roof_big,
@@ -399,8 +426,10 @@ def main():
             "p50_ms_per_step": round(p[len(p) // 2], 3), "p99_ms_per_step": round(p[min(len(p) - 1, int(0.99 * len(p)))], 3),
             "fp64_plain": fp64,
             "mixed_vs_fp64_solves_ratio": (round(value / world / fp64["solves_per_s"], 3) if fp64 else None),
-            "solver": {"outer_iters": outer_iters, "mv_apps": mv_apps, "worst_true_rel_resid": worst_resid,
-                       "all_converged": converged},
+            "solver": {"kind": "bicgstab_reliable_update" if args.solver == "ru" else "richardson_bicgstab",
+                       "delta": args.delta, "iters": outer_iters, "mv_apps": mv_apps,
+                       "worst_true_rel_resid": worst_resid, "all_converged": converged},
+            "other_mixed_solver": other_line,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -1,0 +1,70 @@
+// Drop-in solver interfaces (reference: include/qphix/abs_solver.h:13-267):
+// ResiduumType, AbstractSolver and AbstractMultiSolver with the same
+// operator() signatures.  The concrete solvers run on the device operator of
+// the EvenOddLinearOperator they are given.
+#pragma once
+
+#include <cmath>
+
+#include "qphix/linearOp.h"
+
+namespace QPhiX
+{
+
+enum ResiduumType { ABSOLUTE, RELATIVE, INVALID };
+
+template <typename FT, int V, int S, bool compress12, int num_flav = 1>
+class AbstractSolver
+{
+ public:
+  virtual ~AbstractSolver() {}
+  typedef typename Geometry<FT, V, S, compress12>::FourSpinorBlock Spinor;
+
+  virtual void operator()(Spinor *const x[num_flav], const Spinor *const rhs[num_flav], const double RsdTarget,
+                          int &niters, double &rsd_sq_final, unsigned long &site_flops, unsigned long &mv_apps,
+                          int isign, bool verboseP, int cb = 1, ResiduumType residType = RELATIVE) const = 0;
+
+  void operator()(Spinor *x, const Spinor *rhs, const double RsdTarget, int &niters, double &rsd_sq_final,
+                  unsigned long &site_flops, unsigned long &mv_apps, int isign, bool verboseP, int cb = 1,
+                  ResiduumType residType = RELATIVE) const
+  {
+    Spinor *xa[1] = {x};
+    const Spinor *ra[1] = {rhs};
+    (*this)(xa, ra, RsdTarget, niters, rsd_sq_final, site_flops, mv_apps, isign, verboseP, cb, residType);
+  }
+
+  virtual Geometry<FT, V, S, compress12> &getGeometry() = 0;
+
+  // device description of this solver, used by InvRichardsonMultiPrec for
+  // its inner solve (not part of QPhiX's interface)
+  virtual int gpu_solver_kind() const = 0;
+  virtual qphix_gpu_eo_op gpu_solver_op() const = 0;
+  virtual int gpu_max_iters() const = 0;
+};
+
+template <typename FT, int V, int S, bool compress12, int num_flav = 1>
+class AbstractMultiSolver
+{
+ public:
+  virtual ~AbstractMultiSolver() {}
+  typedef typename Geometry<FT, V, S, compress12>::FourSpinorBlock Spinor;
+
+  virtual void operator()(Spinor **x, const Spinor *rhs, const int n_shift, const double *shifts,
+                          const double *RsdTarget, int &niters, double *rsd_sq_final, unsigned long &site_flops,
+                          unsigned long &mv_apps, int isign, bool verboseP, int cb = 1) const = 0;
+  virtual Geometry<FT, V, S, compress12> &getGeometry() = 0;
+};
+
+namespace gpu
+{
+// relative target for a possibly absolute request
+inline double relative_target(qphix_gpu_field rhs, double rsd, ResiduumType t)
+{
+  if (t == RELATIVE) return rsd;
+  double n2 = 0;
+  check(qphix_gpu_blas_norm2(rhs, &n2), "norm2");
+  return n2 > 0 ? rsd / std::sqrt(n2) : rsd;
+}
+}  // namespace gpu
+
+}  // namespace QPhiX

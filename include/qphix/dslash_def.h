@@ -1,0 +1,235 @@
+// Drop-in Dslash family: Dslash (reference: include/qphix/dslash_def.h:27-58),
+// ClovDslash (clover_dslash_def.h:24-53), TMDslash (tm_dslash_def.h:23-49)
+// and TMClovDslash (tm_clov_dslash_def.h:30-66), same constructors and
+// member functions.  Each call moves its host arrays (QPhiX layout) to the
+// device, runs one sm_100a kernel and moves the result back; `u` is the
+// gauge array of the target checkerboard, as in QPhiX (its eight links per
+// site carry both hop directions).
+#pragma once
+
+#include "qphix/geometry.h"
+
+namespace QPhiX
+{
+
+namespace gpu
+{
+// device gauge field from one QPhiX checkerboard array (forward + back links)
+template <typename G>
+Field upload_gauge_cb(const G &geom, const typename G::SU3MatrixBlock *u, int cb)
+{
+  Field f(geom.lattice(), QPHIX_GPU_GAUGE, G::device_prec(), G::compress12 ? 12 : 18);
+  auto l = geom.host_layout();
+  check(qphix_gpu_field_upload(f.get(), u, &l, 2 + cb, -1), "gauge upload");
+  return f;
+}
+}  // namespace gpu
+
+template <typename FT, int veclen, int soalen, bool compress12>
+class Dslash
+{
+ public:
+  typedef Geometry<FT, veclen, soalen, compress12> Geom;
+  typedef typename Geom::SU3MatrixBlock SU3MatrixBlock;
+  typedef typename Geom::FourSpinorBlock FourSpinorBlock;
+  typedef typename Geom::TwoSpinorBlock TwoSpinorBlock;
+
+  Dslash(Geom *geom_, double t_boundary_, double aniso_coeff_S_, double aniso_coeff_T_, bool use_tbc_[4] = nullptr,
+         double tbc_phases_[4][2] = nullptr)
+      : s(geom_), p(gpu::make_params(QPHIX_GPU_WILSON, t_boundary_, aniso_coeff_S_, aniso_coeff_T_, use_tbc_,
+                                     tbc_phases_))
+  {
+  }
+
+  void dslash(FourSpinorBlock *res, const FourSpinorBlock *psi, const SU3MatrixBlock *u, int isign, int cb)
+  {
+    auto g = gpu::upload_gauge_cb(*s, u, cb);
+    auto in = s->upload_spinor(psi);
+    gpu::Field out(s->lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
+    gpu::check(qphix_gpu_dslash(&p, out.get(), in.get(), g.get(), nullptr, nullptr, isign, cb), "dslash");
+    s->download_spinor(out, res);
+  }
+
+  void dslashAChiMinusBDPsi(FourSpinorBlock *res, const FourSpinorBlock *psi, const FourSpinorBlock *chi,
+                            const SU3MatrixBlock *u, double alpha, double beta, int isign, int cb)
+  {
+    auto g = gpu::upload_gauge_cb(*s, u, cb);
+    auto in = s->upload_spinor(psi);
+    auto x = s->upload_spinor(chi);
+    gpu::Field out(s->lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&p, out.get(), in.get(), x.get(), g.get(), nullptr, alpha, beta, isign,
+                                           cb, 1.0),
+               "dslashAChiMinusBDPsi");
+    s->download_spinor(out, res);
+  }
+
+  void dslashDir(FourSpinorBlock *res, const FourSpinorBlock *psi, const SU3MatrixBlock *u, int cb, int dir)
+  {
+    auto g = gpu::upload_gauge_cb(*s, u, cb);
+    auto in = s->upload_spinor(psi);
+    gpu::Field out(s->lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
+    gpu::check(qphix_gpu_dslash_dir(&p, out.get(), in.get(), g.get(), cb, dir), "dslashDir");
+    s->download_spinor(out, res);
+  }
+
+  void free(void *) {}
+  Geom &getGeometry() { return *s; }
+
+ protected:
+  Geom *s;
+  qphix_gpu_op_params p;
+};
+
+template <typename FT, int veclen, int soalen, bool compress12>
+class ClovDslash : public Dslash<FT, veclen, soalen, compress12>
+{
+ public:
+  typedef Dslash<FT, veclen, soalen, compress12> Base;
+  typedef typename Base::Geom Geom;
+  typedef typename Geom::SU3MatrixBlock SU3MatrixBlock;
+  typedef typename Geom::FourSpinorBlock FourSpinorBlock;
+  typedef typename Geom::CloverBlock CloverBlock;
+
+  ClovDslash(Geom *geom_, double t_boundary_, double dslash_aniso_s_, double dslash_aniso_t_,
+             bool use_tbc_[4] = nullptr, double tbc_phases_[4][2] = nullptr, double const prec_mass_rho = 0.0)
+      : Base(geom_, t_boundary_, dslash_aniso_s_, dslash_aniso_t_, use_tbc_, tbc_phases_)
+  {
+    this->p.kind = QPHIX_GPU_CLOVER_OP;
+    this->p.prec_mass_rho = prec_mass_rho;
+  }
+
+  // res = A^-1 D psi
+  void dslash(FourSpinorBlock *res, const FourSpinorBlock *psi, const SU3MatrixBlock *u, const CloverBlock *invclov,
+              int isign, int cb)
+  {
+    Geom &s = *this->s;
+    auto g = gpu::upload_gauge_cb(s, u, cb);
+    auto c = s.upload_clover(invclov);
+    auto in = s.upload_spinor(psi);
+    gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
+    gpu::check(qphix_gpu_dslash(&this->p, out.get(), in.get(), g.get(), c.get(), nullptr, isign, cb), "clover dslash");
+    s.download_spinor(out, res);
+  }
+
+  // res = A chi + i rho isign g5 chi - beta D psi
+  void dslashAChiMinusBDPsi(FourSpinorBlock *res, const FourSpinorBlock *psi, const FourSpinorBlock *chi,
+                            const SU3MatrixBlock *u, const CloverBlock *clov, const double beta, int isign, int cb)
+  {
+    Geom &s = *this->s;
+    auto g = gpu::upload_gauge_cb(s, u, cb);
+    auto c = s.upload_clover(clov);
+    auto in = s.upload_spinor(psi);
+    auto x = s.upload_spinor(chi);
+    gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&this->p, out.get(), in.get(), x.get(), g.get(), c.get(), 0.0, beta, isign,
+                                           cb, 1.0),
+               "clover dslashAChiMinusBDPsi");
+    s.download_spinor(out, res);
+  }
+
+  void clovMult(FourSpinorBlock *res, const FourSpinorBlock *chi, const CloverBlock *clov)
+  {
+    Geom &s = *this->s;
+    auto c = s.upload_clover(clov);
+    auto x = s.upload_spinor(chi);
+    gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
+    gpu::check(qphix_gpu_clover_apply(out.get(), x.get(), c.get()), "clovMult");
+    s.download_spinor(out, res);
+  }
+};
+
+template <typename FT, int veclen, int soalen, bool compress12>
+class TMDslash : public Dslash<FT, veclen, soalen, compress12>
+{
+ public:
+  typedef Dslash<FT, veclen, soalen, compress12> Base;
+  typedef typename Base::Geom Geom;
+  typedef typename Geom::SU3MatrixBlock SU3MatrixBlock;
+  typedef typename Geom::FourSpinorBlock FourSpinorBlock;
+
+  TMDslash(Geom *geom_, double t_boundary_, double aniso_coeff_S_, double aniso_coeff_T_, double Mass_,
+           double TwistedMass_, bool use_tbc_[4] = nullptr, double tbc_phases_[4][2] = nullptr)
+      : Base(geom_, t_boundary_, aniso_coeff_S_, aniso_coeff_T_, use_tbc_, tbc_phases_)
+  {
+    this->p.kind = QPHIX_GPU_TM;
+    this->p.mass = Mass_;
+    this->p.twisted_mass = TwistedMass_;
+  }
+
+  // res = (alpha - i mu isign g5)/(alpha^2 + mu^2) D psi
+  void dslash(FourSpinorBlock *res, const FourSpinorBlock *psi, const SU3MatrixBlock *u, int isign, int cb)
+  {
+    Base::dslash(res, psi, u, isign, cb);
+  }
+
+  // res = alpha (1 + i isign musign mu/(4+m) g5) chi - beta D psi
+  void dslashAChiMinusBDPsi(FourSpinorBlock *res, const FourSpinorBlock *psi, const FourSpinorBlock *chi,
+                            const SU3MatrixBlock *u, double alpha, double beta, int isign, int cb,
+                            const double musign = 1.0)
+  {
+    Geom &s = *this->s;
+    auto g = gpu::upload_gauge_cb(s, u, cb);
+    auto in = s.upload_spinor(psi);
+    auto x = s.upload_spinor(chi);
+    gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&this->p, out.get(), in.get(), x.get(), g.get(), nullptr, alpha, beta,
+                                           isign, cb, musign),
+               "tm dslashAChiMinusBDPsi");
+    s.download_spinor(out, res);
+  }
+};
+
+template <typename FT, int veclen, int soalen, bool compress12>
+class TMClovDslash : public Dslash<FT, veclen, soalen, compress12>
+{
+ public:
+  typedef Dslash<FT, veclen, soalen, compress12> Base;
+  typedef typename Base::Geom Geom;
+  typedef typename Geom::SU3MatrixBlock SU3MatrixBlock;
+  typedef typename Geom::FourSpinorBlock FourSpinorBlock;
+  typedef typename Geom::CloverBlock CloverBlock;
+  typedef typename Geom::FullCloverBlock FullCloverBlock;
+
+  TMClovDslash(Geom *geom_, double t_boundary_, double dslash_aniso_s_, double dslash_aniso_t_,
+               bool use_tbc_[4] = nullptr, double tbc_phases_[4][2] = nullptr, double const prec_mass_rho = 0.0)
+      : Base(geom_, t_boundary_, dslash_aniso_s_, dslash_aniso_t_, use_tbc_, tbc_phases_)
+  {
+    this->p.kind = QPHIX_GPU_TMCLOVER;
+    this->p.prec_mass_rho = prec_mass_rho;
+  }
+
+  // res = invclov[isign == 1 ? 0 : 1] D psi (flavour 0; tm_clov_dslash_body.h:352)
+  void dslash(FourSpinorBlock *res, const FourSpinorBlock *psi, const SU3MatrixBlock *u,
+              const FullCloverBlock *const invclov[2], int isign, int cb, int fl = 0)
+  {
+    if (fl != 0) throw std::invalid_argument("TMClovDslash: only flavour 0 (degenerate) is supported");
+    Geom &s = *this->s;
+    auto g = gpu::upload_gauge_cb(s, u, cb);
+    auto f0 = s.upload_full_clover(invclov[0]);
+    auto f1 = s.upload_full_clover(invclov[1]);
+    auto in = s.upload_spinor(psi);
+    gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
+    gpu::check(qphix_gpu_dslash(&this->p, out.get(), in.get(), g.get(), f0.get(), f1.get(), isign, cb),
+               "tm clover dslash");
+    s.download_spinor(out, res);
+  }
+
+  void dslashAChiMinusBDPsi(FourSpinorBlock *res, const FourSpinorBlock *psi, const FourSpinorBlock *chi,
+                            const SU3MatrixBlock *u, const CloverBlock *clov, const double beta, int isign, int cb,
+                            int fl = 0)
+  {
+    if (fl != 0) throw std::invalid_argument("TMClovDslash: only flavour 0 (degenerate) is supported");
+    Geom &s = *this->s;
+    auto g = gpu::upload_gauge_cb(s, u, cb);
+    auto c = s.upload_clover(clov);
+    auto in = s.upload_spinor(psi);
+    auto x = s.upload_spinor(chi);
+    gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&this->p, out.get(), in.get(), x.get(), g.get(), c.get(), 0.0, beta, isign,
+                                           cb, 1.0),
+               "tm clover dslashAChiMinusBDPsi");
+    s.download_spinor(out, res);
+  }
+};
+
+}  // namespace QPhiX

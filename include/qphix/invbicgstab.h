@@ -1,0 +1,3 @@
+// InvBiCGStab lives with the other single-shift solvers.
+#pragma once
+#include "qphix/invcg.h"

@@ -119,8 +119,13 @@ int qphix_gpu_field_create(qphix_gpu_lattice lat, int kind, int prec, int recon,
                            qphix_gpu_field *out);
 int qphix_gpu_field_destroy(qphix_gpu_field f);
 int qphix_gpu_field_bytes(qphix_gpu_field f, size_t *bytes);
-/* cb: gauge fields with a qphix layout carry one checkerboard per host array
- * (pass 0 or 1); canonical gauge arrays carry both (pass -1).
+/* cb: canonical gauge arrays carry both checkerboards (pass -1).  A qphix
+ * gauge array belongs to one checkerboard and holds 8 links per site:
+ * pass 0 / 1 to take the forward links U_mu(x) of that checkerboard (upload
+ * both arrays to fill the field), or 2 / 3 to fill the whole field from the
+ * one array of checkerboard cb - 2 (its back links U_mu(x - mu) supply the
+ * other checkerboard's forward links) -- what Dslash::dslash(.., u[cb], cb)
+ * needs.
  * rhs: index of one right-hand side to transfer, or -1 for all. */
 int qphix_gpu_field_upload(qphix_gpu_field f, const void *host, const qphix_gpu_host_layout *layout,
                            int cb, int rhs);
@@ -185,9 +190,27 @@ int qphix_gpu_solve_bicgstab(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_fi
                              int max_iters, int isign, int cb, qphix_gpu_solve_info *info);
 int qphix_gpu_solve_mr(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target,
                        int max_iters, double omega, int isign, int cb, qphix_gpu_solve_info *info);
+/* InvMRSmoother::operator() (invmr.h:302-354): exactly n_iters MR
+ * iterations with over-relaxation omega, no residual test (rsd_sq_final is
+ * reported as -1, like the reference). */
+int qphix_gpu_solve_mr_smoother(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs, int n_iters,
+                                double omega, int isign, int cb, qphix_gpu_solve_info *info);
 int qphix_gpu_solve_mshift_cg(qphix_gpu_eo_op op, qphix_gpu_field *x, qphix_gpu_field rhs, int n_shift,
                               const double *shifts, const double *rsd_target, int max_iters, int isign,
                               int cb, int *n_iters, double *rsd_sq_final, unsigned long *mv_apps);
+/* BiCGStab with reliable updates.  No counterpart in the reference (its
+ * mixed-precision solver is InvRichardsonMultiPrec, which restarts the inner
+ * Krylov solve at every outer step).  The iteration runs on op_low (fields in
+ * 16-bit or FP32 storage, FP32 arithmetic); whenever a right-hand side's
+ * iterated residual has dropped by `delta` since its last update, the
+ * low-precision solution increment is added to x (FP64) and r is replaced by
+ * the true residual b - M x computed with op, without restarting the Krylov
+ * space.  Convergence (rsd_target, relative) is decided on the true
+ * residual.  info: n_iters = low-precision iterations, site_flops = number
+ * of reliable updates, rsd_sq_final = |b - M x|^2. */
+int qphix_gpu_solve_bicgstab_mixed(qphix_gpu_eo_op op, qphix_gpu_eo_op op_low, qphix_gpu_field x,
+                                   qphix_gpu_field rhs, double rsd_target, double delta, int max_iters, int isign,
+                                   int cb, qphix_gpu_solve_info *info);
 int qphix_gpu_solve_richardson(qphix_gpu_eo_op op_outer, qphix_gpu_eo_op op_inner, int inner_solver,
                                qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target, double delta,
                                int max_iters, int inner_max_iters, int isign, int cb,

@@ -68,8 +68,10 @@ _SIGS = {
     "qphix_gpu_solve_cg": ([P, P, P, D, I_, I_, I_, C.POINTER(SolveInfo)], I_),
     "qphix_gpu_solve_bicgstab": ([P, P, P, D, I_, I_, I_, C.POINTER(SolveInfo)], I_),
     "qphix_gpu_solve_mr": ([P, P, P, D, I_, D, I_, I_, C.POINTER(SolveInfo)], I_),
+    "qphix_gpu_solve_mr_smoother": ([P, P, P, I_, D, I_, I_, C.POINTER(SolveInfo)], I_),
     "qphix_gpu_solve_mshift_cg": ([P, PP, P, I_, P, P, I_, I_, I_, C.POINTER(C.c_int), P,
                                    C.POINTER(C.c_ulong)], I_),
+    "qphix_gpu_solve_bicgstab_mixed": ([P, P, P, P, D, D, I_, I_, I_, C.POINTER(SolveInfo)], I_),
     "qphix_gpu_solve_richardson": ([P, P, I_, P, P, D, D, I_, I_, I_, I_, C.POINTER(SolveInfo)], I_),
     "qphix_gpu_blas_norm2": ([P, P], I_),
     "qphix_gpu_blas_norm2_noalloc": ([P, P], I_),

@@ -392,6 +392,19 @@ class InvMR:
         return _as_dicts(inf)
 
 
+class InvMRSmoother:
+    """include/qphix/invmr.h:302-354: a fixed number of MR iterations"""
+
+    def __init__(self, M, max_iters, omega=1.0):
+        self.M, self.max_iters, self.omega = M, max_iters, omega
+
+    def __call__(self, x, rhs, rsd_target=0.0, isign=1, cb=1):
+        inf = _infos(x.nrhs)
+        _solve_rc(L._lib.qphix_gpu_solve_mr_smoother(self.M.h, x.h, rhs.h, self.max_iters, self.omega,
+                                                     isign, cb, inf))
+        return _as_dicts(inf)
+
+
 class InvRichardsonMultiPrec:
     """include/qphix/inv_richardson_multiprec.h:22-42 (inner solver on op_inner)"""
 
@@ -408,6 +421,20 @@ class InvRichardsonMultiPrec:
         _solve_rc(L._lib.qphix_gpu_solve_richardson(self.Mo.h, self.Mi.h, self.inner, x.h, rhs.h,
                                                     rsd_target, self.delta, self.max_iters,
                                                     self.inner_max, isign, cb, inf))
+        return _as_dicts(inf)
+
+
+class InvBiCGStabMixed:
+    """BiCGStab with reliable updates: iterations on M_low, true residuals and
+    the solution on M (no counterpart in the reference)."""
+
+    def __init__(self, M, M_low, delta=0.1, max_iters=10000):
+        self.M, self.Ml, self.delta, self.max_iters = M, M_low, delta, max_iters
+
+    def __call__(self, x, rhs, rsd_target, isign=1, cb=1):
+        inf = _infos(x.nrhs)
+        _solve_rc(L._lib.qphix_gpu_solve_bicgstab_mixed(self.M.h, self.Ml.h, x.h, rhs.h, rsd_target,
+                                                        self.delta, self.max_iters, isign, cb, inf))
         return _as_dicts(inf)
 
 

@@ -54,22 +54,22 @@ void launch_blas(int prec, const BlasArgs &a, dim3 grid, cudaStream_t st)
 }
 
 template <typename P>
-static void conv_from(int pdst, int vh, SpinorArg src, SpinorArg dst, Coef scale, SolverState *state, dim3 grid,
-                      cudaStream_t st)
+static void conv_from(int pdst, int vh, SpinorArg src, SpinorArg dst, Coef scale, SolverState *state, int acc,
+                      dim3 grid, cudaStream_t st)
 {
   switch (pdst) {
-  case PREC_F64: convert_kernel<P, F64><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state); break;
-  case PREC_F32: convert_kernel<P, F32><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state); break;
-  case PREC_F16: convert_kernel<P, F16><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state); break;
-  case PREC_BF16: convert_kernel<P, BF16><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state); break;
+  case PREC_F64: convert_kernel<P, F64><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
+  case PREC_F32: convert_kernel<P, F32><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
+  case PREC_F16: convert_kernel<P, F16><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
+  case PREC_BF16: convert_kernel<P, BF16><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
   default: throw Error(QPHIX_GPU_EINVAL, "bad precision");
   }
 }
 
 void launch_convert(int pdst, int psrc, int vh, SpinorArg src, SpinorArg dst, Coef scale, SolverState *state,
-                    dim3 grid, cudaStream_t st)
+                    dim3 grid, cudaStream_t st, int accumulate)
 {
-  QPX_PREC_SWITCH(psrc, (conv_from<P>(pdst, vh, src, dst, scale, state, grid, st)));
+  QPX_PREC_SWITCH(psrc, (conv_from<P>(pdst, vh, src, dst, scale, state, accumulate, grid, st)));
 }
 
 void launch_spinor_in(int prec, Geom g, HostLayout L, const void *host, SpinorArg f, int nrhs, dim3 grid,
@@ -85,10 +85,10 @@ void launch_spinor_out(int prec, Geom g, HostLayout L, void *host, SpinorArg f, 
 }
 
 void launch_gauge_in(int prec, Geom g, HostLayout L, const void *host, void *dev, long long stride,
-                     long long slab_bytes, int vpc, int recon, int cb, dim3 grid, cudaStream_t st)
+                     long long slab_bytes, int vpc, int recon, int cb, int back, dim3 grid, cudaStream_t st)
 {
   QPX_PREC_SWITCH(prec, (gauge_in_kernel<P><<<grid, QPX_BLOCK, 0, st>>>(g, L, host, dev, stride, slab_bytes, vpc,
-                                                                          recon, cb)));
+                                                                          recon, cb, back)));
 }
 
 void launch_clover_in(int prec, Geom g, HostLayout L, const void *host, void *dev, long long stride, int vpc,
@@ -101,6 +101,11 @@ void launch_clover_out(int prec, Geom g, void *host, const void *dev, long long 
                        dim3 grid, cudaStream_t st)
 {
   QPX_PREC_SWITCH(prec, (clover_out_kernel<P><<<grid, QPX_BLOCK, 0, st>>>(g, host, dev, stride, vpc, nr)));
+}
+
+void launch_mshift(int prec, const MShiftArgs &a, dim3 grid, cudaStream_t st)
+{
+  QPX_PREC_SWITCH(prec, (mshift_update_kernel<P><<<grid, QPX_BLOCK, 0, st>>>(a)));
 }
 
 void launch_dslash_f64(int recon, int epi, int achi, int R, const DslashArgs &a, dim3 grid, cudaStream_t st);

@@ -43,6 +43,7 @@ static int guard(F &&f)
 static int nblocks_for(long long n) { return (int)((n + QPX_BLOCK - 1) / QPX_BLOCK); }
 
 static std::atomic<unsigned long long> g_launches{0};
+static std::atomic<unsigned long long> g_serial{1};
 
 static void check_launch()
 {
@@ -98,7 +99,9 @@ extern "C" int qphix_gpu_lattice_create(const int latt[4], qphix_gpu_lattice *ou
       L->stride = (L->vh + 63) / 64 * 64;
       QPX_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
       L->owns_stream = true;
-      L->partials_len = (size_t)nblocks_for(L->vh) * QPX_MAX_RHS * QPX_MAX_RED;
+      // per-block partials, plus 2 x QPX_MAX_RHS doubles at the end for the
+      // Richardson per-rhs scale factors
+      L->partials_len = (size_t)nblocks_for(L->vh) * QPX_MAX_RHS * QPX_MAX_RED + 2 * QPX_MAX_RHS;
       QPX_CUDA(cudaMalloc(&L->partials, L->partials_len * sizeof(double)));
       QPX_CUDA(cudaMalloc(&L->ticket, 64 * sizeof(unsigned int)));
       QPX_CUDA(cudaMemset(L->ticket, 0, 64 * sizeof(unsigned int)));
@@ -121,6 +124,12 @@ static void lattice_release(qphix_gpu_lattice_s *L)
   if (!L) return;
   if (--L->refs > 0) return;
   if (L->stream) cudaStreamSynchronize(L->stream);
+  for (auto &kv : L->graphs) cudaGraphExecDestroy(kv.second);
+  for (auto *f : L->pool_all) {
+    cudaFree(f->data);
+    cudaFree(f->norm);
+    delete f;
+  }
   cudaFree(L->partials);
   cudaFree(L->ticket);
   cudaFree(L->result);
@@ -184,6 +193,7 @@ extern "C" int qphix_gpu_field_create(qphix_gpu_lattice L, int kind, int prec, i
     QPX_REQUIRE(prec >= PREC_F64 && prec <= PREC_BF16, "bad precision");
     auto *f = new qphix_gpu_field_s();
     f->lat = L;
+    f->serial = g_serial++;
     L->refs++;
     f->kind = kind;
     f->prec = prec;
@@ -344,12 +354,17 @@ extern "C" int qphix_gpu_field_upload(qphix_gpu_field f, const void *host, const
       if (L.kind == HOST_CANONICAL) {
         QPX_REQUIRE(cb == -1, "canonical gauge arrays hold both checkerboards (cb = -1)");
         for (int c = 0; c < 2; c++)
-          launch_gauge_in(f->prec, g, L, st, f->data, lat->stride, slab, f->spec.vpc, f->recon, c,
+          launch_gauge_in(f->prec, g, L, st, f->data, lat->stride, slab, f->spec.vpc, f->recon, c, 0,
                           dim3(nblocks_for(lat->vh), 4), lat->stream);
       } else {
-        QPX_REQUIRE(cb == 0 || cb == 1, "qphix gauge arrays hold one checkerboard (cb = 0 or 1)");
-        launch_gauge_in(f->prec, g, L, st, f->data, lat->stride, slab, f->spec.vpc, f->recon, cb,
+        QPX_REQUIRE(cb >= 0 && cb <= 3, "qphix gauge arrays: cb = 0/1 (forward links of that checkerboard) "
+                                        "or 2/3 (all eight links of checkerboard cb - 2)");
+        int c0 = cb & 1;
+        launch_gauge_in(f->prec, g, L, st, f->data, lat->stride, slab, f->spec.vpc, f->recon, c0, 0,
                         dim3(nblocks_for(lat->vh), 4), lat->stream);
+        if (cb >= 2)
+          launch_gauge_in(f->prec, g, L, st, f->data, lat->stride, slab, f->spec.vpc, f->recon, c0, 1,
+                          dim3(nblocks_for(lat->vh), 4), lat->stream);
       }
       break;
     }
@@ -391,11 +406,12 @@ extern "C" int qphix_gpu_field_download(qphix_gpu_field f, void *host, const qph
   });
 }
 
-static void convert_field(qphix_gpu_field_s *dst, qphix_gpu_field_s *src, Coef scale, SolverState *state)
+static void convert_field(qphix_gpu_field_s *dst, qphix_gpu_field_s *src, Coef scale, SolverState *state,
+                          int accumulate = 0)
 {
   auto *lat = src->lat;
   launch_convert(dst->prec, src->prec, (int)lat->vh, src->sarg(), dst->sarg(), scale, state,
-                 dim3(nblocks_for(lat->vh), src->nrhs), lat->stream);
+                 dim3(nblocks_for(lat->vh), src->nrhs), lat->stream, accumulate);
   check_launch();
 }
 
@@ -446,8 +462,11 @@ static int pick_tile(int prec, int nrhs)
     int R = atoi(force);
     if (R > 0 && nrhs % R == 0 && dslash_tile_ok(prec, R)) return R;
   }
-  for (int R : {4, 2, 1})
-    if (nrhs % R == 0 && dslash_tile_ok(prec, R)) return R;
+  // one right-hand side per thread: wider tiles keep R x 24 accumulators live
+  // and lose more to occupancy than they gain from link reuse (links of the
+  // other right-hand sides are re-read from L2); QPHIX_GPU_RHS_TILE overrides
+  (void)prec;
+  (void)nrhs;
   return 1;
 }
 
@@ -689,6 +708,7 @@ extern "C" int qphix_gpu_eo_op_create(const qphix_gpu_op_params *p, qphix_gpu_fi
     if (p->kind == QPHIX_GPU_CLOVER_OP) QPX_REQUIRE(clov && invclov, "clover operator needs clov and invclov");
     if (p->kind == QPHIX_GPU_TMCLOVER) QPX_REQUIRE(clov && finv0 && finv1, "tm clover operator needs clov, finv0/1");
     auto *op = new qphix_gpu_eo_op_s();
+    op->serial = g_serial++;
     op->p = *p;
     op->gauge = gauge;
     op->clov = clov;
@@ -907,16 +927,33 @@ extern "C" int qphix_gpu_blas_zero(qphix_gpu_field x)
 // ===========================================================================
 namespace {
 
-struct Tmp {  // scoped temporary spinor
+// scoped solver temporary taken from (and returned to) the lattice's pool;
+// pool fields are allocated once and carry no lattice reference
+struct Tmp {
   qphix_gpu_field f = nullptr;
-  Tmp(qphix_gpu_lattice_s *lat, int prec, int nrhs)
+  qphix_gpu_lattice_s *lat;
+  Tmp(qphix_gpu_lattice_s *l, int prec, int nrhs) : lat(l)
   {
+    for (size_t i = lat->pool_free.size(); i-- > 0;) {
+      auto *c = lat->pool_free[i];
+      if (c->prec == prec && c->nrhs == nrhs) {
+        f = c;
+        lat->pool_free.erase(lat->pool_free.begin() + i);
+        return;
+      }
+    }
     int rc = qphix_gpu_field_create(lat, QPHIX_GPU_SPINOR, prec, 0, nrhs, &f);
     if (rc) throw Error(rc, g_last_error);
+    lat->refs--;  // owned by the pool, freed with the lattice
+    lat->pool_all.push_back(f);
   }
-  ~Tmp() { qphix_gpu_field_destroy(f); }
+  ~Tmp() { lat->pool_free.push_back(f); }
+  Tmp(const Tmp &) = delete;
+  Tmp &operator=(const Tmp &) = delete;
   operator qphix_gpu_field_s *() const { return f; }
 };
+
+std::string fkey(const qphix_gpu_field_s *f) { return f ? std::to_string(f->serial) : std::string("-"); }
 
 // push the host copy of the solver state to the device
 void state_upload(qphix_gpu_lattice_s *lat)
@@ -942,14 +979,26 @@ SolverState &state_reset(qphix_gpu_lattice_s *lat, int nrhs, int max_iter)
 
 // Replays `step` (one solver iteration, kernels only) until the device raises
 // state->done.  The step is captured once into a CUDA graph.
+// `key` names everything the captured launches depend on (solver, operator
+// and field serial numbers, isign, cb); a graph captured under the same key
+// is replayed instead of captured again.
 template <typename Step>
-void run_iterations(qphix_gpu_lattice_s *lat, Step &&step, int max_iter)
+void run_iterations(qphix_gpu_lattice_s *lat, Step &&step, int max_iter, const std::string &key)
 {
   const int check = 8;
   bool use_graph = !env_flag("QPHIX_GPU_NO_GRAPH");
   cudaGraphExec_t exec = nullptr;
   unsigned long long nodes = 0;
-  if (use_graph) {
+  bool cached = false;
+  if (use_graph && !key.empty()) {
+    auto it = lat->graphs.find(key);
+    if (it != lat->graphs.end()) {
+      exec = it->second;
+      nodes = lat->graph_nodes[key];
+      cached = true;
+    }
+  }
+  if (use_graph && !cached) {
     cudaGraph_t graph = nullptr;
     unsigned long long before = g_launches.load();
     QPX_CUDA(cudaStreamBeginCapture(lat->stream, cudaStreamCaptureModeThreadLocal));
@@ -966,6 +1015,19 @@ void run_iterations(qphix_gpu_lattice_s *lat, Step &&step, int max_iter)
     cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
     cudaGraphDestroy(graph);
     if (e != cudaSuccess) throw Error(QPHIX_GPU_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    if (!key.empty()) {
+      if (lat->graph_order.size() >= 64) {  // bounded cache: drop the oldest
+        const std::string &old_key = lat->graph_order.front();
+        cudaGraphExecDestroy(lat->graphs[old_key]);
+        lat->graphs.erase(old_key);
+        lat->graph_nodes.erase(old_key);
+        lat->graph_order.erase(lat->graph_order.begin());
+      }
+      lat->graphs[key] = exec;
+      lat->graph_nodes[key] = nodes;
+      lat->graph_order.push_back(key);
+      cached = true;
+    }
   }
   int launched = 0;
   try {
@@ -985,10 +1047,10 @@ void run_iterations(qphix_gpu_lattice_s *lat, Step &&step, int max_iter)
       if (launched > max_iter + 2 * check) break;  // the device enforces max_iter; belt and braces
     }
   } catch (...) {
-    if (exec) cudaGraphExecDestroy(exec);
+    if (exec && !cached) cudaGraphExecDestroy(exec);
     throw;
   }
-  if (exec) QPX_CUDA(cudaGraphExecDestroy(exec));
+  if (exec && !cached) QPX_CUDA(cudaGraphExecDestroy(exec));
   state_download(lat);
 }
 
@@ -1058,7 +1120,7 @@ void true_residual(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_
 // ---------------------------------------------------------------------------
 // CG on M^dag M (include/qphix/invcg.h:88-456)
 void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs, const double *rsd,
-              int max_iters, int isign, int cb, qphix_gpu_solve_info *info)
+              int max_iters, int isign, int cb, qphix_gpu_solve_info *info, bool final_resid = true)
 {
   check_solver_fields(op, x, rhs);
   auto *lat = x->lat;
@@ -1122,13 +1184,15 @@ void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
       pu.state = ds;
       blas_launch(lat, prec, nr, pu);
     };
-    run_iterations(lat, step, max_iters + 1);
+    std::string key = "cg/" + std::to_string(op->serial) + "/" + fkey(x) + "/" + fkey(mp) + fkey(mmp) + fkey(r) +
+                      fkey(p) + "/" + std::to_string(isign) + std::to_string(cb);
+    run_iterations(lat, step, max_iters + 1, key);
     mv += 2ul * lat->h_state->iter;
   }
   // true residual (not counted in mv_apps: the reference's own recompute is
   // compiled out, include/qphix/invcg.h:342-403)
-  std::vector<double> abs2, rel;
-  true_residual(op, x, rhs, mmp, r, isign, cb, true, chi, abs2, rel);
+  std::vector<double> abs2(nr, -1.0), rel(nr, -1.0);
+  if (final_resid) true_residual(op, x, rhs, mmp, r, isign, cb, true, chi, abs2, rel);
   const SolverState &H = *lat->h_state;
   double secs = timer.stop();
   for (int i = 0; i < nr; i++) {
@@ -1145,7 +1209,7 @@ void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
 // ---------------------------------------------------------------------------
 // BiCGStab (include/qphix/invbicgstab.h:80-263)
 void solve_bicgstab(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs, const double *rsd,
-                    int max_iters, int isign, int cb, qphix_gpu_solve_info *info)
+                    int max_iters, int isign, int cb, qphix_gpu_solve_info *info, bool final_resid = true)
 {
   check_solver_fields(op, x, rhs);
   auto *lat = x->lat;
@@ -1240,11 +1304,13 @@ void solve_bicgstab(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field
       rx.state = ds;
       blas_launch(lat, prec, nr, rx);
     };
-    run_iterations(lat, step, max_iters);
+    std::string key = "bicg/" + std::to_string(op->serial) + "/" + fkey(x) + "/" + fkey(r0) + fkey(r) + fkey(p) +
+                      fkey(v) + fkey(t) + "/" + std::to_string(isign) + std::to_string(cb);
+    run_iterations(lat, step, max_iters, key);
     mv += 2ul * lat->h_state->iter;
   }
-  std::vector<double> abs2, rel;
-  true_residual(op, x, rhs, t, r, isign, cb, false, bn, abs2, rel);
+  std::vector<double> abs2(nr, -1.0), rel(nr, -1.0);
+  if (final_resid) true_residual(op, x, rhs, t, r, isign, cb, false, bn, abs2, rel);
   const SolverState &H = *lat->h_state;
   double secs = timer.stop();
   for (int i = 0; i < nr; i++) {
@@ -1263,8 +1329,11 @@ void solve_bicgstab(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field
 
 // ---------------------------------------------------------------------------
 // MR (include/qphix/invmr.h:62-210), terminating on the relative residual
+// terminate = false: InvMRSmoother, exactly max_iters iterations with no
+// residual test (include/qphix/invmr.h:302-354, terminateOnResiduum false)
 void solve_mr(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs, const double *rsd, int max_iters,
-              double omega, int isign, int cb, qphix_gpu_solve_info *info)
+              double omega, int isign, int cb, qphix_gpu_solve_info *info, bool final_resid = true,
+              bool terminate = true)
 {
   check_solver_fields(op, x, rhs);
   auto *lat = x->lat;
@@ -1292,10 +1361,10 @@ void solve_mr(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
   SolverState &S = state_reset(lat, nr, max_iters);
   bool all = true;
   for (int i = 0; i < nr; i++) {
-    S.v[S_RSD][i] = rsd[i] * rsd[i] * bn[i];
+    S.v[S_RSD][i] = terminate ? rsd[i] * rsd[i] * bn[i] : -1.0;  // |r|^2 > -1 always: no residual stop
     S.v[S_RNORM][i] = cp[i];
     S.v[S_AUX0][i] = omega;
-    if (cp[i] < S.v[S_RSD][i] || bn[i] == 0.0) {
+    if (terminate && (cp[i] < S.v[S_RSD][i] || bn[i] == 0.0)) {
       S.rhs_done[i] = 1;
       S.rhs_iter[i] = 0;
     }
@@ -1323,20 +1392,24 @@ void solve_mr(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
       u.state = ds;
       blas_launch(lat, prec, nr, u);
     };
-    run_iterations(lat, step, max_iters);
+    std::string key = "mr/" + std::to_string(op->serial) + "/" + fkey(x) + "/" + fkey(r) + fkey(Mr) + "/" +
+                      std::to_string(isign) + std::to_string(cb);
+    run_iterations(lat, step, max_iters, key);
     mv += lat->h_state->iter;
   }
-  std::vector<double> abs2, rel;
-  Tmp t(lat, prec, nr), rr(lat, prec, nr);
-  true_residual(op, x, rhs, t, rr, isign, cb, false, bn, abs2, rel);
+  std::vector<double> abs2(nr, -1.0), rel(nr, -1.0);
+  if (final_resid) {
+    Tmp t(lat, prec, nr), rr(lat, prec, nr);
+    true_residual(op, x, rhs, t, rr, isign, cb, false, bn, abs2, rel);
+  }
   const SolverState &H = *lat->h_state;
   double secs = timer.stop();
   for (int i = 0; i < nr; i++) {
     info[i].n_iters = H.rhs_done[i] ? H.rhs_iter[i] : H.iter;
-    info[i].rsd_sq_final = H.v[S_RNORM][i] / bn[i];
+    info[i].rsd_sq_final = terminate ? H.v[S_RNORM][i] / bn[i] : -1.0;
     info[i].mv_apps = mv;
     info[i].site_flops = (unsigned long)(24 + 8 * 12 + H.iter * (12 * 12 + 2 * 8 * 12 + 4 * 12));
-    info[i].status = H.rhs_done[i] ? 0 : 1;
+    info[i].status = (H.rhs_done[i] || !terminate) ? 0 : 1;
     info[i].true_rel_resid = rel[i];
     info[i].seconds = secs;
   }
@@ -1349,12 +1422,17 @@ void solve_richardson(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opi, int inner, 
                       int cb, qphix_gpu_solve_info *info)
 {
   check_solver_fields(op, x, rhs);
-  QPX_REQUIRE(opi && opi->gauge->lat == x->lat, "inner operator must live on the same lattice");
+  QPX_REQUIRE(opi, "null inner operator");
   auto *lat = x->lat;
+  // the inner operator may live on its own lattice object (QPhiX gives the
+  // inner solver its own Geometry) of the same shape; the two streams are
+  // ordered by synchronising at each hand-over
+  auto *lati = opi->gauge->lat;
+  for (int d = 0; d < 4; d++) QPX_REQUIRE(lati->dims[d] == lat->dims[d], "inner and outer lattices differ");
   const int nr = x->nrhs, prec = x->prec, iprec = opi->gauge->prec;
   Timer timer(lat);
   Tmp r(lat, prec, nr), tmp(lat, prec, nr), dx(lat, prec, nr);
-  Tmp rin(lat, iprec, nr), dxin(lat, iprec, nr);
+  Tmp rin(lati, iprec, nr), dxin(lati, iprec, nr);
   std::vector<double> bn = norm2_host(rhs);
   std::vector<double> rsd_t(nr);
   for (int i = 0; i < nr; i++) rsd_t[i] = rsd * rsd * bn[i];
@@ -1378,8 +1456,8 @@ void solve_richardson(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opi, int inner, 
   int iter = 0;
   // per-rhs scale factors live in the state's AUX slots between inner solves
   std::vector<double> scale_dn(nr), scale_up(nr), inner_rsd(nr);
-  double *d_scales = nullptr;
-  QPX_CUDA(cudaMalloc(&d_scales, sizeof(double) * 2 * QPX_MAX_RHS));
+  // the two per-rhs scale vectors live at the end of the reduction workspace
+  double *d_scales = lat->partials + lat->partials_len - 2 * QPX_MAX_RHS;
   std::vector<qphix_gpu_solve_info> ii(nr);
   try {
     if (!all) {
@@ -1398,19 +1476,21 @@ void solve_richardson(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opi, int inner, 
         }
         QPX_CUDA(cudaMemcpyAsync(d_scales, sc.data(), sizeof(double) * 2 * QPX_MAX_RHS, cudaMemcpyHostToDevice,
                                  lat->stream));
-        convert_field(rin, r, Coef{0, 0, d_scales, nullptr}, nullptr);
+        convert_field(rin, r, Coef{0, 0, d_scales, nullptr}, nullptr);  // on the outer stream
         BlasCall z;
         z.op = B_ZERO;
         z.x = dxin;
         blas_launch(lat, iprec, nr, z);
+        if (lati != lat) QPX_CUDA(cudaStreamSynchronize(lat->stream));
         if (inner == QPHIX_GPU_SOLVER_BICGSTAB)
-          solve_bicgstab(opi, dxin, rin, inner_rsd.data(), inner_max, isign, cb, ii.data());
+          solve_bicgstab(opi, dxin, rin, inner_rsd.data(), inner_max, isign, cb, ii.data(), false);
         else if (inner == QPHIX_GPU_SOLVER_MR)
-          solve_mr(opi, dxin, rin, inner_rsd.data(), inner_max, 1.0, isign, cb, ii.data());
+          solve_mr(opi, dxin, rin, inner_rsd.data(), inner_max, 1.0, isign, cb, ii.data(), false);
         else
-          solve_cg(opi, dxin, rin, inner_rsd.data(), inner_max, isign, cb, ii.data());
+          solve_cg(opi, dxin, rin, inner_rsd.data(), inner_max, isign, cb, ii.data(), false);
         mv_inner += ii[0].mv_apps;
-        convert_field(dx, dxin, Coef{0, 0, d_scales + QPX_MAX_RHS, nullptr}, nullptr);
+        convert_field(dx, dxin, Coef{0, 0, d_scales + QPX_MAX_RHS, nullptr}, nullptr);  // inner stream
+        if (lati != lat) QPX_CUDA(cudaStreamSynchronize(lati->stream));
         eo_apply(op, tmp, dx, isign, cb, ApplyOpts());
         mv_outer++;
         BlasCall u;
@@ -1432,10 +1512,8 @@ void solve_richardson(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opi, int inner, 
       }
     }
   } catch (...) {
-    cudaFree(d_scales);
     throw;
   }
-  cudaFree(d_scales);
   std::vector<double> abs2, rel;
   true_residual(op, x, rhs, tmp, r, isign, cb, false, bn, abs2, rel);
   mv_outer++;
@@ -1446,6 +1524,209 @@ void solve_richardson(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opi, int inner, 
     info[i].mv_apps = mv_outer + mv_inner;
     info[i].site_flops = 0;
     info[i].status = done[i] ? 0 : 1;
+    info[i].true_rel_resid = rel[i];
+    info[i].seconds = secs;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// BiCGStab with reliable updates (no counterpart in the reference): the
+// Krylov iteration runs on op_lo (16-bit or FP32 storage, FP32 arithmetic)
+// and is never restarted; the low-precision solution increment is folded into
+// the FP64 solution and r is replaced by the FP64 true residual b - M x
+// whenever a right-hand side's iterated residual has dropped by `delta`
+// since its last update (or reaches the target).  Convergence is decided on
+// the true residual only.
+void solve_bicgstab_mixed(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opl, qphix_gpu_field_s *x,
+                          qphix_gpu_field_s *rhs, double rsd, double delta, int max_iters, int isign, int cb,
+                          qphix_gpu_solve_info *info)
+{
+  check_solver_fields(op, x, rhs);
+  QPX_REQUIRE(opl, "null low-precision operator");
+  auto *lat = x->lat;
+  auto *latl = opl->gauge->lat;
+  for (int d = 0; d < 4; d++) QPX_REQUIRE(latl->dims[d] == lat->dims[d], "the two operators' lattices differ");
+  const int nr = x->nrhs, prec = x->prec, lp = opl->gauge->prec;
+  Timer timer(lat);
+  Tmp rh(lat, prec, nr), th(lat, prec, nr);
+  Tmp r0(latl, lp, nr), r(latl, lp, nr), p(latl, lp, nr), v(latl, lp, nr), t(latl, lp, nr), xl(latl, lp, nr);
+  auto sync_hi = [&] {
+    if (latl != lat) QPX_CUDA(cudaStreamSynchronize(lat->stream));
+  };
+  auto sync_lo = [&] {
+    if (latl != lat) QPX_CUDA(cudaStreamSynchronize(latl->stream));
+  };
+  std::vector<double> bn = norm2_host(rhs);
+  // true residual in FP64 -> rh, |rh|^2
+  auto true_r = [&]() {
+    eo_apply(op, th, x, isign, cb, ApplyOpts());
+    BlasCall c;
+    c.op = B_XMY_NORM;
+    c.x = rhs;
+    c.y = th;
+    c.z = rh;
+    c.slots = 0x1;
+    blas_launch(lat, prec, nr, c);
+    const double *h = fetch_result(lat, nr, 1);
+    return std::vector<double>(h, h + nr);
+  };
+  std::vector<double> rn = true_r();
+  unsigned long mv_hi = 1, updates = 0;
+  std::vector<int> conv(nr, 0);
+  bool all = true;
+  for (int i = 0; i < nr; i++) {
+    conv[i] = (rn[i] < rsd * rsd * bn[i]) || bn[i] == 0.0;
+    all = all && conv[i];
+  }
+  int low_iters = 0;
+  if (!all) {
+    // r = r0 = convert(rh); xl = p = v = 0
+    convert_field(r, rh, cval(1.0), nullptr);
+    sync_hi();
+    BlasCall cpy;
+    cpy.op = B_COPY;
+    cpy.x = r;
+    cpy.y = r0;
+    blas_launch(latl, lp, nr, cpy);
+    BlasCall z;
+    z.op = B_ZERO;
+    z.x = p;
+    blas_launch(latl, lp, nr, z);
+    z.x = v;
+    blas_launch(latl, lp, nr, z);
+    z.x = xl;
+    blas_launch(latl, lp, nr, z);
+    SolverState &S = state_reset(latl, nr, max_iters);
+    for (int i = 0; i < nr; i++) {
+      S.v[S_RSD][i] = rsd * rsd * bn[i];
+      S.v[S_AUX1][i] = delta * delta * rn[i];
+      S.v[S_RNORM][i] = rn[i];
+      S.v[S_RHO_RE][i] = rn[i];
+      S.v[S_RHOP_RE][i] = 1.0;
+      S.v[S_ALPHA_RE][i] = 1.0;
+      S.v[S_OMEGA_RE][i] = 1.0;
+      S.v[S_BETA_RE][i] = rn[i];
+      if (conv[i]) {
+        S.rhs_done[i] = 1;
+        S.v[S_BETA_RE][i] = S.v[S_ALPHA_RE][i] = S.v[S_OMEGA_RE][i] = 0.0;
+      }
+    }
+    state_upload(latl);
+    SolverState *ds = latl->state;
+    auto step = [&] {
+      BlasCall pu;
+      pu.op = B_BICG_P;
+      pu.x = r;
+      pu.y = p;
+      pu.z = v;
+      pu.a = cslot(ds, S_BETA_RE, S_BETA_IM);
+      pu.b = cslot(ds, S_OMEGA_RE, S_OMEGA_IM);
+      pu.state = ds;
+      blas_launch(latl, lp, nr, pu);
+      ApplyOpts o1;
+      o1.red_mask = RED_DOT_W_OUT;
+      o1.fin = FIN_BICG_ALPHA;
+      o1.state = ds;
+      o1.w = r0;
+      eo_apply(opl, v, p, isign, cb, o1);
+      BlasCall su;
+      su.op = B_BICG_S;
+      su.x = r;
+      su.y = v;
+      su.a = cslot(ds, S_ALPHA_RE, S_ALPHA_IM);
+      su.state = ds;
+      blas_launch(latl, lp, nr, su);
+      ApplyOpts o2;
+      o2.red_mask = RED_NORM_OUT | RED_DOT_OUT_CHI;
+      o2.fin = FIN_BICG_OMEGA;
+      o2.state = ds;
+      eo_apply(opl, t, r, isign, cb, o2);
+      BlasCall rx;
+      rx.op = B_BICG_RX;
+      rx.x = xl;
+      rx.y = r;
+      rx.z = t;
+      rx.v = p;
+      rx.w = r0;
+      rx.a = cslot(ds, S_OMEGA_RE, S_OMEGA_IM);
+      rx.b = cslot(ds, S_ALPHA_RE, S_ALPHA_IM);
+      rx.slots = 0x7;
+      rx.fin = FIN_BICG_RU;
+      rx.state = ds;
+      blas_launch(latl, lp, nr, rx);
+    };
+    std::string key = "bicg-ru/" + std::to_string(opl->serial) + "/" + fkey(xl) + fkey(r0) + fkey(r) + fkey(p) +
+                      fkey(v) + fkey(t) + "/" + std::to_string(isign) + std::to_string(cb);
+    while (true) {
+      run_iterations(latl, step, max_iters, key);
+      SolverState &H = *latl->h_state;
+      low_iters = H.iter;
+      // reliable update for every active rhs: x += xl, xl = 0, rh = b - M x
+      convert_field(x, xl, cval(1.0), nullptr, 1);
+      sync_lo();
+      BlasCall zx;
+      zx.op = B_ZERO;
+      zx.x = xl;
+      blas_launch(latl, lp, nr, zx);
+      rn = true_r();
+      mv_hi++;
+      updates++;
+      all = true;
+      for (int i = 0; i < nr; i++) {
+        if (!conv[i] && rn[i] < rsd * rsd * bn[i]) conv[i] = 1;
+        all = all && conv[i];
+      }
+      bool out_of_iters = H.iter >= max_iters || H.status == 2;
+      if (all || out_of_iters) break;
+      // r = convert(rh); rho = <r0, r>; beta from it; restart the graph
+      convert_field(r, rh, cval(1.0), nullptr);
+      sync_hi();
+      BlasCall dt;
+      dt.op = B_DOT;
+      dt.x = r0;
+      dt.y = r;
+      dt.slots = 0x3;
+      blas_launch(latl, lp, nr, dt);
+      const double *rho = fetch_result(latl, nr, 2);
+      for (int i = 0; i < nr; i++) {
+        if (conv[i]) {
+          if (!H.rhs_done[i]) {
+            H.rhs_done[i] = 1;
+            H.rhs_iter[i] = H.iter;
+          }
+          H.v[S_BETA_RE][i] = H.v[S_BETA_IM][i] = 0.0;
+          H.v[S_ALPHA_RE][i] = H.v[S_ALPHA_IM][i] = 0.0;
+          H.v[S_OMEGA_RE][i] = H.v[S_OMEGA_IM][i] = 0.0;
+          continue;
+        }
+        double rr = rho[2 * i], ri = rho[2 * i + 1];
+        H.v[S_RHO_RE][i] = rr;
+        H.v[S_RHO_IM][i] = ri;
+        double t1r, t1i, t2r, t2i, d1 = H.v[S_RHOP_RE][i] * H.v[S_RHOP_RE][i] + H.v[S_RHOP_IM][i] * H.v[S_RHOP_IM][i];
+        t1r = (rr * H.v[S_RHOP_RE][i] + ri * H.v[S_RHOP_IM][i]) / d1;
+        t1i = (ri * H.v[S_RHOP_RE][i] - rr * H.v[S_RHOP_IM][i]) / d1;
+        double d2 = H.v[S_OMEGA_RE][i] * H.v[S_OMEGA_RE][i] + H.v[S_OMEGA_IM][i] * H.v[S_OMEGA_IM][i];
+        t2r = (H.v[S_ALPHA_RE][i] * H.v[S_OMEGA_RE][i] + H.v[S_ALPHA_IM][i] * H.v[S_OMEGA_IM][i]) / d2;
+        t2i = (H.v[S_ALPHA_IM][i] * H.v[S_OMEGA_RE][i] - H.v[S_ALPHA_RE][i] * H.v[S_OMEGA_IM][i]) / d2;
+        H.v[S_BETA_RE][i] = t1r * t2r - t1i * t2i;
+        H.v[S_BETA_IM][i] = t1r * t2i + t1i * t2r;
+        H.v[S_AUX1][i] = delta * delta * rn[i];
+      }
+      H.done = 0;
+      H.status = 0;
+      state_upload(latl);
+    }
+  }
+  std::vector<double> abs2(rn), rel(nr);
+  for (int i = 0; i < nr; i++) rel[i] = bn[i] > 0 ? std::sqrt(rn[i] / bn[i]) : 0.0;
+  const SolverState &H = *latl->h_state;
+  double secs = timer.stop();
+  for (int i = 0; i < nr; i++) {
+    info[i].n_iters = low_iters;
+    info[i].rsd_sq_final = abs2[i];
+    info[i].mv_apps = mv_hi + 2ul * (unsigned long)low_iters;
+    info[i].site_flops = updates;  // number of reliable updates
+    info[i].status = conv[i] ? 0 : (H.status == 2 ? 2 : 1);
     info[i].true_rel_resid = rel[i];
     info[i].seconds = secs;
   }
@@ -1500,6 +1781,28 @@ extern "C" int qphix_gpu_solve_mr(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_g
   })
 }
 
+extern "C" int qphix_gpu_solve_mr_smoother(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs,
+                                           int n_iters, double omega, int isign, int cb, qphix_gpu_solve_info *info)
+{
+  QPX_SOLVE_ENTRY({
+    QPX_REQUIRE(info && x, "null argument");
+    QPX_REQUIRE(n_iters >= 0, "n_iters must be >= 0");
+    std::vector<double> rs(x->nrhs, 0.0);
+    solve_mr(op, x, rhs, rs.data(), n_iters, omega, isign, cb, info, true, false);
+  })
+}
+
+extern "C" int qphix_gpu_solve_bicgstab_mixed(qphix_gpu_eo_op op, qphix_gpu_eo_op op_low, qphix_gpu_field x,
+                                              qphix_gpu_field rhs, double rsd_target, double delta, int max_iters,
+                                              int isign, int cb, qphix_gpu_solve_info *info)
+{
+  QPX_SOLVE_ENTRY({
+    QPX_REQUIRE(info && x, "null argument");
+    QPX_REQUIRE(delta > 0.0 && delta < 1.0, "delta must be in (0, 1)");
+    solve_bicgstab_mixed(op, op_low, x, rhs, rsd_target, delta, max_iters, isign, cb, info);
+  })
+}
+
 extern "C" int qphix_gpu_solve_richardson(qphix_gpu_eo_op op_outer, qphix_gpu_eo_op op_inner, int inner_solver,
                                           qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target, double delta,
                                           int max_iters, int inner_max_iters, int isign, int cb,
@@ -1512,12 +1815,153 @@ extern "C" int qphix_gpu_solve_richardson(qphix_gpu_eo_op op_outer, qphix_gpu_eo
   })
 }
 
+// ---------------------------------------------------------------------------
+// multishift CG (include/qphix/minvcg.h:77-387): one M^dag M per iteration
+// for the base system; the per-shift zeta / beta recurrences run on the device
+// (FIN_MCG_*), r += b M^dag M p0 is fused into the second Dslash, and every
+// shifted x / p update plus p0 = r + a p0 is one multi-vector kernel.
+static void solve_mshift(qphix_gpu_eo_op_s *op, qphix_gpu_field_s **x, qphix_gpu_field_s *rhs, int ns,
+                         const double *shifts, const double *rsd, int max_iters, int isign, int cb, int *n_iters,
+                         double *rsd_sq_final, unsigned long *mv_apps)
+{
+  QPX_REQUIRE(op && x && rhs && shifts && rsd && n_iters && rsd_sq_final && mv_apps, "null argument");
+  QPX_REQUIRE(ns >= 1 && ns <= QPX_MAX_SHIFTS, "n_shift must be in [1, 32]");
+  require_spinor(rhs, "rhs");
+  QPX_REQUIRE(rhs->nrhs == 1, "multishift CG takes one right-hand side");
+  for (int s = 0; s < ns; s++) {
+    require_spinor(x[s], "x");
+    require_same(x[s], rhs);
+    QPX_REQUIRE(x[s]->nrhs == 1, "multishift CG solutions hold one right-hand side");
+  }
+  require_same(rhs, op->gauge);
+  auto *lat = rhs->lat;
+  const int prec = rhs->prec;
+  Tmp r(lat, prec, 1), p0(lat, prec, 1), mp(lat, prec, 1), mmp(lat, prec, 1);
+  std::vector<Tmp *> ps;
+  for (int s = 0; s < ns; s++) ps.push_back(new Tmp(lat, prec, 1));
+  struct Free {
+    std::vector<Tmp *> &v;
+    ~Free()
+    {
+      for (auto *t : v) delete t;
+    }
+  } free_ps{ps};
+  double cp = norm2_host(rhs)[0];
+  // r = p0 = p_s = rhs
+  BlasCall cpy;
+  cpy.op = B_COPY;
+  cpy.x = rhs;
+  cpy.y = r;
+  blas_launch(lat, prec, 1, cpy);
+  cpy.y = p0;
+  blas_launch(lat, prec, 1, cpy);
+  for (int s = 0; s < ns; s++) {
+    cpy.y = *ps[s];
+    blas_launch(lat, prec, 1, cpy);
+  }
+  eo_apply(op, mp, p0, isign, cb, ApplyOpts());
+  eo_apply(op, mmp, mp, -isign, cb, ApplyOpts());
+  unsigned long mv = 2;
+  double d = norm2_host(mp)[0];
+  double b = -cp / d;
+  // r = r + b mmp, c = |r|^2
+  BlasCall ax;
+  ax.op = B_CAXPBY_NORM;
+  ax.x = mmp;
+  ax.y = r;
+  ax.a = cval(b);
+  ax.b = cval(1.0);
+  ax.slots = 0x1;
+  blas_launch(lat, prec, 1, ax);
+  double c = fetch_result(lat, 1, 1)[0];
+  SolverState &S = state_reset(lat, ns, max_iters);
+  std::vector<double> beta(ns);
+  for (int s = 0; s < ns; s++) {
+    double z = 1.0 / (1.0 - shifts[s] * b);
+    beta[s] = b / (1.0 - shifts[s] * b);
+    S.v[S_AUX1][s] = 1.0;  // zeta_prev
+    S.v[S_AUX0][s] = z;
+    S.v[S_BETA_RE][s] = beta[s];
+    S.v[S_AUX3][s] = shifts[s];
+    S.v[S_RSD][s] = rsd[s] * rsd[s] * cp;
+    S.v[S_AUX6][s] = 0.0;  // no pending x update before the first iteration
+    rsd_sq_final[s] = 0.0;
+  }
+  // first iteration's coefficients: a = c / cp, as_s = a zeta beta / (zeta_prev b)
+  double a = c / cp;
+  S.v[S_A][0] = a;
+  S.v[S_B][0] = b;
+  S.v[S_C][0] = c;
+  for (int s = 0; s < ns; s++) S.v[S_AUX2][s] = a * S.v[S_AUX0][s] * S.v[S_BETA_RE][s] / (1.0 * b);
+  S.done = (max_iters <= 1) ? 1 : 0;
+  // x_s = -beta_s rhs
+  for (int s = 0; s < ns; s++) {
+    BlasCall xb;
+    xb.op = B_CAXPBY;
+    xb.x = rhs;
+    xb.y = x[s];
+    xb.a = cval(-beta[s]);
+    xb.b = cval(0.0);
+    blas_launch(lat, prec, 1, xb);
+  }
+  state_upload(lat);
+  SolverState *ds = lat->state;
+  MShiftArgs ma;
+  memset(&ma, 0, sizeof(ma));
+  ma.vh = (int)lat->vh;
+  ma.nshift = ns;
+  ma.r = static_cast<qphix_gpu_field_s *>(r)->sarg();
+  ma.p0 = static_cast<qphix_gpu_field_s *>(p0)->sarg();
+  for (int s = 0; s < ns; s++) {
+    ma.x[s] = x[s]->sarg();
+    ma.p[s] = static_cast<qphix_gpu_field_s *>(*ps[s])->sarg();
+  }
+  ma.state = ds;
+  if (!S.done) {
+    auto step = [&] {
+      MShiftArgs m = ma;
+      m.x_only = 0;
+      launch_mshift(prec, m, dim3(nblocks_for(lat->vh)), lat->stream);
+      check_launch();
+      ApplyOpts o1;
+      o1.red_mask = RED_NORM_OUT;
+      o1.fin = FIN_MCG_D;
+      o1.state = ds;
+      eo_apply(op, mp, p0, isign, cb, o1);
+      ApplyOpts o2;
+      o2.post = POST_RAXPY;
+      o2.red_mask = RED_NORM_R;
+      o2.fin = FIN_MCG_R;
+      o2.state = ds;
+      o2.r = r;
+      eo_apply(op, mmp, mp, -isign, cb, o2);
+    };
+    std::string key = "mcg/" + std::to_string(op->serial) + "/" + fkey(r) + fkey(p0) + fkey(mp) + fkey(mmp) + "/";
+    for (int s = 0; s < ns; s++) key += fkey(x[s]) + "," + fkey(*ps[s]) + ";";
+    key += "/" + std::to_string(isign) + std::to_string(cb);
+    run_iterations(lat, step, max_iters, key);
+    mv += 2ul * lat->h_state->iter;
+    // the x update of the last iteration is still pending
+    MShiftArgs m = ma;
+    m.x_only = 1;
+    launch_mshift(prec, m, dim3(nblocks_for(lat->vh)), lat->stream);
+    check_launch();
+    QPX_CUDA(cudaStreamSynchronize(lat->stream));
+  }
+  const SolverState &H = *lat->h_state;
+  *n_iters = H.iter;
+  for (int s = 0; s < ns; s++) rsd_sq_final[s] = H.rhs_done[s] ? H.v[S_RNORM][s] : 0.0;
+  *mv_apps = mv;
+  bool all = true;
+  for (int s = 0; s < ns; s++) all = all && H.rhs_done[s];
+  if (!all && !S.done) throw Error(QPHIX_GPU_ENOTCONV, "multishift CG did not converge");
+}
+
 extern "C" int qphix_gpu_solve_mshift_cg(qphix_gpu_eo_op op, qphix_gpu_field *x, qphix_gpu_field rhs, int n_shift,
                                          const double *shifts, const double *rsd_target, int max_iters, int isign,
                                          int cb, int *n_iters, double *rsd_sq_final, unsigned long *mv_apps)
 {
-  (void)op; (void)x; (void)rhs; (void)n_shift; (void)shifts; (void)rsd_target; (void)max_iters; (void)isign;
-  (void)cb; (void)n_iters; (void)rsd_sq_final; (void)mv_apps;
-  g_last_error = "multishift CG is not built yet";
-  return QPHIX_GPU_EUNSUPPORTED;
+  return guard([&] {
+    solve_mshift(op, x, rhs, n_shift, shifts, rsd_target, max_iters, isign, cb, n_iters, rsd_sq_final, mv_apps);
+  });
 }

@@ -245,12 +245,70 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
   if (a.red.mask) reduce_epilogue<1>(a.red, a.state, a.nrhs, rhs, a.red.mask, red);
 }
 
+// Multishift CG vector update (include/qphix/minvcg.h:279-384), fused across
+// iterations: the x update of iteration k (x_s -= beta_s p_s, with
+// xcoef_s = beta_s for shifts still active in k, else 0) and the p updates of
+// iteration k+1 (p_s = zeta_s r + as_s p_s for shifts not yet converged;
+// p0 = r + a p0) in one pass over r, p0 and every (x_s, p_s).
+constexpr int QPX_MAX_SHIFTS = 32;
+struct MShiftArgs {
+  int vh;
+  int nshift;
+  int x_only;          // 1: apply only the pending x update (after the last iteration)
+  SpinorArg r, p0;
+  SpinorArg x[QPX_MAX_SHIFTS], p[QPX_MAX_SHIFTS];
+  SolverState *state;  // coefficients; its done flag stops the update unless x_only
+};
+
+template <typename P>
+__global__ void __launch_bounds__(QPX_BLOCK) mshift_update_kernel(const MShiftArgs a)
+{
+  using T = typename P::real;
+  using IO = SpinorIO<P>;
+  const SolverState *st = a.state;
+  if (!a.x_only && st->done) return;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.vh) return;
+  T r[24];
+  if (!a.x_only) IO::load(a.r, 0, s, r);
+  for (int sh = 0; sh < a.nshift; sh++) {
+    const T xc = (T)st->v[S_AUX6][sh];
+    const bool pact = !a.x_only && !st->rhs_done[sh];
+    if (xc == (T)0 && !pact) continue;
+    T p[24];
+    IO::load(a.p[sh], 0, s, p);
+    if (xc != (T)0) {
+      T x[24];
+      IO::load(a.x[sh], 0, s, x);
+#pragma unroll
+      for (int k = 0; k < 24; k++) x[k] -= xc * p[k];
+      IO::store(a.x[sh], 0, s, x);
+    }
+    if (pact) {
+      const T z = (T)st->v[S_AUX0][sh], as = (T)st->v[S_AUX2][sh];
+#pragma unroll
+      for (int k = 0; k < 24; k++) p[k] = z * r[k] + as * p[k];
+      IO::store(a.p[sh], 0, s, p);
+    }
+  }
+  if (!a.x_only) {
+    T p0[24];
+    IO::load(a.p0, 0, s, p0);
+    const T aa = (T)st->v[S_A][0];
+#pragma unroll
+    for (int k = 0; k < 24; k++) p0[k] = r[k] + aa * p0[k];
+    IO::store(a.p0, 0, s, p0);
+  }
+}
+
 // y (precision Q) = scale * x (precision P): the precision conversion of
 // InvRichardsonMultiPrec (blas_new_c.h:852-960), scale = 1/|r| going down
 // and |r| coming back up.  `scale` may be a per-rhs device value.
+// accumulate = 1: y += scale * x (folds a low-precision solution increment
+// into a high-precision solution).
 template <typename P, typename Q>
 __global__ void __launch_bounds__(QPX_BLOCK) convert_kernel(int vh, SpinorArg x, SpinorArg y, Coef scale,
-                                                            SolverState *state)
+                                                            SolverState *state, int accumulate)
 {
   if (state && state->done) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -260,8 +318,14 @@ __global__ void __launch_bounds__(QPX_BLOCK) convert_kernel(int vh, SpinorArg x,
   typename Q::real yv[24];
   SpinorIO<P>::load(x, rhs, s, xv);
   const double sc = scale.r(rhs);
+  if (accumulate) {
+    SpinorIO<Q>::load(y, rhs, s, yv);
 #pragma unroll
-  for (int k = 0; k < 24; k++) yv[k] = (typename Q::real)((double)xv[k] * sc);
+    for (int k = 0; k < 24; k++) yv[k] = (typename Q::real)((double)yv[k] + (double)xv[k] * sc);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 24; k++) yv[k] = (typename Q::real)((double)xv[k] * sc);
+  }
   SpinorIO<Q>::store(y, rhs, s, yv);
 }
 

@@ -439,15 +439,16 @@ template <typename H, int NR>
 struct CloverIO16 {
   static constexpr int nchunk = NR / 8;
   static constexpr size_t chunk_bytes = 16;
-  // k0, n multiples of 4: loads whole 8-value chunks and picks the needed half
+  // k0, n multiples of 4: every 16-byte chunk overlapping [k0, k0 + n) is
+  // loaded once and the needed halves unpacked
   __device__ __forceinline__ static void load(const CloverArg &c, long long s, int k0, int n, float *v)
   {
     const uint4 *p = reinterpret_cast<const uint4 *>(c.data) + s;
-    for (int k = 0; k < n; k += 4) {
-      int q = k0 + k;
+#pragma unroll
+    for (int q = (k0 / 8) * 8; q < k0 + n; q += 8) {
       uint4 d = __ldg(p + (q / 8) * c.stride);
-      uint2 h = (q % 8 == 0) ? make_uint2(d.x, d.y) : make_uint2(d.z, d.w);
-      unpack4(h, v + k, H());
+      if (q >= k0) unpack4(make_uint2(d.x, d.y), v + (q - k0), H());
+      if (q + 4 < k0 + n && q + 4 >= k0) unpack4(make_uint2(d.z, d.w), v + (q + 4 - k0), H());
     }
   }
 };

@@ -24,7 +24,11 @@ namespace qpx {
 
 enum Epi : int { EPI_NONE = 0, EPI_CLOV = 1, EPI_TMINV = 2, EPI_FCLOV = 3 };
 enum Achi : int { ACHI_NONE = 0, ACHI_ALPHA = 1, ACHI_CLOV = 2, ACHI_TM = 3 };
-enum Post : int { POST_STORE = 0, POST_CG = 1 };
+enum Post : int {
+  POST_STORE = 0,  // store out
+  POST_CG = 1,     // r -= a out ; x += a p ; |r|^2   (a = state S_A[rhs]); out not stored
+  POST_RAXPY = 2,  // r += b out ; |r|^2             (b = state S_B[rhs]); out not stored
+};
 // reduction value bits (values appear in this order)
 enum RedBit : int {
   RED_NORM_OUT = 1,   // |out|^2                   (1 value,  slot 0)
@@ -419,6 +423,18 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
       }
       if (a.post == POST_STORE) {
         SpinorIO<P>::store(a.out, rr, s, res[r]);
+      } else if (a.post == POST_RAXPY) {  // r += b mmp ; |r|^2
+        const T cb_ = (T)a.state->v[S_B][rr];
+        T rv[24];
+        SpinorIO<P>::load(a.r, rr, s, rv);
+        double n2 = 0;
+#pragma unroll
+        for (int k = 0; k < 24; k++) {
+          rv[k] += cb_ * res[r][k];
+          n2 += (double)rv[k] * rv[k];
+        }
+        SpinorIO<P>::store(a.r, rr, s, rv);
+        red[r][5] = n2;
       } else {  // POST_CG: r -= a mmp ; x += a p ; |r|^2
         const T ca = (T)a.state->v[S_A][rr];
         T rv[24], xv[24], pv[24];

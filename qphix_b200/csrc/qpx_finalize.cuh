@@ -136,6 +136,39 @@ __device__ inline void finalize(int fin, SolverState *st, const double *res, int
     }
     end_iteration(st, nrhs);
     break;
+  // ---- BiCGStab with reliable updates ---------------------------------------
+  // As FIN_BICG_RX, but a right-hand side whose iterated residual fell below
+  // its update threshold (S_AUX1, delta^2 |r_true|^2 at the last update) or
+  // its target asks the host for a reliable update instead of stopping:
+  // st->status = 3 and the iteration graph stops (done) until the host has
+  // replaced r by the recomputed true residual.
+  case FIN_BICG_RU: {
+    bool request = false;
+    for (int r = 0; r < nrhs; r++) {
+      if (st->rhs_done[r]) continue;
+      double rn = res[r * nval];
+      v[S_RNORM][r] = rn;
+      if (rn < v[S_AUX1][r] || rn < v[S_RSD][r]) request = true;
+      double rr = res[r * nval + 1], ri = res[r * nval + 2];
+      if (rr == 0.0 && ri == 0.0) {
+        request = true;  // let the true residual decide
+        continue;
+      }
+      v[S_RHO_RE][r] = rr;
+      v[S_RHO_IM][r] = ri;
+      double t1r, t1i, t2r, t2i;
+      cdiv(t1r, t1i, rr, ri, v[S_RHOP_RE][r], v[S_RHOP_IM][r]);
+      cdiv(t2r, t2i, v[S_ALPHA_RE][r], v[S_ALPHA_IM][r], v[S_OMEGA_RE][r], v[S_OMEGA_IM][r]);
+      v[S_BETA_RE][r] = t1r * t2r - t1i * t2i;
+      v[S_BETA_IM][r] = t1r * t2i + t1i * t2r;
+    }
+    end_iteration(st, nrhs);
+    if (request) {
+      st->done = 1;
+      st->status = 3;
+    }
+    break;
+  }
   // ---- MR (include/qphix/invmr.h:143-190) ---------------------------------
   case FIN_MR_A:
     for (int r = 0; r < nrhs; r++) {
@@ -154,6 +187,57 @@ __device__ inline void finalize(int fin, SolverState *st, const double *res, int
     }
     end_iteration(st, nrhs);
     break;
+  // ---- multishift CG (include/qphix/minvcg.h:279-384) -------------------
+  // scalars in slot [0]: a S_A, b S_B, c S_C, d S_D, cp S_AUX4, bp S_AUX5;
+  // per shift s: zeta S_AUX0, zeta_prev S_AUX1, beta S_BETA_RE, as S_AUX2,
+  // shift S_AUX3, pending x coefficient S_AUX6, target S_RSD, final S_RNORM
+  case FIN_MCG_D: {
+    v[S_AUX4][0] = v[S_C][0];  // cp = c
+    v[S_AUX5][0] = v[S_B][0];  // bp = b
+    v[S_D][0] = res[0];
+    v[S_B][0] = -v[S_AUX4][0] / v[S_D][0];
+    break;
+  }
+  case FIN_MCG_R: {
+    // one base system (nrhs = 1); the shifts are the state's st->nrhs entries
+    const int nsh = st->nrhs;
+    const double c = res[0], b = v[S_B][0], bp = v[S_AUX5][0], a = v[S_A][0];
+    v[S_C][0] = c;
+    bool all = true;
+    for (int sh = 0; sh < nsh; sh++) {
+      if (st->rhs_done[sh]) {
+        v[S_AUX6][sh] = 0.0;
+        continue;
+      }
+      double z0 = v[S_AUX0][sh], z1 = v[S_AUX1][sh];
+      v[S_AUX1][sh] = z0;
+      double z = z0 * z1 * bp;
+      z /= (b * a * (z1 - z0) + z1 * bp * (1.0 - v[S_AUX3][sh] * b));
+      v[S_AUX0][sh] = z;
+      v[S_BETA_RE][sh] = b * z / z0;
+      v[S_AUX6][sh] = v[S_BETA_RE][sh];
+      double css = c * z * z;
+      if (css < v[S_RSD][sh]) {
+        st->rhs_done[sh] = 1;
+        st->rhs_iter[sh] = st->iter + 1;
+        v[S_RNORM][sh] = css;
+      }
+      all = all && st->rhs_done[sh];
+    }
+    // coefficients of the next iteration's p updates
+    const double an = c / v[S_AUX4][0];
+    v[S_A][0] = an;
+    for (int sh = 0; sh < nsh; sh++)
+      if (!st->rhs_done[sh]) v[S_AUX2][sh] = an * v[S_AUX0][sh] * v[S_BETA_RE][sh] / (v[S_AUX1][sh] * b);
+    st->iter++;
+    if (all) {
+      st->done = 1;
+    } else if (st->iter + 1 >= st->max_iter) {  // the reference loop runs k = 1 .. MaxIters - 1
+      st->done = 1;
+      st->status = 1;
+    }
+    break;
+  }
   default:
     break;
   }

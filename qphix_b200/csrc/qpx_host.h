@@ -7,6 +7,7 @@
 #include <map>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../../include/qphix_b200.h"
 #include "qpx_blas.cuh"
@@ -65,6 +66,12 @@ struct qphix_gpu_lattice_s {
   qpx::SolverState *h_state = nullptr; // pinned mirror
   void *staging = nullptr;
   size_t staging_bytes = 0;
+  // solver temporaries, reused across solves (they hold no lattice reference)
+  std::vector<struct qphix_gpu_field_s *> pool_free, pool_all;
+  // instantiated solver-iteration graphs, keyed by what they were captured on
+  std::map<std::string, cudaGraphExec_t> graphs;
+  std::map<std::string, unsigned long long> graph_nodes;
+  std::vector<std::string> graph_order;
   qpx::Geom geom() const
   {
     qpx::Geom g;
@@ -81,6 +88,7 @@ struct qphix_gpu_lattice_s {
 struct qphix_gpu_field_s {
   qphix_gpu_lattice_s *lat;
   int kind, prec, recon, nrhs;
+  unsigned long long serial = 0;  // unique per created field
   qpx::ChunkSpec spec;
   void *data = nullptr;
   float *norm = nullptr;
@@ -112,6 +120,7 @@ struct qphix_gpu_field_s {
 };
 
 struct qphix_gpu_eo_op_s {
+  unsigned long long serial = 0;  // unique per created operator
   qphix_gpu_op_params p;
   qphix_gpu_field_s *gauge, *clov, *invclov, *finv0, *finv1;
   std::map<int, qphix_gpu_field_s *> tmp;  // by nrhs
@@ -124,17 +133,18 @@ void launch_dslash(int prec, int recon, int epi, int achi, int R, const DslashAr
                    cudaStream_t st);
 void launch_blas(int prec, const BlasArgs &a, dim3 grid, cudaStream_t st);
 void launch_convert(int pdst, int psrc, int vh, SpinorArg src, SpinorArg dst, Coef scale, SolverState *state,
-                    dim3 grid, cudaStream_t st);
+                    dim3 grid, cudaStream_t st, int accumulate = 0);
 void launch_spinor_in(int prec, Geom g, HostLayout L, const void *host, SpinorArg f, int nrhs, dim3 grid,
                       cudaStream_t st);
 void launch_spinor_out(int prec, Geom g, HostLayout L, void *host, SpinorArg f, int nrhs, dim3 grid,
                        cudaStream_t st);
 void launch_gauge_in(int prec, Geom g, HostLayout L, const void *host, void *dev, long long stride,
-                     long long slab_bytes, int vpc, int recon, int cb, dim3 grid, cudaStream_t st);
+                     long long slab_bytes, int vpc, int recon, int cb, int back, dim3 grid, cudaStream_t st);
 void launch_clover_in(int prec, Geom g, HostLayout L, const void *host, void *dev, long long stride, int vpc,
                       int nr, dim3 grid, cudaStream_t st);
 void launch_clover_out(int prec, Geom g, void *host, const void *dev, long long stride, int vpc, int nr,
                        dim3 grid, cudaStream_t st);
+void launch_mshift(int prec, const MShiftArgs &a, dim3 grid, cudaStream_t st);
 
 // tile sizes compiled for each precision
 bool dslash_tile_ok(int prec, int R);

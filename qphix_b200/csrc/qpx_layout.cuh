@@ -125,13 +125,27 @@ __device__ __forceinline__ double dev_load_real(const void *base, long long stri
 // Gauge: reads U_mu(x) for x in checkerboard `cb` (canonical: both cbs in one
 // array, `cb` selects; qphix: the array of that cb, forward slot 2 mu + 1,
 // stored [c][c2] = U(c2, c), compressed arrays keep columns 0 and 1).
+//
+// back = 1 (qphix only): read the back-link slot 2 mu of checkerboard cb,
+// U_mu(x - mu) (qdp_packer_parscalar.h:94-110), and store it as the forward
+// link of site x - mu in the other checkerboard's slab.
 template <typename P>
 __global__ void gauge_in_kernel(Geom g, HostLayout L, const void *host, void *dev, long long stride,
-                                long long slab_bytes, int vpc, int recon, int cb)
+                                long long slab_bytes, int vpc, int recon, int cb, int back)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int mu = blockIdx.y;
   if (s >= g.vh) return;
+  int dst_cb = cb, dst_s = s;
+  if (back) {
+    int xh, y, z, t, par;
+    site_coords(g, s, cb, xh, y, z, t, par);
+    int c[4] = {2 * xh + par, y, z, t};
+    int n[4] = {g.nx, g.ny, g.nz, g.nt};
+    c[mu] = (c[mu] - 1 + n[mu]) % n[mu];
+    dst_cb = 1 - cb;
+    dst_s = ((c[3] * g.nz + c[2]) * g.ny + c[1]) * g.nxh + c[0] / 2;
+  }
   double u[3][3][2];
   if (L.kind == HOST_CANONICAL) {
     long long base = (((long long)cb * 4 + mu) * g.vh + s) * 18;
@@ -144,7 +158,7 @@ __global__ void gauge_in_kernel(Geom g, HostLayout L, const void *host, void *de
     host_gblock(L, g, s, blk, lane);
     int nc = L.c12 ? 2 : 3;
     long long bsz = 8LL * nc * 3 * 2 * L.V;
-    int slot = 2 * mu + 1;
+    int slot = back ? 2 * mu : 2 * mu + 1;
     for (int c = 0; c < nc; c++)
       for (int c2 = 0; c2 < 3; c2++)
         for (int ri = 0; ri < 2; ri++)
@@ -162,11 +176,11 @@ __global__ void gauge_in_kernel(Geom g, HostLayout L, const void *host, void *de
       }
     }
   }
-  char *slab = reinterpret_cast<char *>(dev) + ((long long)cb * 4 + mu) * slab_bytes;
+  char *slab = reinterpret_cast<char *>(dev) + ((long long)dst_cb * 4 + mu) * slab_bytes;
   int nstore = (recon == 12) ? 2 : 3;
   for (int r = 0; r < nstore; r++)
     for (int c = 0; c < 3; c++)
-      for (int ri = 0; ri < 2; ri++) dev_store_real<P>(slab, stride, vpc, s, (r * 3 + c) * 2 + ri, u[r][c][ri]);
+      for (int ri = 0; ri < 2; ri++) dev_store_real<P>(slab, stride, vpc, dst_s, (r * 3 + c) * 2 + ri, u[r][c][ri]);
 }
 
 // clover / full clover: NR reals per site, canonical [Vh][NR] or qphix

@@ -55,6 +55,7 @@ enum FinOp : int {
   FIN_STORE,       // plain reduction: result only
   FIN_MCG_D,       // multishift CG: d = |Mp|^2, b = -cp/d
   FIN_MCG_R,       // multishift CG: c = |r|^2, zeta/beta per shift, convergence
+  FIN_BICG_RU,     // BiCGStab with reliable updates: as FIN_BICG_RX, asks for an update
 };
 
 struct ReduceArg {

@@ -1,0 +1,152 @@
+// Drives the QPhiX drop-in headers (include/qphix/) the way a QPhiX caller
+// does: Geometry-allocated host arrays in QPhiX's blocked layout, Dslash /
+// operator / solver objects, results back in the host arrays.  Inputs and
+// outputs are raw binary files in a directory given on the command line;
+// tests/test_dropin_gpu.py writes the inputs (packed from seeded canonical
+// fields) and checks the outputs against the CPU oracle.
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "qphix/clover.h"
+#include "qphix/geometry.h"
+#include "qphix/inv_richardson_multiprec.h"
+#include "qphix/invbicgstab.h"
+#include "qphix/invcg.h"
+#include "qphix/minvcg.h"
+#include "qphix/wilson.h"
+
+using namespace QPhiX;
+
+static std::string dir;
+
+template <typename T>
+void read_into(const std::string &name, T *p, size_t bytes)
+{
+  std::ifstream f(dir + "/" + name, std::ios::binary);
+  if (!f) throw std::runtime_error("missing input " + name);
+  f.read(reinterpret_cast<char *>(p), bytes);
+  if (!f) throw std::runtime_error("short input " + name);
+}
+
+template <typename T>
+void write_from(const std::string &name, const T *p, size_t bytes)
+{
+  std::ofstream f(dir + "/" + name, std::ios::binary);
+  f.write(reinterpret_cast<const char *>(p), bytes);
+}
+
+template <typename FT, int V, int S>
+struct Fields {
+  typedef Geometry<FT, V, S, true> G;
+  G &g;
+  typename G::SU3MatrixBlock *u[2];
+  typename G::CloverBlock *A_odd, *Ainv_even;
+  size_t gbytes, cbytes;
+  Fields(G &geom, const std::string &tag) : g(geom)
+  {
+    gbytes = (size_t)(g.getPxyz() * g.Nt() * S / V) * sizeof(typename G::SU3MatrixBlock);
+    cbytes = (size_t)(g.getPxyz() * g.Nt() * S / V) * sizeof(typename G::CloverBlock);
+    for (int cb = 0; cb < 2; cb++) {
+      u[cb] = g.allocCBGauge();
+      read_into(tag + "u" + std::to_string(cb), u[cb], gbytes);
+    }
+    A_odd = g.allocCBClov();
+    Ainv_even = g.allocCBClov();
+    read_into(tag + "A_odd", A_odd, cbytes);
+    read_into(tag + "Ainv_even", Ainv_even, cbytes);
+  }
+  ~Fields()
+  {
+    g.free(u[0]);
+    g.free(u[1]);
+    g.free(A_odd);
+    g.free(Ainv_even);
+  }
+};
+
+int main(int argc, char **argv)
+{
+  if (argc < 2) {
+    fprintf(stderr, "usage: %s <dir>\n", argv[0]);
+    return 2;
+  }
+  dir = argv[1];
+  int latt[4];
+  read_into("dims", latt, sizeof(latt));
+  double mass;
+  read_into("mass", &mass, sizeof(double));
+  try {
+    qphix_gpu_init(0);
+    // double, veclen 4, soalen 2, 12-real links, padding on
+    Geometry<double, 4, 2, true> geom(latt, 2, 2, 1, 1, 1, 1, 1, 1);
+    Geometry<float, 8, 2, true> geomf(latt, 4, 2, 1, 1, 1, 1, 1, 1);
+    Fields<double, 4, 2> F(geom, "d_");
+    Fields<float, 8, 2> Ff(geomf, "f_");
+    size_t sbytes = (size_t)(geom.getPxyz() * geom.Nt()) * sizeof(Geometry<double, 4, 2, true>::FourSpinorBlock);
+    auto *psi = geom.allocCBFourSpinor();
+    auto *res = geom.allocCBFourSpinor();
+    auto *x = geom.allocCBFourSpinor();
+    read_into("d_psi", psi, sbytes);
+
+    // 1. Dslash::dslash onto cb 0 with u[0] (isign +1, antiperiodic t)
+    Dslash<double, 4, 2, true> D(&geom, -1.0, 1.0, 1.0);
+    D.dslash(res, psi, F.u[0], 1, 0);
+    write_from("out_dslash", res, sbytes);
+
+    // 2. EvenOddCloverOperator applied on the odd checkerboard
+    EvenOddCloverOperator<double, 4, 2, true> M(F.u, F.A_odd, F.Ainv_even, &geom, -1.0, 1.0, 1.0);
+    M(res, psi, 1, 1);
+    write_from("out_clover_op", res, sbytes);
+
+    // 3. InvBiCGStab on it
+    int n_iters;
+    double rsd_sq;
+    unsigned long flops, mv;
+    InvBiCGStab<double, 4, 2, true> bicg(M, 2000);
+    bicg(x, psi, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
+    write_from("out_bicgstab_x", x, sbytes);
+    double info[3] = {(double)n_iters, rsd_sq, (double)mv};
+    write_from("out_bicgstab_info", info, sizeof(info));
+
+    // 4. InvCG on the Wilson operator
+    EvenOddWilsonOperator<double, 4, 2, true> W(mass, F.u, &geom, -1.0, 1.0, 1.0);
+    auto *y = geom.allocCBFourSpinor();
+    InvCG<double, 4, 2, true> cg(W, 2000);
+    cg(y, psi, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
+    write_from("out_cg_x", y, sbytes);
+    double cinfo[3] = {(double)n_iters, rsd_sq, (double)mv};
+    write_from("out_cg_info", cinfo, sizeof(cinfo));
+
+    // 5. InvRichardsonMultiPrec: double outer, float BiCGStab inner
+    EvenOddCloverOperator<float, 8, 2, true> Mf(Ff.u, Ff.A_odd, Ff.Ainv_even, &geomf, -1.0, 1.0, 1.0);
+    InvBiCGStab<float, 8, 2, true> inner(Mf, 2000);
+    InvRichardsonMultiPrec<double, 4, 2, true, float, 8, 2, true> rich(M, inner, 0.1, 100);
+    auto *z = geom.allocCBFourSpinor();
+    rich(z, psi, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
+    write_from("out_rich_x", z, sbytes);
+
+    // 6. MInvCG on the clover operator
+    const int ns = 3;
+    double shifts[ns] = {0.01, 0.1, 0.5}, rsd[ns] = {1e-9, 1e-9, 1e-9}, fin[ns];
+    Geometry<double, 4, 2, true>::FourSpinorBlock *xs[ns];
+    for (int s = 0; s < ns; s++) xs[s] = geom.allocCBFourSpinor();
+    MInvCG<double, 4, 2, true> mcg(M, 2000, ns);
+    mcg(xs, psi, ns, shifts, rsd, n_iters, fin, flops, mv, 1, false, 1);
+    for (int s = 0; s < ns; s++) write_from("out_minv_x" + std::to_string(s), xs[s], sbytes);
+
+    for (int s = 0; s < ns; s++) geom.free(xs[s]);
+    geom.free(psi);
+    geom.free(res);
+    geom.free(x);
+    geom.free(y);
+    geom.free(z);
+  } catch (const std::exception &e) {
+    fprintf(stderr, "drop-in test failed: %s\n", e.what());
+    return 1;
+  }
+  printf("drop-in ok\n");
+  return 0;
+}

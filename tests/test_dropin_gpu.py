@@ -1,0 +1,68 @@
+"""The C++ drop-in headers (include/qphix/) used the way a QPhiX caller uses
+QPhiX: tests/cpp/dropin_main.cc is compiled with g++ against the headers and
+the library, fed QPhiX-layout host arrays (Geometry<double,4,2,true> with
+padding, and Geometry<float,8,2,true> for the inner solver of
+InvRichardsonMultiPrec) packed from seeded fields, and its outputs -- a
+Dslash, the clover operator, BiCGStab, CG, Richardson and multishift-CG
+solves -- are checked against the CPU oracle."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import make_setup, rel_l2
+from qphix_b200 import fields as F
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_cpp_dropin(tmp_path, oracle):
+    exe = tmp_path / "dropin"
+    subprocess.check_call(["g++", "-std=c++14", "-O1", "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "cpp", "dropin_main.cc"),
+                           "-L", os.path.join(ROOT, "qphix_b200"), "-lqphix_b200",
+                           "-Wl,-rpath," + os.path.join(ROOT, "qphix_b200"), "-o", str(exe)])
+    dims = (8, 4, 4, 8)
+    s = make_setup(dims, seed=31, gauge_kind="weak", mass=0.1)
+    d = tmp_path
+    np.array(dims, dtype=np.int32).tofile(d / "dims")
+    np.array([s["mass"]], dtype=np.float64).tofile(d / "mass")
+    # Geometry(latt, By=2, Bz=2, 1, 1, 1, PadXY=1, PadXYZ=1): double V=4 S=2 / float V=8 S=2
+    for tag, V, S, dt in (("d_", 4, 2, np.float64), ("f_", 8, 2, np.float32)):
+        lay = F.QPhiXLayout(dims, V, S, True, pad_xy=1, pad_xyz=1)
+        for cb in range(2):
+            lay.pack_gauge(s["gauge"], cb, dt).tofile(d / f"{tag}u{cb}")
+        lay.pack_clover(s["clov"][1], dt).tofile(d / f"{tag}A_odd")
+        lay.pack_clover(s["invclov"][0], dt).tofile(d / f"{tag}Ainv_even")
+    lay = F.QPhiXLayout(dims, 4, 2, True, pad_xy=1, pad_xyz=1)
+    psi = F.gaussian_spinor(dims, 32)
+    lay.pack_spinor(psi)[1:].tofile(d / "d_psi")  # block 0 = what allocCBFourSpinor returns
+    out = subprocess.run([str(exe), str(d)], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr + out.stdout
+
+    def load(name):
+        a = np.fromfile(d / name, dtype=np.float64)
+        full = np.zeros((lay.n_spinor_blocks,) + (3, 4, 2, 2))
+        full[1:] = a.reshape((-1, 3, 4, 2, 2))
+        return lay.unpack_spinor(full)
+
+    L = oracle.make_lattice(dims, -1.0)
+    assert rel_l2(load("out_dslash"), oracle.dslash(L, psi, s["gauge"], 1, 0)) < 1e-13
+    O = oracle.OracleOp("clover", L, s["gauge"], clov=s["clov"][1], invclov=s["invclov"][0])
+    assert rel_l2(load("out_clover_op"), O.apply(psi, 1, 1)) < 1e-13
+    x = load("out_bicgstab_x")
+    assert np.linalg.norm(psi - O.apply(x, 1)) / np.linalg.norm(psi) < 2e-10
+    info = np.fromfile(d / "out_bicgstab_info")
+    xo, io = oracle.bicgstab(O, psi, 1e-10, 2000)
+    assert abs(int(info[0]) - io.n_iters) <= 1
+    W = oracle.OracleOp("wilson", L, s["gauge"], mass=s["mass"])
+    y = load("out_cg_x")
+    assert np.linalg.norm(psi - W.apply(W.apply(y, 1), -1)) / np.linalg.norm(psi) < 2e-10
+    z = load("out_rich_x")
+    assert np.linalg.norm(psi - O.apply(z, 1)) / np.linalg.norm(psi) < 1e-10
+    for i, sh in enumerate((0.01, 0.1, 0.5)):
+        xs = load(f"out_minv_x{i}")
+        r = psi - (O.apply(O.apply(xs, 1), -1) + sh * xs)
+        assert np.linalg.norm(r) / np.linalg.norm(psi) < 3e-9

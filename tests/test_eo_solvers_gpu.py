@@ -171,3 +171,52 @@ def test_multi_rhs_block_matches_single(api, oracle, setup):
             r = bs[i] - O.apply(xs[i], 1)
             assert np.linalg.norm(r) / np.linalg.norm(bs[i]) < (2e-5 if prec == "f32" else 2e-10)
             assert infos[i]["status"] == 0
+
+
+@pytest.mark.parametrize("kind", ["wilson", "clover"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_minvcg(api, oracle, setup, kind, prec):
+    """Multishift CG (include/qphix/minvcg.h): same iteration count as the
+    oracle in FP64, every shifted system solved to its target."""
+    lat, M, O = build_ops(api, oracle, setup, kind, prec)
+    b = F.gaussian_spinor(setup["dims"], 61)
+    shifts = [1e-4, 1e-3, 0.01, 0.1, 1.0]
+    tol = 1e-9 if prec == "f64" else 1e-5
+    gb = lat.spinor(prec).upload(b)
+    xs = [lat.spinor(prec) for _ in shifts]
+    it, fin, mv = api.MInvCG(M, 2000)(xs, gb, shifts, [tol] * len(shifts))
+    xo, io, fo, mvo = oracle.minvcg(O, b, shifts, [tol] * len(shifts), 2000)
+    if prec == "f64":
+        assert it == io and mv == mvo
+    for s, x in zip(shifts, xs):
+        xv = x.download()
+        r = b - (O.apply(O.apply(xv, 1), -1) + s * xv)
+        assert np.linalg.norm(r) / np.linalg.norm(b) < (3 * tol if prec == "f64" else 50 * tol), s
+    if prec == "f64":
+        for x, xr in zip(xs, xo):
+            assert rel_l2(x.download(), xr) < 1e-7
+
+
+@pytest.mark.parametrize("low", ["f16", "bf16", "f32"])
+@pytest.mark.parametrize("nrhs", [1, 3])
+def test_bicgstab_reliable_update(api, oracle, setup, low, nrhs):
+    """BiCGStab with reliable updates (FP64 true residuals, low-precision
+    iterations): every right-hand side reaches 1e-10 in the FP64 true
+    residual, recomputed here with the oracle."""
+    s = setup
+    lat, M, O = build_ops(api, oracle, s, "clover")
+    u_l = lat.gauge(low, 12).upload(s["gauge"])
+    A = lat.clover(low).upload(s["clov"][1])
+    Ai = lat.clover(low).upload(s["invclov"][0])
+    Ml = api.EvenOddCloverOperator(u_l, A, Ai)
+    bs = [F.gaussian_spinor(s["dims"], 80 + i) for i in range(nrhs)]
+    gb = lat.spinor("f64", nrhs).upload(np.stack(bs))
+    gx = lat.spinor("f64", nrhs)
+    infos = api.InvBiCGStabMixed(M, Ml, delta=0.1)(gx, gb, 1e-10)
+    xs = gx.download()
+    if nrhs == 1:
+        xs = xs[None]
+    for i in range(nrhs):
+        r = bs[i] - O.apply(xs[i], 1)
+        assert np.linalg.norm(r) / np.linalg.norm(bs[i]) < 1e-10
+        assert infos[i]["status"] == 0 and infos[i]["true_rel_resid"] < 1e-10
