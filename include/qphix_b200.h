@@ -155,6 +155,23 @@ int qphix_gpu_dslash_dir(const qphix_gpu_op_params *p, qphix_gpu_field res, qphi
                          qphix_gpu_field gauge, int cb, int dir);
 int qphix_gpu_clover_apply(qphix_gpu_field res, qphix_gpu_field chi, qphix_gpu_field clov);
 
+/* ---- clover term on the device ----------------------------------------------
+ * QPhiX takes the clover term and its inverse from its caller (Chroma's
+ * QDPCloverTerm); these build them on the GPU from a resident FP64 gauge field:
+ *   qphix_gpu_clover_build   A on checkerboard cb: diag_mass + sigma.F with the
+ *     clover-leaf field strength (tests/mesfield.cc:25-64) and the packing /
+ *     coefficient convention of tests/clover_term_qdp_w.h:114-200,325-442
+ *     (isotropic Wilson-clover: diag_mass = 4 + m, csw_r = csw_t = c_sw)
+ *   qphix_gpu_clover_invert  packed A^-1
+ *   qphix_gpu_clover_invert_twisted  full (A + i mu g5)^-1, (A - i mu g5)^-1
+ *   qphix_gpu_clover_convert precision change of a clover / full clover field */
+int qphix_gpu_clover_build(qphix_gpu_field clov, qphix_gpu_field gauge, int cb, double diag_mass, double csw_r,
+                           double csw_t);
+int qphix_gpu_clover_invert(qphix_gpu_field dst, qphix_gpu_field src);
+int qphix_gpu_clover_invert_twisted(qphix_gpu_field dst_plus, qphix_gpu_field dst_minus, qphix_gpu_field src,
+                                    double mu);
+int qphix_gpu_clover_convert(qphix_gpu_field dst, qphix_gpu_field src);
+
 /* ---- even-odd operators ----------------------------------------------------
  * Replace EvenOddWilsonOperator (include/qphix/wilson.h:20), EvenOddClover-
  * Operator (clover.h:31), EvenOddTMWilsonOperator (twisted_mass.h:22) and

@@ -62,6 +62,10 @@ _SIGS = {
     "qphix_gpu_dslash_achimbdpsi": ([C.POINTER(OpParams), P, P, P, P, P, D, D, I_, I_, D], I_),
     "qphix_gpu_dslash_dir": ([C.POINTER(OpParams), P, P, P, I_, I_], I_),
     "qphix_gpu_clover_apply": ([P, P, P], I_),
+    "qphix_gpu_clover_build": ([P, P, I_, D, D, D], I_),
+    "qphix_gpu_clover_invert": ([P, P], I_),
+    "qphix_gpu_clover_invert_twisted": ([P, P, P, D], I_),
+    "qphix_gpu_clover_convert": ([P, P], I_),
     "qphix_gpu_eo_op_create": ([C.POINTER(OpParams), P, P, P, P, P, PP], I_),
     "qphix_gpu_eo_op_destroy": ([P], I_),
     "qphix_gpu_eo_op_apply": ([P, P, P, I_, I_], I_),

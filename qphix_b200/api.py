@@ -268,6 +268,32 @@ class TMClovDslash(Dslash):
 
 
 # ---------------------------------------------------------------------------
+# clover term on the device
+# ---------------------------------------------------------------------------
+
+
+def clover_build(clov, gauge, cb, mass, csw, csw_t=None):
+    """A = (4 + mass) + sigma.F (clover leaf, c_sw) on checkerboard cb."""
+    check(L._lib.qphix_gpu_clover_build(clov.h, gauge.h, cb, 4.0 + mass, csw, csw if csw_t is None else csw_t))
+    return clov
+
+
+def clover_invert(dst, src):
+    check(L._lib.qphix_gpu_clover_invert(dst.h, src.h))
+    return dst
+
+
+def clover_invert_twisted(dst_plus, dst_minus, src, mu):
+    check(L._lib.qphix_gpu_clover_invert_twisted(dst_plus.h, dst_minus.h, src.h, mu))
+    return dst_plus, dst_minus
+
+
+def clover_convert(dst, src):
+    check(L._lib.qphix_gpu_clover_convert(dst.h, src.h))
+    return dst
+
+
+# ---------------------------------------------------------------------------
 # even-odd operators
 # ---------------------------------------------------------------------------
 

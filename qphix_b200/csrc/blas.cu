@@ -127,8 +127,8 @@ void launch_dslash(int prec, int recon, int epi, int achi, int R, const DslashAr
 
 bool dslash_tile_ok(int prec, int R)
 {
-  if (prec == PREC_F64) return R == 1 || R == 2;
-  return R == 1 || R == 2 || R == 4;
+  if (prec == PREC_F64) return R == 1;
+  return R == 1 || R == 2;
 }
 
 }  // namespace qpx

@@ -500,9 +500,18 @@ static void require_spinor(const qphix_gpu_field_s *f, const char *what)
   if (!f || f->kind != QPHIX_GPU_SPINOR) throw Error(QPHIX_GPU_EINVAL, std::string(what) + " must be a spinor field");
 }
 
+// Fields combine if their lattices have the same shape (a field of one
+// lattice object, e.g. a resident gauge field, can serve operators whose
+// work runs on another lattice object's stream and workspace).
+static bool same_shape(const qphix_gpu_lattice_s *a, const qphix_gpu_lattice_s *b)
+{
+  return a == b || (a->dims[0] == b->dims[0] && a->dims[1] == b->dims[1] && a->dims[2] == b->dims[2] &&
+                    a->dims[3] == b->dims[3]);
+}
+
 static void require_same(const qphix_gpu_field_s *a, const qphix_gpu_field_s *b)
 {
-  if (a->lat != b->lat) throw Error(QPHIX_GPU_EINVAL, "fields belong to different lattices");
+  if (!same_shape(a->lat, b->lat)) throw Error(QPHIX_GPU_EINVAL, "fields belong to lattices of different shape");
   if (a->prec != b->prec) throw Error(QPHIX_GPU_EINVAL, "fields have different precisions");
 }
 
@@ -696,6 +705,73 @@ extern "C" int qphix_gpu_clover_apply(qphix_gpu_field res, qphix_gpu_field chi, 
 }
 
 // ===========================================================================
+// clover term construction / inversion on the device (clover_build.cu)
+// ===========================================================================
+extern "C" int qphix_gpu_clover_build(qphix_gpu_field clov, qphix_gpu_field gauge, int cb, double diag_mass,
+                                      double csw_r, double csw_t)
+{
+  return guard([&] {
+    QPX_REQUIRE(clov && clov->kind == QPHIX_GPU_CLOVER, "clov must be a clover field");
+    QPX_REQUIRE(gauge && gauge->kind == QPHIX_GPU_GAUGE && gauge->prec == PREC_F64,
+                "the clover term is built from an FP64 gauge field");
+    QPX_REQUIRE(same_shape(clov->lat, gauge->lat), "fields belong to lattices of different shape");
+    QPX_REQUIRE(cb == 0 || cb == 1, "cb must be 0 or 1");
+    auto *lat = clov->lat;
+    // tests/clover_term_qdp_w.h:133-137: the coefficients enter multiplied by 1/2
+    launch_clover_build(gauge->recon, clov->prec, lat->geom(), gauge->garg(), clov->data, lat->stride, clov->spec.vpc,
+                        cb, diag_mass, 0.5 * csw_r, 0.5 * csw_t, dim3((unsigned)((lat->vh + 63) / 64)), lat->stream);
+    check_launch();
+  });
+}
+
+extern "C" int qphix_gpu_clover_invert(qphix_gpu_field dst, qphix_gpu_field src)
+{
+  return guard([&] {
+    QPX_REQUIRE(dst && src && dst->kind == QPHIX_GPU_CLOVER && src->kind == QPHIX_GPU_CLOVER,
+                "dst and src must be clover fields");
+    QPX_REQUIRE(same_shape(dst->lat, src->lat) && dst != src, "distinct fields of one lattice shape required");
+    auto *lat = src->lat;
+    launch_clover_invert(src->prec, dst->prec, lat->geom(), src->data, lat->stride, src->spec.vpc, dst->data, nullptr,
+                         dst->spec.vpc, 0, 0.0, dim3((unsigned)((lat->vh + 63) / 64)), lat->stream);
+    check_launch();
+  });
+}
+
+extern "C" int qphix_gpu_clover_invert_twisted(qphix_gpu_field dst_plus, qphix_gpu_field dst_minus,
+                                               qphix_gpu_field src, double mu)
+{
+  return guard([&] {
+    QPX_REQUIRE(dst_plus && dst_minus && src, "null argument");
+    QPX_REQUIRE(dst_plus->kind == QPHIX_GPU_FULLCLOVER && dst_minus->kind == QPHIX_GPU_FULLCLOVER,
+                "destinations must be full clover fields");
+    QPX_REQUIRE(src->kind == QPHIX_GPU_CLOVER, "src must be a clover field");
+    QPX_REQUIRE(dst_plus->prec == dst_minus->prec, "destinations must share a precision");
+    QPX_REQUIRE(same_shape(dst_plus->lat, src->lat) && same_shape(dst_minus->lat, src->lat),
+                "fields belong to lattices of different shape");
+    auto *lat = src->lat;
+    launch_clover_invert(src->prec, dst_plus->prec, lat->geom(), src->data, lat->stride, src->spec.vpc,
+                         dst_plus->data, dst_minus->data, dst_plus->spec.vpc, 1, mu,
+                         dim3((unsigned)((lat->vh + 63) / 64)), lat->stream);
+    check_launch();
+  });
+}
+
+extern "C" int qphix_gpu_clover_convert(qphix_gpu_field dst, qphix_gpu_field src)
+{
+  return guard([&] {
+    QPX_REQUIRE(dst && src && dst->kind == src->kind &&
+                    (src->kind == QPHIX_GPU_CLOVER || src->kind == QPHIX_GPU_FULLCLOVER),
+                "dst and src must be clover fields of the same kind");
+    QPX_REQUIRE(same_shape(dst->lat, src->lat), "fields belong to lattices of different shape");
+    auto *lat = dst->lat;
+    launch_clover_convert(src->prec, dst->prec, lat->geom(), src->data, src->spec.vpc, dst->data, dst->spec.vpc,
+                          lat->stride, src->kind == QPHIX_GPU_CLOVER ? 72 : 144, dim3(nblocks_for(lat->vh)),
+                          lat->stream);
+    check_launch();
+  });
+}
+
+// ===========================================================================
 // even-odd operators
 // ===========================================================================
 extern "C" int qphix_gpu_eo_op_create(const qphix_gpu_op_params *p, qphix_gpu_field gauge, qphix_gpu_field clov,
@@ -728,12 +804,14 @@ extern "C" int qphix_gpu_eo_op_destroy(qphix_gpu_eo_op op)
   });
 }
 
-static qphix_gpu_field_s *op_tmp(qphix_gpu_eo_op_s *op, int nrhs)
+// the operator's temporary, created on the lattice (stream) of the first
+// field it is applied to
+static qphix_gpu_field_s *op_tmp(qphix_gpu_eo_op_s *op, int nrhs, qphix_gpu_lattice_s *lat = nullptr)
 {
   auto it = op->tmp.find(nrhs);
   if (it != op->tmp.end()) return it->second;
   qphix_gpu_field f = nullptr;
-  int rc = qphix_gpu_field_create(op->gauge->lat, QPHIX_GPU_SPINOR, op->gauge->prec, 0, nrhs, &f);
+  int rc = qphix_gpu_field_create(lat ? lat : op->gauge->lat, QPHIX_GPU_SPINOR, op->gauge->prec, 0, nrhs, &f);
   if (rc) throw Error(rc, g_last_error);
   op->tmp[nrhs] = f;
   return f;
@@ -744,7 +822,7 @@ static void eo_apply(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *res, qphix_gpu_fi
                      const ApplyOpts &o)
 {
   require_spinor(in, "in");
-  qphix_gpu_field_s *tmp = op_tmp(op, in->nrhs);
+  qphix_gpu_field_s *tmp = op_tmp(op, in->nrhs, in->lat);
   const auto &p = op->p;
   int other = 1 - target_cb;
   switch (p.kind) {
@@ -1655,6 +1733,7 @@ void solve_bicgstab_mixed(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opl, qphix_g
       rx.state = ds;
       blas_launch(latl, lp, nr, rx);
     };
+    op_tmp(opl, nr, latl);  // the operator's temporary must exist before graph capture
     std::string key = "bicg-ru/" + std::to_string(opl->serial) + "/" + fkey(xl) + fkey(r0) + fkey(r) + fkey(p) +
                       fkey(v) + fkey(t) + "/" + std::to_string(isign) + std::to_string(cb);
     while (true) {

@@ -8,7 +8,6 @@ void launch_dslash_bf16(int recon, int epi, int achi, int R, const DslashArgs &a
   switch (R) {
   case 1: launch_dslash_r<BF16, 1>(recon, epi, achi, a, grid, st); return;
   case 2: launch_dslash_r<BF16, 2>(recon, epi, achi, a, grid, st); return;
-  case 4: launch_dslash_r<BF16, 4>(recon, epi, achi, a, grid, st); return;
   }
   throw Error(QPHIX_GPU_EINVAL, "unsupported rhs tile for BF16");
 }

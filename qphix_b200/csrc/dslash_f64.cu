@@ -7,7 +7,6 @@ void launch_dslash_f64(int recon, int epi, int achi, int R, const DslashArgs &a,
 {
   switch (R) {
   case 1: launch_dslash_r<F64, 1>(recon, epi, achi, a, grid, st); return;
-  case 2: launch_dslash_r<F64, 2>(recon, epi, achi, a, grid, st); return;
   }
   throw Error(QPHIX_GPU_EINVAL, "unsupported rhs tile for F64");
 }

@@ -188,10 +188,17 @@ struct SpinorArg {
 template <typename P>
 struct SpinorIO;
 
+// load_raw(f, rhs, s, v, nrm): the stored values and the per-site scale
+// separately (v * nrm are the spinor's components); nrm == 1 without a norm.
 template <>
 struct SpinorIO<F64> {
   static constexpr int nchunk = 12;
   static constexpr size_t chunk_bytes = 16;
+  __device__ __forceinline__ static void load_raw(const SpinorArg &f, int rhs, long long s, double v[24], double &nrm)
+  {
+    load(f, rhs, s, v);
+    nrm = 1.0;
+  }
   __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, long long s, double v[24])
   {
     const double2 *p = reinterpret_cast<const double2 *>(f.data) + rhs * f.rhs_stride_chunks + s;
@@ -214,6 +221,11 @@ template <>
 struct SpinorIO<F32> {
   static constexpr int nchunk = 6;
   static constexpr size_t chunk_bytes = 16;
+  __device__ __forceinline__ static void load_raw(const SpinorArg &f, int rhs, long long s, float v[24], float &nrm)
+  {
+    load(f, rhs, s, v);
+    nrm = 1.0f;
+  }
   __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, long long s, float v[24])
   {
     const float4 *p = reinterpret_cast<const float4 *>(f.data) + rhs * f.rhs_stride_chunks + s;
@@ -239,6 +251,13 @@ template <typename H>
 struct SpinorIO16 {
   static constexpr int nchunk = 3;
   static constexpr size_t chunk_bytes = 16;
+  __device__ __forceinline__ static void load_raw(const SpinorArg &f, int rhs, long long s, float v[24], float &nrm)
+  {
+    const uint4 *p = reinterpret_cast<const uint4 *>(f.data) + rhs * f.rhs_stride_chunks + s;
+    nrm = __ldg(f.norm + rhs * f.stride + s);
+#pragma unroll
+    for (int k = 0; k < 3; k++) unpack8(__ldg(p + k * f.stride), v + 8 * k, H());
+  }
   __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, long long s, float v[24])
   {
     const uint4 *p = reinterpret_cast<const uint4 *>(f.data) + rhs * f.rhs_stride_chunks + s;

@@ -72,9 +72,9 @@ struct DslashArgs {
   SolverState *state;   // nullable; supplies the done flag and POST_CG's a
 };
 
-// --- spin projection (1 + sg gamma_mu) psi -> two colour vectors ----------
-template <int MU, typename T>
-__device__ __forceinline__ void project(T sg, const T *psi, cx<T> h[2][3])
+// --- spin projection (1 + SG gamma_mu) psi -> two colour vectors, SG = +-1 ---
+template <int MU, int SG, typename T>
+__device__ __forceinline__ void project(const T *psi, cx<T> h[2][3])
 {
 #pragma unroll
   for (int c = 0; c < 3; c++) {
@@ -82,26 +82,27 @@ __device__ __forceinline__ void project(T sg, const T *psi, cx<T> h[2][3])
     cx<T> p1 = {psi[(1 * 3 + c) * 2], psi[(1 * 3 + c) * 2 + 1]};
     cx<T> p2 = {psi[(2 * 3 + c) * 2], psi[(2 * 3 + c) * 2 + 1]};
     cx<T> p3 = {psi[(3 * 3 + c) * 2], psi[(3 * 3 + c) * 2 + 1]};
-    if (MU == 0) {        // h0 = p0 + sg i p3, h1 = p1 + sg i p2
-      h[0][c] = {p0.re - sg * p3.im, p0.im + sg * p3.re};
-      h[1][c] = {p1.re - sg * p2.im, p1.im + sg * p2.re};
-    } else if (MU == 1) { // h0 = p0 - sg p3, h1 = p1 + sg p2
-      h[0][c] = {p0.re - sg * p3.re, p0.im - sg * p3.im};
-      h[1][c] = {p1.re + sg * p2.re, p1.im + sg * p2.im};
-    } else if (MU == 2) { // h0 = p0 + sg i p2, h1 = p1 - sg i p3
-      h[0][c] = {p0.re - sg * p2.im, p0.im + sg * p2.re};
-      h[1][c] = {p1.re + sg * p3.im, p1.im - sg * p3.re};
-    } else {              // h0 = p0 + sg p2, h1 = p1 + sg p3
-      h[0][c] = {p0.re + sg * p2.re, p0.im + sg * p2.im};
-      h[1][c] = {p1.re + sg * p3.re, p1.im + sg * p3.im};
+    if (MU == 0) {        // h0 = p0 + SG i p3, h1 = p1 + SG i p2
+      h[0][c] = SG > 0 ? cx<T>{p0.re - p3.im, p0.im + p3.re} : cx<T>{p0.re + p3.im, p0.im - p3.re};
+      h[1][c] = SG > 0 ? cx<T>{p1.re - p2.im, p1.im + p2.re} : cx<T>{p1.re + p2.im, p1.im - p2.re};
+    } else if (MU == 1) { // h0 = p0 - SG p3, h1 = p1 + SG p2
+      h[0][c] = SG > 0 ? p0 - p3 : p0 + p3;
+      h[1][c] = SG > 0 ? p1 + p2 : p1 - p2;
+    } else if (MU == 2) { // h0 = p0 + SG i p2, h1 = p1 - SG i p3
+      h[0][c] = SG > 0 ? cx<T>{p0.re - p2.im, p0.im + p2.re} : cx<T>{p0.re + p2.im, p0.im - p2.re};
+      h[1][c] = SG > 0 ? cx<T>{p1.re + p3.im, p1.im - p3.re} : cx<T>{p1.re - p3.im, p1.im + p3.re};
+    } else {              // h0 = p0 + SG p2, h1 = p1 + SG p3
+      h[0][c] = SG > 0 ? p0 + p2 : p0 - p2;
+      h[1][c] = SG > 0 ? p1 + p3 : p1 - p3;
     }
   }
 }
 
-// --- reconstruct-accumulate of (1 + sg gamma_mu) from chi = U h -------------
-template <int MU, typename T>
-__device__ __forceinline__ void recons_add(T sg, const cx<T> ch[2][3], T *acc)
+// --- reconstruct-accumulate of (1 + SG gamma_mu) from chi = U h -------------
+template <int MU, int SG, typename T>
+__device__ __forceinline__ void recons_add(const cx<T> ch[2][3], T *acc)
 {
+  const T sg = (T)SG;  // +-1: folded into add / subtract by the compiler
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     cx<T> c0 = ch[0][c], c1 = ch[1][c];
@@ -109,22 +110,22 @@ __device__ __forceinline__ void recons_add(T sg, const cx<T> ch[2][3], T *acc)
     acc[(0 * 3 + c) * 2 + 1] += c0.im;
     acc[(1 * 3 + c) * 2] += c1.re;
     acc[(1 * 3 + c) * 2 + 1] += c1.im;
-    if (MU == 0) {        // o2 += -sg i c1, o3 += -sg i c0
+    if (MU == 0) {        // o2 += -SG i c1, o3 += -SG i c0
       acc[(2 * 3 + c) * 2] += sg * c1.im;
       acc[(2 * 3 + c) * 2 + 1] -= sg * c1.re;
       acc[(3 * 3 + c) * 2] += sg * c0.im;
       acc[(3 * 3 + c) * 2 + 1] -= sg * c0.re;
-    } else if (MU == 1) { // o2 += sg c1, o3 += -sg c0
+    } else if (MU == 1) { // o2 += SG c1, o3 += -SG c0
       acc[(2 * 3 + c) * 2] += sg * c1.re;
       acc[(2 * 3 + c) * 2 + 1] += sg * c1.im;
       acc[(3 * 3 + c) * 2] -= sg * c0.re;
       acc[(3 * 3 + c) * 2 + 1] -= sg * c0.im;
-    } else if (MU == 2) { // o2 += -sg i c0, o3 += sg i c1
+    } else if (MU == 2) { // o2 += -SG i c0, o3 += SG i c1
       acc[(2 * 3 + c) * 2] += sg * c0.im;
       acc[(2 * 3 + c) * 2 + 1] -= sg * c0.re;
       acc[(3 * 3 + c) * 2] -= sg * c1.im;
       acc[(3 * 3 + c) * 2 + 1] += sg * c1.re;
-    } else {              // o2 += sg c0, o3 += sg c1
+    } else {              // o2 += SG c0, o3 += SG c1
       acc[(2 * 3 + c) * 2] += sg * c0.re;
       acc[(2 * 3 + c) * 2 + 1] += sg * c0.im;
       acc[(3 * 3 + c) * 2] += sg * c1.re;
@@ -133,10 +134,29 @@ __device__ __forceinline__ void recons_add(T sg, const cx<T> ch[2][3], T *acc)
   }
 }
 
-// chi = coeff * U h (ADJ: U^+ h), times the twisted phase if requested
+// scale the projected half spinor once by the hop's coefficient x the
+// spinor's per-site norm (x the twisted-boundary phase): the link multiply is
+// linear, so this equals scaling its result
+template <typename T>
+__device__ __forceinline__ void scale_h(cx<T> h[2][3], T coeff, bool tw, cx<T> ph)
+{
+  if (tw) {
+    cx<T> f = {coeff * ph.re, coeff * ph.im};
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) h[s][c] = h[s][c] * f;
+  } else {
+#pragma unroll
+    for (int s = 0; s < 2; s++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) h[s][c] = coeff * h[s][c];
+  }
+}
+
+// chi = U h (ADJ: U^+ h)
 template <bool ADJ, typename T>
-__device__ __forceinline__ void link_mult(const cx<T> u[3][3], const cx<T> h[2][3], T coeff, bool tw,
-                                          cx<T> ph, cx<T> ch[2][3])
+__device__ __forceinline__ void link_mult(const cx<T> u[3][3], const cx<T> h[2][3], cx<T> ch[2][3])
 {
 #pragma unroll
   for (int s = 0; s < 2; s++) {
@@ -152,8 +172,7 @@ __device__ __forceinline__ void link_mult(const cx<T> u[3][3], const cx<T> h[2][
         v = v + cmulc(u[1][r], h[s][1]);
         v = v + cmulc(u[2][r], h[s][2]);
       }
-      if (tw) v = v * ph;
-      ch[s][r] = coeff * v;
+      ch[s][r] = v;
     }
   }
 }
@@ -208,7 +227,7 @@ __device__ __forceinline__ void full6_apply(const T *blk, const T *in, T *out, i
 }
 
 // ---------------------------------------------------------------------------
-template <typename P, int RECON, int EPI, int ACHI, int R>
+template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN>
 __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
 {
   using T = typename P::real;
@@ -243,7 +262,7 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
       nb[3][1] = s + ((t + 1 == g.nt) ? -(g.nt - 1) * sxyzt : sxyzt);
       nb[3][0] = s + ((t == 0) ? (g.nt - 1) * sxyzt : -sxyzt);
     }
-    const T sgn = (T)a.isign;
+    const T sgn = (T)ISIGN;
     T acc[R][24];
 #pragma unroll
     for (int r = 0; r < R; r++)
@@ -263,12 +282,13 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
       cx<T> ph = {(T)a.tbc[MU][0], (T)a.tbc[MU][1]};                                      \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
-        T psi[24];                                                                        \
-        SpinorIO<P>::load(a.in, rhs0 + r, nb[MU][1], psi);                               \
+        T psi[24], nrm;                                                                   \
+        SpinorIO<P>::load_raw(a.in, rhs0 + r, nb[MU][1], psi, nrm);                      \
         cx<T> h[2][3], ch[2][3];                                                          \
-        project<MU>(-sgn, psi, h);                                                        \
-        link_mult<false>(u, h, cf, tw, ph, ch);                                           \
-        recons_add<MU>(-sgn, ch, acc[r]);                                                 \
+        project<MU, -ISIGN>(psi, h);                                                      \
+        scale_h(h, cf * nrm, tw, ph);                                                     \
+        link_mult<false>(u, h, ch);                                                       \
+        recons_add<MU, -ISIGN>(ch, acc[r]);                                               \
       }                                                                                   \
     }                                                                                     \
     /* backward hop: U_mu(x - mu)^+ (1 + isign g) psi(x - mu) */                          \
@@ -280,12 +300,13 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
       cx<T> ph = {(T)a.tbc[MU][0], -(T)a.tbc[MU][1]};                                     \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
-        T psi[24];                                                                        \
-        SpinorIO<P>::load(a.in, rhs0 + r, nb[MU][0], psi);                               \
+        T psi[24], nrm;                                                                   \
+        SpinorIO<P>::load_raw(a.in, rhs0 + r, nb[MU][0], psi, nrm);                      \
         cx<T> h[2][3], ch[2][3];                                                          \
-        project<MU>(sgn, psi, h);                                                         \
-        link_mult<true>(u, h, cf, tw, ph, ch);                                            \
-        recons_add<MU>(sgn, ch, acc[r]);                                                  \
+        project<MU, ISIGN>(psi, h);                                                       \
+        scale_h(h, cf * nrm, tw, ph);                                                     \
+        link_mult<true>(u, h, ch);                                                        \
+        recons_add<MU, ISIGN>(ch, acc[r]);                                                \
       }                                                                                   \
     }                                                                                     \
   }

@@ -145,6 +145,12 @@ void launch_clover_in(int prec, Geom g, HostLayout L, const void *host, void *de
 void launch_clover_out(int prec, Geom g, void *host, const void *dev, long long stride, int vpc, int nr,
                        dim3 grid, cudaStream_t st);
 void launch_mshift(int prec, const MShiftArgs &a, dim3 grid, cudaStream_t st);
+void launch_clover_build(int recon, int prec_out, Geom geo, GaugeArg g, void *out, long long stride, int vpc, int cb,
+                         double diag_mass, double cr, double ct, dim3 grid, cudaStream_t st);
+void launch_clover_invert(int prec_in, int prec_out, Geom geo, const void *in, long long stride, int vpc_in, void *o0,
+                          void *o1, int vpc_out, int mode, double mu, dim3 grid, cudaStream_t st);
+void launch_clover_convert(int prec_in, int prec_out, Geom geo, const void *in, int vpc_in, void *out, int vpc_out,
+                           long long stride, int nr, dim3 grid, cudaStream_t st);
 
 // tile sizes compiled for each precision
 bool dslash_tile_ok(int prec, int R);
