@@ -105,6 +105,18 @@ int qphix_gpu_init(int device);
  * replay counts every kernel node it runs. */
 int qphix_gpu_launch_count(unsigned long long *out);
 
+/* ---- Dslash launch-shape autotuner (no reference counterpart: QPhiX picks
+ * its blocking by hand, Geometry(..., By, Bz, NCores, Sy, Sz, ...),
+ * include/qphix/geometry.h:130).  Each Dslash configuration (precision,
+ * links, epilogue, lattice, nrhs) is timed over its built shapes (right-hand
+ * sides per thread, lattice sites per thread) the first time it runs
+ * outside CUDA-graph capture; the fastest shape is kept for the process.
+ * Entries are listed in key order. */
+int qphix_gpu_tune_enable(int enable);
+int qphix_gpu_tune_entries(int *count);
+int qphix_gpu_tune_entry(int index, char *key, size_t key_len, int *rhs_tile, int *sites_per_thread,
+                         double *launch_us);
+
 /* ---- lattice (replaces Geometry<FT,V,S,c12>, include/qphix/geometry.h:130) */
 int qphix_gpu_lattice_create(const int latt_size[4], qphix_gpu_lattice *out);
 int qphix_gpu_lattice_destroy(qphix_gpu_lattice lat);
@@ -258,6 +270,78 @@ int qphix_gpu_blas_zero(qphix_gpu_field x);                                     
  * first call before any stream capture.  Every call shares the array, so
  * calls whose kernels overlap on the GPU race. */
 int qphix_gpu_blas_norm2_noalloc(qphix_gpu_field x, double *out_dev);
+
+/* ---- serving layer (no reference counterpart: the reference is a library
+ * called one solve at a time; this is a request loop on top of it) --------
+ * A server keeps gauge ensembles resident on the device (FP64 and low-
+ * precision 12-real links) and runs up to `slots` requests at once, each on
+ * its own worker thread, CUDA stream and device memory, so that requests of
+ * different lattice sizes and operators overlap on the GPU.  Request memory
+ * comes from one stream-ordered pool and is admitted against
+ * `hbm_budget_bytes` (ensembles included): waiting requests are taken in
+ * arrival order when a slot and the budget allow; one that does not fit may
+ * be passed by later requests at most `max_bypass` times.  A request builds
+ * its clover term on the device from the resident FP64 links and solves
+ * M x = b on the odd checkerboard (target_cb = 1, isign = +1) with
+ * qphix_gpu_solve_bicgstab_mixed (low-precision iterations, FP64 reliable
+ * updates with threshold `delta`).  Its arithmetic is independent of the
+ * other requests in flight (fixed-order reductions).
+ * Host spinors use the canonical layout [nrhs][Vh][4][3][2] (FP64); rhs and
+ * x must stay valid until qphix_gpu_server_wait returns. */
+typedef struct qphix_gpu_server_s *qphix_gpu_server;
+
+typedef struct {
+  size_t hbm_budget_bytes;
+  int slots;       /* requests in flight at once, 1 .. 64 */
+  int low_prec;    /* QPHIX_GPU_F32 / _F16 / _BF16 */
+  int max_bypass;
+  double delta;    /* reliable-update threshold, (0, 1) */
+} qphix_gpu_server_config;
+
+typedef struct {
+  int ensemble;          /* id from qphix_gpu_server_add_ensemble */
+  int op_kind;           /* QPHIX_GPU_WILSON / _CLOVER_OP / _TM / _TMCLOVER */
+  double mass;           /* bare mass, m = 1 / (2 kappa) - 4 */
+  double csw;            /* clover coefficient (clover kinds) */
+  double twisted_mass;   /* mu (twisted kinds; prec_mass_rho for TM clover) */
+  double t_boundary;     /* +1 periodic, -1 antiperiodic in t */
+  int nrhs;              /* 1 .. 32 */
+  double rsd_target;     /* relative FP64 true residual */
+  int max_iters;
+  const double *rhs;
+  double *x;
+} qphix_gpu_request;
+
+typedef struct {
+  int status;              /* QPHIX_GPU_OK, _ENOTCONV, or the failing call's code */
+  int n_iters;             /* max over the request's right-hand sides */
+  unsigned long mv_apps;
+  double true_rel_resid;   /* worst over the request's right-hand sides */
+  double queue_s;          /* submit -> admission */
+  double solve_s;          /* admission -> x written */
+  double latency_s;        /* submit -> x written */
+  size_t bytes;            /* device memory reserved for the request */
+} qphix_gpu_request_result;
+
+typedef struct {
+  long long completed, failed, waiting, bypasses;
+  int running, running_peak;
+  size_t resident_bytes, reserved_bytes, reserved_peak_bytes, pool_used_peak_bytes;
+} qphix_gpu_server_stats;
+
+/* The server runs on the calling thread's current device. */
+int qphix_gpu_server_create(const qphix_gpu_server_config *cfg, qphix_gpu_server *out);
+/* gauge: canonical layout [2 cb][4 mu][Vh][3][3][2] (FP64) */
+int qphix_gpu_server_add_ensemble(qphix_gpu_server s, const int dims[4], const double *gauge_canonical,
+                                  int *ensemble_id);
+int qphix_gpu_server_request_bytes(qphix_gpu_server s, const qphix_gpu_request *req, size_t *bytes);
+int qphix_gpu_server_submit(qphix_gpu_server s, const qphix_gpu_request *req, long long *ticket);
+int qphix_gpu_server_poll(qphix_gpu_server s, long long ticket, int *done);
+/* Blocks until done; returns the request's status and forgets the ticket. */
+int qphix_gpu_server_wait(qphix_gpu_server s, long long ticket, qphix_gpu_request_result *res);
+int qphix_gpu_server_get_stats(qphix_gpu_server s, qphix_gpu_server_stats *stats);
+/* Finishes admitted requests, drops waiting ones, frees everything. */
+int qphix_gpu_server_destroy(qphix_gpu_server s);
 
 #ifdef __cplusplus
 }

@@ -37,6 +37,30 @@ class SolveInfo(C.Structure):
                 ("seconds", C.c_double)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("slots", C.c_int), ("low_prec", C.c_int),
+                ("max_bypass", C.c_int), ("delta", C.c_double)]
+
+
+class Request(C.Structure):
+    _fields_ = [("ensemble", C.c_int), ("op_kind", C.c_int), ("mass", C.c_double), ("csw", C.c_double),
+                ("twisted_mass", C.c_double), ("t_boundary", C.c_double), ("nrhs", C.c_int),
+                ("rsd_target", C.c_double), ("max_iters", C.c_int), ("rhs", C.c_void_p), ("x", C.c_void_p)]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("n_iters", C.c_int), ("mv_apps", C.c_ulong),
+                ("true_rel_resid", C.c_double), ("queue_s", C.c_double), ("solve_s", C.c_double),
+                ("latency_s", C.c_double), ("bytes", C.c_size_t)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("completed", C.c_longlong), ("failed", C.c_longlong), ("waiting", C.c_longlong),
+                ("bypasses", C.c_longlong), ("running", C.c_int), ("running_peak", C.c_int),
+                ("resident_bytes", C.c_size_t), ("reserved_bytes", C.c_size_t),
+                ("reserved_peak_bytes", C.c_size_t), ("pool_used_peak_bytes", C.c_size_t)]
+
+
 P = C.c_void_p
 I_ = C.c_int
 D = C.c_double
@@ -47,6 +71,10 @@ _SIGS = {
     "qphix_gpu_last_error": ([], C.c_char_p),
     "qphix_gpu_init": ([I_], I_),
     "qphix_gpu_launch_count": ([C.POINTER(C.c_ulonglong)], I_),
+    "qphix_gpu_tune_enable": ([I_], I_),
+    "qphix_gpu_tune_entries": ([C.POINTER(C.c_int)], I_),
+    "qphix_gpu_tune_entry": ([I_, C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                              C.POINTER(C.c_double)], I_),
     "qphix_gpu_lattice_create": ([C.POINTER(C.c_int), PP], I_),
     "qphix_gpu_lattice_destroy": ([P], I_),
     "qphix_gpu_lattice_set_stream": ([P, P], I_),
@@ -83,6 +111,14 @@ _SIGS = {
     "qphix_gpu_blas_caxpby": ([P, P, P, P], I_),
     "qphix_gpu_blas_copy": ([P, P], I_),
     "qphix_gpu_blas_zero": ([P], I_),
+    "qphix_gpu_server_create": ([C.POINTER(ServerConfig), PP], I_),
+    "qphix_gpu_server_add_ensemble": ([P, C.POINTER(C.c_int), P, C.POINTER(C.c_int)], I_),
+    "qphix_gpu_server_request_bytes": ([P, C.POINTER(Request), C.POINTER(C.c_size_t)], I_),
+    "qphix_gpu_server_submit": ([P, C.POINTER(Request), C.POINTER(C.c_longlong)], I_),
+    "qphix_gpu_server_poll": ([P, C.c_longlong, C.POINTER(C.c_int)], I_),
+    "qphix_gpu_server_wait": ([P, C.c_longlong, C.POINTER(RequestResult)], I_),
+    "qphix_gpu_server_get_stats": ([P, C.POINTER(ServerStats)], I_),
+    "qphix_gpu_server_destroy": ([P], I_),
 }
 
 EXPORTED = sorted(_SIGS)

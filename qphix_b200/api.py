@@ -517,3 +517,120 @@ def copy(dst, src):
 
 def zero(x):
     check(L._lib.qphix_gpu_blas_zero(x.h))
+
+
+# ---------------------------------------------------------------------------
+# Dslash launch-shape autotuner
+# ---------------------------------------------------------------------------
+def tune_enable(enable=True):
+    """Switch timing of new Dslash configurations on or off (off: default shape)."""
+    lib()
+    check(L._lib.qphix_gpu_tune_enable(1 if enable else 0))
+
+
+def tune_entries():
+    """{key: (rhs_per_thread, sites_per_thread, launch_us)} for every tuned
+    Dslash configuration of this process."""
+    lib()
+    n = C.c_int(0)
+    check(L._lib.qphix_gpu_tune_entries(C.byref(n)))
+    out = {}
+    buf = C.create_string_buffer(256)
+    for i in range(n.value):
+        r, sp, us = C.c_int(0), C.c_int(0), C.c_double(0)
+        check(L._lib.qphix_gpu_tune_entry(i, buf, 256, C.byref(r), C.byref(sp), C.byref(us)))
+        out[buf.value.decode()] = (r.value, sp.value, us.value)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# serving layer
+# ---------------------------------------------------------------------------
+OP_KINDS = {"wilson": L.WILSON, "clover": L.CLOVER_OP, "tm": L.TM, "tmclover": L.TMCLOVER}
+
+
+class Server:
+    """Request loop with resident ensembles (qphix_gpu_server_* in
+    include/qphix_b200.h): `slots` solves in flight, each on its own stream,
+    admitted against an HBM budget; results are the FP64 solutions of
+    M x = b on the odd checkerboard."""
+
+    def __init__(self, hbm_budget_bytes, slots=4, low_prec="f16", max_bypass=4, delta=0.1, device=0):
+        lib()
+        check(L._lib.qphix_gpu_init(device))
+        cfg = L.ServerConfig(int(hbm_budget_bytes), int(slots), PREC[low_prec], int(max_bypass), float(delta))
+        h = C.c_void_p()
+        check(L._lib.qphix_gpu_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.dims = {}
+        self._pending = {}  # ticket -> (rhs buffer, x buffer, request struct)
+
+    def close(self):
+        if getattr(self, "h", None):
+            L._lib.qphix_gpu_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_ensemble(self, dims, gauge):
+        """gauge: complex [2, 4, Vh, 3, 3] (canonical); returns the ensemble id."""
+        g = np.asarray(gauge)
+        g = np.ascontiguousarray(np.stack([g.real, g.imag], axis=-1), dtype=np.float64)
+        arr = (C.c_int * 4)(*[int(d) for d in dims])
+        eid = C.c_int(-1)
+        check(L._lib.qphix_gpu_server_add_ensemble(self.h, arr, g.ctypes.data_as(C.c_void_p), C.byref(eid)))
+        self.dims[eid.value] = tuple(int(d) for d in dims)
+        return eid.value
+
+    @staticmethod
+    def _request(ensemble, kind, rhs, mass, csw, mu, t_boundary, rsd_target, max_iters):
+        b = np.asarray(rhs)
+        if b.ndim == 3:
+            b = b[None]
+        nrhs = b.shape[0]
+        bb = np.ascontiguousarray(np.stack([b.real, b.imag], axis=-1), dtype=np.float64)
+        xx = np.zeros_like(bb)
+        req = L.Request(int(ensemble), OP_KINDS[kind], float(mass), float(csw), float(mu), float(t_boundary),
+                        int(nrhs), float(rsd_target), int(max_iters), bb.ctypes.data, xx.ctypes.data)
+        return req, bb, xx
+
+    def request_bytes(self, ensemble, kind, rhs, mass=0.0, csw=1.0, mu=0.0, t_boundary=-1.0):
+        req, _, _ = self._request(ensemble, kind, rhs, mass, csw, mu, t_boundary, 1e-10, 1)
+        n = C.c_size_t(0)
+        check(L._lib.qphix_gpu_server_request_bytes(self.h, C.byref(req), C.byref(n)))
+        return n.value
+
+    def submit(self, ensemble, kind, rhs, mass, csw=1.0, mu=0.0, t_boundary=-1.0, rsd_target=1e-10,
+               max_iters=5000):
+        """rhs: complex [(nrhs,) Vh, 4, 3] odd-checkerboard spinors; returns a ticket."""
+        req, bb, xx = self._request(ensemble, kind, rhs, mass, csw, mu, t_boundary, rsd_target, max_iters)
+        t = C.c_longlong(0)
+        check(L._lib.qphix_gpu_server_submit(self.h, C.byref(req), C.byref(t)))
+        self._pending[t.value] = (bb, xx, req)
+        return t.value
+
+    def done(self, ticket):
+        d = C.c_int(0)
+        check(L._lib.qphix_gpu_server_poll(self.h, C.c_longlong(ticket), C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket, raise_on_error=True):
+        """(x complex [nrhs, Vh, 4, 3], result dict) of a submitted request."""
+        res = L.RequestResult()
+        rc = L._lib.qphix_gpu_server_wait(self.h, C.c_longlong(ticket), C.byref(res))
+        bb, xx, _ = self._pending.pop(ticket)
+        out = {k: getattr(res, k) for k, _ in L.RequestResult._fields_}
+        if rc != L.OK:
+            out["error"] = L._lib.qphix_gpu_last_error().decode()
+            if raise_on_error:
+                check(rc)
+        return xx[..., 0] + 1j * xx[..., 1], out
+
+    def stats(self):
+        st = L.ServerStats()
+        check(L._lib.qphix_gpu_server_get_stats(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in L.ServerStats._fields_}

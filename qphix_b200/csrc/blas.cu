@@ -108,27 +108,25 @@ void launch_mshift(int prec, const MShiftArgs &a, dim3 grid, cudaStream_t st)
   QPX_PREC_SWITCH(prec, (mshift_update_kernel<P><<<grid, QPX_BLOCK, 0, st>>>(a)));
 }
 
-void launch_dslash_f64(int recon, int epi, int achi, int R, const DslashArgs &a, dim3 grid, cudaStream_t st);
-void launch_dslash_f32(int recon, int epi, int achi, int R, const DslashArgs &a, dim3 grid, cudaStream_t st);
-void launch_dslash_f16(int recon, int epi, int achi, int R, const DslashArgs &a, dim3 grid, cudaStream_t st);
-void launch_dslash_bf16(int recon, int epi, int achi, int R, const DslashArgs &a, dim3 grid, cudaStream_t st);
+bool launch_dslash_f64(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
+                      cudaStream_t st);
+bool launch_dslash_f32(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
+                      cudaStream_t st);
+bool launch_dslash_f16(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
+                      cudaStream_t st);
+bool launch_dslash_bf16(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
+                       cudaStream_t st);
 
-void launch_dslash(int prec, int recon, int epi, int achi, int R, const DslashArgs &a, dim3 grid,
+bool launch_dslash(int prec, int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
                    cudaStream_t st)
 {
   switch (prec) {
-  case PREC_F64: launch_dslash_f64(recon, epi, achi, R, a, grid, st); return;
-  case PREC_F32: launch_dslash_f32(recon, epi, achi, R, a, grid, st); return;
-  case PREC_F16: launch_dslash_f16(recon, epi, achi, R, a, grid, st); return;
-  case PREC_BF16: launch_dslash_bf16(recon, epi, achi, R, a, grid, st); return;
+  case PREC_F64: return launch_dslash_f64(recon, epi, achi, sh, a, grid, st);
+  case PREC_F32: return launch_dslash_f32(recon, epi, achi, sh, a, grid, st);
+  case PREC_F16: return launch_dslash_f16(recon, epi, achi, sh, a, grid, st);
+  case PREC_BF16: return launch_dslash_bf16(recon, epi, achi, sh, a, grid, st);
   }
-  throw Error(QPHIX_GPU_EINVAL, "bad precision");
-}
-
-bool dslash_tile_ok(int prec, int R)
-{
-  if (prec == PREC_F64) return R == 1;
-  return R == 1 || R == 2;
+  return false;
 }
 
 }  // namespace qpx

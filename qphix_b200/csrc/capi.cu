@@ -9,6 +9,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <iterator>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -60,6 +63,23 @@ extern "C" int qphix_gpu_launch_count(unsigned long long *out)
 }
 
 static void lattice_release(qphix_gpu_lattice_s *L);
+static void field_free(qphix_gpu_field_s *f);
+
+// device memory of a lattice's fields: stream-ordered from its pool, or cudaMalloc
+static cudaError_t dev_alloc(qphix_gpu_lattice_s *L, void **p, size_t bytes)
+{
+  if (L->mempool) return cudaMallocFromPoolAsync(p, bytes, L->mempool, L->stream);
+  return cudaMalloc(p, bytes);
+}
+
+static void dev_free(qphix_gpu_lattice_s *L, bool pooled, void *p)
+{
+  if (!p) return;
+  if (pooled)
+    cudaFreeAsync(p, L->stream);
+  else
+    cudaFree(p);
+}
 
 static bool env_flag(const char *name)
 {
@@ -83,13 +103,42 @@ extern "C" int qphix_gpu_init(int device)
   });
 }
 
+static void create_lattice(const int latt[4], cudaMemPool_t pool, qphix_gpu_lattice *out);
+
 extern "C" int qphix_gpu_lattice_create(const int latt[4], qphix_gpu_lattice *out)
 {
+  return guard([&] { create_lattice(latt, nullptr, out); });
+}
+
+int qpx::lattice_create_pooled(const int latt[4], cudaMemPool_t pool, qphix_gpu_lattice_s **out)
+{
   return guard([&] {
+    QPX_REQUIRE(pool, "null memory pool");
+    create_lattice(latt, pool, out);
+  });
+}
+
+void qpx::lattice_trim(qphix_gpu_lattice_s *L)
+{
+  QPX_CUDA(cudaStreamSynchronize(L->stream));
+  for (auto &kv : L->graphs) cudaGraphExecDestroy(kv.second);
+  L->graphs.clear();
+  L->graph_nodes.clear();
+  L->graph_order.clear();
+  for (auto *f : L->pool_all) field_free(f);
+  L->pool_all.clear();
+  L->pool_free.clear();
+  if (L->staging) dev_free(L, L->mempool != nullptr, L->staging);
+  L->staging = nullptr;
+  L->staging_bytes = 0;
+}
+
+static void create_lattice(const int latt[4], cudaMemPool_t pool, qphix_gpu_lattice *out)
+{
+  {
     QPX_REQUIRE(latt && out, "null argument");
     for (int i = 0; i < 4; i++) QPX_REQUIRE(latt[i] >= 2, "every lattice extent must be >= 2");
     QPX_REQUIRE(latt[0] % 2 == 0, "Nx must be even (checkerboarding)");
-    QPX_REQUIRE((latt[1] * latt[2] * latt[3]) % 2 == 0 || true, "");
     auto *L = new qphix_gpu_lattice_s();
     try {
       for (int i = 0; i < 4; i++) L->dims[i] = latt[i];
@@ -99,6 +148,7 @@ extern "C" int qphix_gpu_lattice_create(const int latt[4], qphix_gpu_lattice *ou
       L->stride = (L->vh + 63) / 64 * 64;
       QPX_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
       L->owns_stream = true;
+      L->mempool = pool;
       // per-block partials, plus 2 x QPX_MAX_RHS doubles at the end for the
       // Richardson per-rhs scale factors
       L->partials_len = (size_t)nblocks_for(L->vh) * QPX_MAX_RHS * QPX_MAX_RED + 2 * QPX_MAX_RHS;
@@ -116,7 +166,7 @@ extern "C" int qphix_gpu_lattice_create(const int latt[4], qphix_gpu_lattice *ou
       throw;
     }
     *out = L;
-  });
+  }
 }
 
 static void lattice_release(qphix_gpu_lattice_s *L)
@@ -125,18 +175,15 @@ static void lattice_release(qphix_gpu_lattice_s *L)
   if (--L->refs > 0) return;
   if (L->stream) cudaStreamSynchronize(L->stream);
   for (auto &kv : L->graphs) cudaGraphExecDestroy(kv.second);
-  for (auto *f : L->pool_all) {
-    cudaFree(f->data);
-    cudaFree(f->norm);
-    delete f;
-  }
+  for (auto *f : L->pool_all) field_free(f);
+  if (L->staging) dev_free(L, L->mempool != nullptr, L->staging);
+  if (L->stream) cudaStreamSynchronize(L->stream);
   cudaFree(L->partials);
   cudaFree(L->ticket);
   cudaFree(L->result);
   cudaFreeHost(L->h_result);
   cudaFree(L->state);
   cudaFreeHost(L->h_state);
-  cudaFree(L->staging);
   if (L->stream && L->owns_stream) cudaStreamDestroy(L->stream);
   delete L;
 }
@@ -172,11 +219,11 @@ extern "C" long qphix_gpu_lattice_volcb(qphix_gpu_lattice L) { return L ? (long)
 static void *staging(qphix_gpu_lattice_s *L, size_t bytes)
 {
   if (bytes > L->staging_bytes) {
-    QPX_CUDA(cudaStreamSynchronize(L->stream));
-    cudaFree(L->staging);
+    if (!L->mempool) QPX_CUDA(cudaStreamSynchronize(L->stream));
+    dev_free(L, L->mempool != nullptr, L->staging);
     L->staging = nullptr;
     L->staging_bytes = 0;
-    QPX_CUDA(cudaMalloc(&L->staging, bytes));
+    QPX_CUDA(dev_alloc(L, &L->staging, bytes));
     L->staging_bytes = bytes;
   }
   return L->staging;
@@ -227,7 +274,8 @@ extern "C" int qphix_gpu_field_create(qphix_gpu_lattice L, int kind, int prec, i
       throw Error(QPHIX_GPU_EINVAL, "bad field kind");
     }
     f->bytes = rows * f->spec.nchunk * (size_t)f->spec.chunk_bytes * L->stride;
-    cudaError_t e = cudaMalloc(&f->data, f->bytes);
+    f->pooled = L->mempool != nullptr;
+    cudaError_t e = dev_alloc(L, &f->data, f->bytes);
     if (e != cudaSuccess) {
       L->refs--;
       delete f;
@@ -235,29 +283,40 @@ extern "C" int qphix_gpu_field_create(qphix_gpu_lattice L, int kind, int prec, i
     }
     cudaMemsetAsync(f->data, 0, f->bytes, L->stream);
     if (kind == QPHIX_GPU_SPINOR && prec >= PREC_F16) {
-      e = cudaMalloc(&f->norm, sizeof(float) * L->stride * f->nrhs);
+      void *nm = nullptr;
+      e = dev_alloc(L, &nm, sizeof(float) * L->stride * f->nrhs);
       if (e != cudaSuccess) {
-        cudaFree(f->data);
+        dev_free(L, f->pooled, f->data);
         L->refs--;
         delete f;
         throw Error(QPHIX_GPU_ENOMEM, std::string("norm allocation: ") + cudaGetErrorString(e));
       }
+      f->norm = static_cast<float *>(nm);
       cudaMemsetAsync(f->norm, 0, sizeof(float) * L->stride * f->nrhs, L->stream);
       f->bytes += sizeof(float) * L->stride * f->nrhs;
     }
+    L->field_bytes += f->bytes;
+    if (L->field_bytes > L->field_bytes_peak) L->field_bytes_peak = L->field_bytes;
     *out = f;
   });
+}
+
+static void field_free(qphix_gpu_field_s *f)
+{
+  qphix_gpu_lattice_s *L = f->lat;
+  if (!f->pooled) cudaStreamSynchronize(L->stream);
+  dev_free(L, f->pooled, f->data);
+  dev_free(L, f->pooled, f->norm);
+  L->field_bytes -= f->bytes;
+  delete f;
 }
 
 extern "C" int qphix_gpu_field_destroy(qphix_gpu_field f)
 {
   return guard([&] {
     if (!f) return;
-    cudaStreamSynchronize(f->lat->stream);
-    cudaFree(f->data);
-    cudaFree(f->norm);
     qphix_gpu_lattice_s *L = f->lat;
-    delete f;
+    field_free(f);
     lattice_release(L);
   });
 }
@@ -455,19 +514,197 @@ static DslashArgs base_args(const qphix_gpu_op_params &p, qphix_gpu_lattice_s *l
   return a;
 }
 
-static int pick_tile(int prec, int nrhs)
-{
-  const char *force = getenv("QPHIX_GPU_RHS_TILE");
-  if (force) {
-    int R = atoi(force);
-    if (R > 0 && nrhs % R == 0 && dslash_tile_ok(prec, R)) return R;
+namespace {
+// scoped solver temporary taken from (and returned to) the lattice's pool;
+// pool fields are allocated once and carry no lattice reference
+struct Tmp {
+  qphix_gpu_field f = nullptr;
+  qphix_gpu_lattice_s *lat;
+  Tmp(qphix_gpu_lattice_s *l, int prec, int nrhs) : lat(l)
+  {
+    for (size_t i = lat->pool_free.size(); i-- > 0;) {
+      auto *c = lat->pool_free[i];
+      if (c->prec == prec && c->nrhs == nrhs) {
+        f = c;
+        lat->pool_free.erase(lat->pool_free.begin() + i);
+        return;
+      }
+    }
+    int rc = qphix_gpu_field_create(lat, QPHIX_GPU_SPINOR, prec, 0, nrhs, &f);
+    if (rc) throw Error(rc, g_last_error);
+    lat->refs--;  // owned by the pool, freed with the lattice
+    lat->pool_all.push_back(f);
   }
-  // one right-hand side per thread: wider tiles keep R x 24 accumulators live
-  // and lose more to occupancy than they gain from link reuse (links of the
-  // other right-hand sides are re-read from L2); QPHIX_GPU_RHS_TILE overrides
-  (void)prec;
-  (void)nrhs;
-  return 1;
+  ~Tmp() { lat->pool_free.push_back(f); }
+  Tmp(const Tmp &) = delete;
+  Tmp &operator=(const Tmp &) = delete;
+  operator qphix_gpu_field_s *() const { return f; }
+};
+
+}  // namespace
+
+// ---- Dslash launch shapes and their autotuner ------------------------------
+// A shape (right-hand sides per thread R, sites per thread SP) is chosen per
+// (precision, links, epilogue, lattice, nrhs) the first time that Dslash runs
+// outside stream capture: every built shape is timed on a scratch output
+// (one warm-up and three timed launches each, CUDA events on the lattice's
+// stream) and the fastest is kept for the life of the process.  Launches
+// that differ only in their fused solver updates or reductions share the
+// entry.  QPHIX_GPU_TUNE=0 (or qphix_gpu_tune_enable(0)) switches timing off
+// and uses the default shape; QPHIX_GPU_RHS_TILE / QPHIX_GPU_SITES_PER_THREAD
+// force R / SP where that shape is built.
+namespace {
+struct TuneEntry {
+  DslashShape sh;
+  float us = 0.f;
+  int candidates = 0;
+};
+std::mutex g_tune_mu;
+std::map<std::string, TuneEntry> g_tune;
+std::atomic<int> g_tune_on{-1};
+
+bool tune_enabled()
+{
+  int v = g_tune_on.load();
+  if (v < 0) {
+    const char *e = getenv("QPHIX_GPU_TUNE");
+    v = (e && atoi(e) == 0) ? 0 : 1;
+    g_tune_on = v;
+  }
+  return v != 0;
+}
+
+dim3 dslash_grid(const qphix_gpu_lattice_s *lat, const DslashShape &sh, int nrhs)
+{
+  long long per = (long long)QPX_BLOCK * sh.SP;
+  long long nsb = (lat->vh + per - 1) / per;
+  return dim3((unsigned)(nsb * (nrhs / sh.R)));
+}
+
+bool shape_built(int prec, int recon, int epi, int achi, const DslashShape &sh, int nrhs)
+{
+  if (nrhs % sh.R) return false;
+  return launch_dslash(prec, recon, epi, achi, sh, nullptr, dim3(1), nullptr);
+}
+
+DslashShape default_shape(int prec, bool gen)
+{
+  DslashShape sh;
+  sh.gen = gen;
+  // FP32 arithmetic: two sites per thread in float2 lanes (paired FP32 ops)
+  if (!gen && prec != PREC_F64) sh.SP = 2;
+  return sh;
+}
+
+std::string tune_key(const qphix_gpu_lattice_s *lat, int prec, int recon, int epi, int achi, int nrhs)
+{
+  char buf[160];
+  snprintf(buf, sizeof(buf), "dslash p%d r%d e%d a%d %dx%dx%dx%d n%d", prec, recon, epi, achi, lat->dims[0],
+           lat->dims[1], lat->dims[2], lat->dims[3], nrhs);
+  return buf;
+}
+}  // namespace
+
+static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, int epi, int achi,
+                                const DslashArgs &a)
+{
+  const bool gen = a.dir_mask != 0xFFu || a.tbc_mask != 0;
+  if (gen) return default_shape(prec, true);
+  // forced shapes (experiments)
+  const char *fr = getenv("QPHIX_GPU_RHS_TILE"), *fs = getenv("QPHIX_GPU_SITES_PER_THREAD");
+  if (fr || fs) {
+    DslashShape sh = default_shape(prec, false);
+    if (fr) sh.R = atoi(fr);
+    if (fs) sh.SP = atoi(fs);
+    if (sh.R == 2 && !fs) sh.SP = 1;
+    if (sh.R >= 1 && sh.SP >= 1 && shape_built(prec, recon, epi, achi, sh, a.nrhs)) return sh;
+  }
+  std::vector<DslashShape> cands;
+  for (int sp = 1; sp <= 2; sp++)
+    for (int r = 1; r <= 2; r++) {
+      DslashShape sh;
+      sh.R = r;
+      sh.SP = sp;
+      if (shape_built(prec, recon, epi, achi, sh, a.nrhs)) cands.push_back(sh);
+    }
+  if (cands.size() <= 1) return cands.empty() ? default_shape(prec, false) : cands[0];
+  const std::string key = tune_key(lat, prec, recon, epi, achi, a.nrhs);
+  {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second.sh;
+  }
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  QPX_CUDA(cudaStreamIsCapturing(lat->stream, &cap));
+  if (!tune_enabled() || cap != cudaStreamCaptureStatusNone) return default_shape(prec, false);
+
+  // time every candidate writing a scratch field; no fused updates, no
+  // reductions, no solver state
+  Tmp scratch(lat, prec, a.nrhs);
+  DslashArgs t = a;
+  t.out = static_cast<qphix_gpu_field_s *>(scratch)->sarg();
+  t.post = POST_STORE;
+  t.red.mask = 0;
+  t.state = nullptr;
+  cudaEvent_t e0, e1;
+  QPX_CUDA(cudaEventCreate(&e0));
+  QPX_CUDA(cudaEventCreate(&e1));
+  TuneEntry best;
+  best.us = 1e30f;
+  best.candidates = (int)cands.size();
+  for (const auto &sh : cands) {
+    dim3 grid = dslash_grid(lat, sh, a.nrhs);
+    launch_dslash(prec, recon, epi, achi, sh, &t, grid, lat->stream);
+    check_launch();
+    cudaEventRecord(e0, lat->stream);
+    for (int i = 0; i < 3; i++) {
+      launch_dslash(prec, recon, epi, achi, sh, &t, grid, lat->stream);
+      check_launch();
+    }
+    cudaEventRecord(e1, lat->stream);
+    QPX_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    QPX_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    const float us = ms * 1000.f / 3.f;
+    if (us < best.us) {
+      best.us = us;
+      best.sh = sh;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  std::lock_guard<std::mutex> g(g_tune_mu);
+  g_tune[key] = best;
+  return best.sh;
+}
+
+extern "C" int qphix_gpu_tune_enable(int enable)
+{
+  return guard([&] { g_tune_on = enable ? 1 : 0; });
+}
+
+extern "C" int qphix_gpu_tune_entries(int *count)
+{
+  return guard([&] {
+    QPX_REQUIRE(count, "null argument");
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    *count = (int)g_tune.size();
+  });
+}
+
+extern "C" int qphix_gpu_tune_entry(int index, char *key, size_t key_len, int *rhs_tile, int *sites_per_thread,
+                                    double *launch_us)
+{
+  return guard([&] {
+    std::lock_guard<std::mutex> g(g_tune_mu);
+    QPX_REQUIRE(index >= 0 && index < (int)g_tune.size(), "tune entry index out of range");
+    auto it = g_tune.begin();
+    std::advance(it, index);
+    if (key && key_len) snprintf(key, key_len, "%s", it->first.c_str());
+    if (rhs_tile) *rhs_tile = it->second.sh.R;
+    if (sites_per_thread) *sites_per_thread = it->second.sh.SP;
+    if (launch_us) *launch_us = it->second.us;
+  });
 }
 
 static void set_reduce(DslashArgs &a, qphix_gpu_lattice_s *lat, int mask, int fin, SolverState *st)
@@ -483,15 +720,15 @@ static void set_reduce(DslashArgs &a, qphix_gpu_lattice_s *lat, int mask, int fi
 
 static void dslash_launch(qphix_gpu_lattice_s *lat, int prec, int recon, int epi, int achi, DslashArgs &a)
 {
-  int R = pick_tile(prec, a.nrhs);
+  DslashShape sh = choose_shape(lat, prec, recon, epi, achi, a);
   if (a.red.mask) {
     a.red.partials = lat->partials;
     a.red.ticket = lat->ticket;
     a.red.result = lat->result;
     a.red.nval = red_nval(a.red.mask);
   }
-  dim3 grid(nblocks_for(lat->vh), a.nrhs / R);
-  launch_dslash(prec, recon, epi, achi, R, a, grid, lat->stream);
+  if (!launch_dslash(prec, recon, epi, achi, sh, &a, dslash_grid(lat, sh, a.nrhs), lat->stream))
+    throw Error(QPHIX_GPU_EINVAL, "no Dslash kernel built for this precision / link / shape combination");
   check_launch();
 }
 
@@ -1005,32 +1242,6 @@ extern "C" int qphix_gpu_blas_zero(qphix_gpu_field x)
 // ===========================================================================
 namespace {
 
-// scoped solver temporary taken from (and returned to) the lattice's pool;
-// pool fields are allocated once and carry no lattice reference
-struct Tmp {
-  qphix_gpu_field f = nullptr;
-  qphix_gpu_lattice_s *lat;
-  Tmp(qphix_gpu_lattice_s *l, int prec, int nrhs) : lat(l)
-  {
-    for (size_t i = lat->pool_free.size(); i-- > 0;) {
-      auto *c = lat->pool_free[i];
-      if (c->prec == prec && c->nrhs == nrhs) {
-        f = c;
-        lat->pool_free.erase(lat->pool_free.begin() + i);
-        return;
-      }
-    }
-    int rc = qphix_gpu_field_create(lat, QPHIX_GPU_SPINOR, prec, 0, nrhs, &f);
-    if (rc) throw Error(rc, g_last_error);
-    lat->refs--;  // owned by the pool, freed with the lattice
-    lat->pool_all.push_back(f);
-  }
-  ~Tmp() { lat->pool_free.push_back(f); }
-  Tmp(const Tmp &) = delete;
-  Tmp &operator=(const Tmp &) = delete;
-  operator qphix_gpu_field_s *() const { return f; }
-};
-
 std::string fkey(const qphix_gpu_field_s *f) { return f ? std::to_string(f->serial) : std::string("-"); }
 
 // push the host copy of the solver state to the device
@@ -1161,6 +1372,26 @@ struct Timer {
   }
 };
 
+// An operator's fields may belong to other lattice objects of the same shape
+// (a resident gauge field shared by many solves): their streams are
+// synchronised once, so that the fields are complete before a solve's work,
+// which all runs on the stream of x's lattice, reads them.
+void sync_op_fields(const qphix_gpu_eo_op_s *op, const qphix_gpu_lattice_s *lat)
+{
+  const qphix_gpu_field_s *fs[5] = {op->gauge, op->clov, op->invclov, op->finv0, op->finv1};
+  const qphix_gpu_lattice_s *done[5];
+  int nd = 0;
+  for (const auto *f : fs) {
+    if (!f || f->lat == lat) continue;
+    QPX_REQUIRE(same_shape(f->lat, lat), "operator fields belong to a lattice of different shape");
+    bool seen = false;
+    for (int i = 0; i < nd; i++) seen = seen || done[i] == f->lat;
+    if (seen) continue;
+    QPX_CUDA(cudaStreamSynchronize(f->lat->stream));
+    done[nd++] = f->lat;
+  }
+}
+
 void check_solver_fields(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs)
 {
   QPX_REQUIRE(op, "null operator");
@@ -1169,6 +1400,7 @@ void check_solver_fields(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_
   require_same(x, rhs);
   require_same(x, op->gauge);
   QPX_REQUIRE(x->nrhs == rhs->nrhs, "rhs count mismatch");
+  sync_op_fields(op, x->lat);
 }
 
 // true residual |b - M x|^2 per rhs (and relative), t: scratch
@@ -1502,11 +1734,13 @@ void solve_richardson(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opi, int inner, 
   check_solver_fields(op, x, rhs);
   QPX_REQUIRE(opi, "null inner operator");
   auto *lat = x->lat;
-  // the inner operator may live on its own lattice object (QPhiX gives the
-  // inner solver its own Geometry) of the same shape; the two streams are
-  // ordered by synchronising at each hand-over
-  auto *lati = opi->gauge->lat;
-  for (int d = 0; d < 4; d++) QPX_REQUIRE(lati->dims[d] == lat->dims[d], "inner and outer lattices differ");
+  // the inner operator's fields may live on another lattice object of the
+  // same shape (QPhiX gives the inner solver its own Geometry): that stream
+  // is synchronised once, so the fields are complete, and every step of the
+  // solve, inner temporaries included, then runs on x's lattice and stream
+  QPX_REQUIRE(same_shape(opi->gauge->lat, lat), "inner and outer lattices differ");
+  sync_op_fields(opi, lat);
+  auto *lati = lat;
   const int nr = x->nrhs, prec = x->prec, iprec = opi->gauge->prec;
   Timer timer(lat);
   Tmp r(lat, prec, nr), tmp(lat, prec, nr), dx(lat, prec, nr);
@@ -1554,12 +1788,11 @@ void solve_richardson(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opi, int inner, 
         }
         QPX_CUDA(cudaMemcpyAsync(d_scales, sc.data(), sizeof(double) * 2 * QPX_MAX_RHS, cudaMemcpyHostToDevice,
                                  lat->stream));
-        convert_field(rin, r, Coef{0, 0, d_scales, nullptr}, nullptr);  // on the outer stream
+        convert_field(rin, r, Coef{0, 0, d_scales, nullptr}, nullptr);
         BlasCall z;
         z.op = B_ZERO;
         z.x = dxin;
         blas_launch(lat, iprec, nr, z);
-        if (lati != lat) QPX_CUDA(cudaStreamSynchronize(lat->stream));
         if (inner == QPHIX_GPU_SOLVER_BICGSTAB)
           solve_bicgstab(opi, dxin, rin, inner_rsd.data(), inner_max, isign, cb, ii.data(), false);
         else if (inner == QPHIX_GPU_SOLVER_MR)
@@ -1567,8 +1800,7 @@ void solve_richardson(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opi, int inner, 
         else
           solve_cg(opi, dxin, rin, inner_rsd.data(), inner_max, isign, cb, ii.data(), false);
         mv_inner += ii[0].mv_apps;
-        convert_field(dx, dxin, Coef{0, 0, d_scales + QPX_MAX_RHS, nullptr}, nullptr);  // inner stream
-        if (lati != lat) QPX_CUDA(cudaStreamSynchronize(lati->stream));
+        convert_field(dx, dxin, Coef{0, 0, d_scales + QPX_MAX_RHS, nullptr}, nullptr);
         eo_apply(op, tmp, dx, isign, cb, ApplyOpts());
         mv_outer++;
         BlasCall u;
@@ -1622,18 +1854,16 @@ void solve_bicgstab_mixed(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opl, qphix_g
   check_solver_fields(op, x, rhs);
   QPX_REQUIRE(opl, "null low-precision operator");
   auto *lat = x->lat;
-  auto *latl = opl->gauge->lat;
-  for (int d = 0; d < 4; d++) QPX_REQUIRE(latl->dims[d] == lat->dims[d], "the two operators' lattices differ");
+  // the low-precision operator's fields may live on another lattice object of
+  // the same shape: that stream is synchronised once, and every step of the
+  // solve then runs on x's lattice and stream
+  QPX_REQUIRE(same_shape(opl->gauge->lat, lat), "the two operators' lattices differ");
+  sync_op_fields(opl, lat);
+  auto *latl = lat;
   const int nr = x->nrhs, prec = x->prec, lp = opl->gauge->prec;
   Timer timer(lat);
   Tmp rh(lat, prec, nr), th(lat, prec, nr);
   Tmp r0(latl, lp, nr), r(latl, lp, nr), p(latl, lp, nr), v(latl, lp, nr), t(latl, lp, nr), xl(latl, lp, nr);
-  auto sync_hi = [&] {
-    if (latl != lat) QPX_CUDA(cudaStreamSynchronize(lat->stream));
-  };
-  auto sync_lo = [&] {
-    if (latl != lat) QPX_CUDA(cudaStreamSynchronize(latl->stream));
-  };
   std::vector<double> bn = norm2_host(rhs);
   // true residual in FP64 -> rh, |rh|^2
   auto true_r = [&]() {
@@ -1660,7 +1890,6 @@ void solve_bicgstab_mixed(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opl, qphix_g
   if (!all) {
     // r = r0 = convert(rh); xl = p = v = 0
     convert_field(r, rh, cval(1.0), nullptr);
-    sync_hi();
     BlasCall cpy;
     cpy.op = B_COPY;
     cpy.x = r;
@@ -1742,7 +1971,6 @@ void solve_bicgstab_mixed(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opl, qphix_g
       low_iters = H.iter;
       // reliable update for every active rhs: x += xl, xl = 0, rh = b - M x
       convert_field(x, xl, cval(1.0), nullptr, 1);
-      sync_lo();
       BlasCall zx;
       zx.op = B_ZERO;
       zx.x = xl;
@@ -1759,7 +1987,6 @@ void solve_bicgstab_mixed(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opl, qphix_g
       if (all || out_of_iters) break;
       // r = convert(rh); rho = <r0, r>; beta from it; restart the graph
       convert_field(r, rh, cval(1.0), nullptr);
-      sync_hi();
       BlasCall dt;
       dt.op = B_DOT;
       dt.x = r0;

@@ -3,13 +3,10 @@
 
 namespace qpx {
 
-void launch_dslash_bf16(int recon, int epi, int achi, int R, const DslashArgs &a, dim3 grid, cudaStream_t st)
+bool launch_dslash_bf16(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
+                     cudaStream_t st)
 {
-  switch (R) {
-  case 1: launch_dslash_r<BF16, 1>(recon, epi, achi, a, grid, st); return;
-  case 2: launch_dslash_r<BF16, 2>(recon, epi, achi, a, grid, st); return;
-  }
-  throw Error(QPHIX_GPU_EINVAL, "unsupported rhs tile for BF16");
+  return launch_dslash_p<BF16>(recon, epi, achi, sh, a, grid, st);
 }
 
 }  // namespace qpx

@@ -2,49 +2,85 @@
 // precision lives in its own translation unit so they compile in parallel.
 #pragma once
 
+#include <type_traits>
+
 #include "qpx_finalize.cuh"
 #include "qpx_host.h"
 
 namespace qpx {
 
-template <typename P, int RECON, int R, int S>
-void launch_dslash_prs(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStream_t st)
+template <typename P, int RECON, int R, int S, int SP, bool GEN>
+void launch_dslash_k(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStream_t st)
 {
   dim3 block(QPX_BLOCK);
   if (achi == ACHI_NONE) {
     switch (epi) {
-    case EPI_NONE: dslash_kernel<P, RECON, EPI_NONE, ACHI_NONE, R, S><<<grid, block, 0, st>>>(a); return;
-    case EPI_CLOV: dslash_kernel<P, RECON, EPI_CLOV, ACHI_NONE, R, S><<<grid, block, 0, st>>>(a); return;
-    case EPI_TMINV: dslash_kernel<P, RECON, EPI_TMINV, ACHI_NONE, R, S><<<grid, block, 0, st>>>(a); return;
-    case EPI_FCLOV: dslash_kernel<P, RECON, EPI_FCLOV, ACHI_NONE, R, S><<<grid, block, 0, st>>>(a); return;
+    case EPI_NONE: dslash_kernel<P, RECON, EPI_NONE, ACHI_NONE, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
+    case EPI_CLOV: dslash_kernel<P, RECON, EPI_CLOV, ACHI_NONE, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
+    case EPI_TMINV: dslash_kernel<P, RECON, EPI_TMINV, ACHI_NONE, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
+    case EPI_FCLOV: dslash_kernel<P, RECON, EPI_FCLOV, ACHI_NONE, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
     }
   } else if (epi == EPI_NONE) {
     switch (achi) {
-    case ACHI_ALPHA: dslash_kernel<P, RECON, EPI_NONE, ACHI_ALPHA, R, S><<<grid, block, 0, st>>>(a); return;
-    case ACHI_CLOV: dslash_kernel<P, RECON, EPI_NONE, ACHI_CLOV, R, S><<<grid, block, 0, st>>>(a); return;
-    case ACHI_TM: dslash_kernel<P, RECON, EPI_NONE, ACHI_TM, R, S><<<grid, block, 0, st>>>(a); return;
+    case ACHI_ALPHA: dslash_kernel<P, RECON, EPI_NONE, ACHI_ALPHA, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
+    case ACHI_CLOV: dslash_kernel<P, RECON, EPI_NONE, ACHI_CLOV, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
+    case ACHI_TM: dslash_kernel<P, RECON, EPI_NONE, ACHI_TM, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
     }
   }
   throw Error(QPHIX_GPU_EINVAL, "unsupported dslash epilogue combination");
 }
 
 // isign is a template parameter: the projector signs become adds / subtracts
-template <typename P, int RECON, int R>
-void launch_dslash_pr(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStream_t st)
+template <typename P, int RECON, int R, int SP, bool GEN>
+void launch_dslash_s(int epi, int achi, const DslashArgs *a, dim3 grid, cudaStream_t st)
 {
-  if (a.isign == 1)
-    launch_dslash_prs<P, RECON, R, 1>(epi, achi, a, grid, st);
+  if (!a) return;  // shape query
+  if (a->isign == 1)
+    launch_dslash_k<P, RECON, R, 1, SP, GEN>(epi, achi, *a, grid, st);
   else
-    launch_dslash_prs<P, RECON, R, -1>(epi, achi, a, grid, st);
+    launch_dslash_k<P, RECON, R, -1, SP, GEN>(epi, achi, *a, grid, st);
 }
 
-template <typename P, int R>
-void launch_dslash_r(int recon, int epi, int achi, const DslashArgs &a, dim3 grid, cudaStream_t st)
+// The shapes built for storage P.  a == nullptr: only report whether the
+// shape exists.  Returns false for a shape that is not built.
+//   general path (dir mask, twisted phases): R = 1, SP = 1
+//   fast path: R = 1 SP = 1 for every precision; for FP32 arithmetic also
+//   SP = 2 (both link kinds) and R = 2 (12-real links)
+template <typename P>
+bool launch_dslash_p(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
+                     cudaStream_t st)
 {
-  if (recon == 12)
-    launch_dslash_pr<P, 12, R>(epi, achi, a, grid, st);
-  else
-    launch_dslash_pr<P, 18, R>(epi, achi, a, grid, st);
+  constexpr bool fp32 = std::is_same<typename P::real, float>::value;
+  if (recon != 12 && recon != 18) return false;
+  if (sh.gen) {
+    if (sh.R != 1 || sh.SP != 1) return false;
+    if (recon == 12)
+      launch_dslash_s<P, 12, 1, 1, true>(epi, achi, a, grid, st);
+    else
+      launch_dslash_s<P, 18, 1, 1, true>(epi, achi, a, grid, st);
+    return true;
+  }
+  if (sh.R == 1 && sh.SP == 1) {
+    if (recon == 12)
+      launch_dslash_s<P, 12, 1, 1, false>(epi, achi, a, grid, st);
+    else
+      launch_dslash_s<P, 18, 1, 1, false>(epi, achi, a, grid, st);
+    return true;
+  }
+  if constexpr (fp32) {
+    if (sh.R == 1 && sh.SP == 2) {
+      if (recon == 12)
+        launch_dslash_s<P, 12, 1, 2, false>(epi, achi, a, grid, st);
+      else
+        launch_dslash_s<P, 18, 1, 2, false>(epi, achi, a, grid, st);
+      return true;
+    }
+    if (sh.R == 2 && sh.SP == 1 && recon == 12) {
+      launch_dslash_s<P, 12, 2, 1, false>(epi, achi, a, grid, st);
+      return true;
+    }
+  }
+  return false;
 }
 
 }  // namespace qpx

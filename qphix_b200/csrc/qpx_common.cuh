@@ -56,6 +56,63 @@ template <typename T>
 __device__ __forceinline__ cx<T> itimes(cx<T> a) { return {-a.im, a.re}; }
 
 // ---------------------------------------------------------------------------
+// Two sites per thread: the lanes of a float2 hold the same component of two
+// lattice sites, so that Blackwell's paired FP32 instructions (FADD2, FMUL2,
+// FFMA2; IEEE round-to-nearest per lane, like their scalar forms) do the
+// work of two scalar instructions.  Every operation below is lane-wise.
+// ---------------------------------------------------------------------------
+using f2 = float2;
+__device__ __forceinline__ f2 operator+(f2 a, f2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ f2 operator-(f2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ f2 operator-(f2 a, f2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ f2 operator*(f2 a, f2 b) { return __fmul2_rn(a, b); }
+
+// fused multiply-add c + a b for every arithmetic type
+__device__ __forceinline__ double mad(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float mad(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ f2 mad(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
+
+// a scalar broadcast to the arithmetic type (both lanes for f2)
+template <typename T>
+__device__ __forceinline__ T splat(double v) { return (T)v; }
+template <>
+__device__ __forceinline__ f2 splat<f2>(double v) { return make_float2((float)v, (float)v); }
+
+// lane l of a value (l = 0 for scalar types)
+__device__ __forceinline__ double lane(double v, int) { return v; }
+__device__ __forceinline__ float lane(float v, int) { return v; }
+__device__ __forceinline__ float lane(f2 v, int l) { return l ? v.y : v.x; }
+
+// complex products with explicit fused multiply-adds
+// c + a b
+template <typename T>
+__device__ __forceinline__ cx<T> cmad(cx<T> a, cx<T> b, cx<T> c)
+{
+  return {mad(a.re, b.re, mad(-a.im, b.im, c.re)), mad(a.re, b.im, mad(a.im, b.re, c.im))};
+}
+// c + conj(a) b
+template <typename T>
+__device__ __forceinline__ cx<T> cmadc(cx<T> a, cx<T> b, cx<T> c)
+{
+  return {mad(a.re, b.re, mad(a.im, b.im, c.re)), mad(a.re, b.im, mad(-a.im, b.re, c.im))};
+}
+// a b
+template <typename T>
+__device__ __forceinline__ cx<T> cmul(cx<T> a, cx<T> b)
+{
+  return {mad(a.re, b.re, -(a.im * b.im)), mad(a.re, b.im, a.im * b.re)};
+}
+// conj(a) b
+template <typename T>
+__device__ __forceinline__ cx<T> cmulcf(cx<T> a, cx<T> b)
+{
+  return {mad(a.re, b.re, a.im * b.im), mad(a.re, b.im, -(a.im * b.re))};
+}
+// real s times complex a
+template <typename T>
+__device__ __forceinline__ cx<T> rmul(T s, cx<T> a) { return {s * a.re, s * a.im}; }
+
+// ---------------------------------------------------------------------------
 // precision traits
 // ---------------------------------------------------------------------------
 struct F64 {
@@ -303,9 +360,11 @@ struct GaugeArg {
 template <typename T>
 __device__ __forceinline__ void recon12(cx<T> u[3][3])
 {
-  u[2][0] = conj(u[0][1] * u[1][2] - u[0][2] * u[1][1]);
-  u[2][1] = conj(u[0][2] * u[1][0] - u[0][0] * u[1][2]);
-  u[2][2] = conj(u[0][0] * u[1][1] - u[0][1] * u[1][0]);
+  // a b - c d with fused products: cmad(-c, d, a b)
+  const cx<T> n02 = {-u[0][2].re, -u[0][2].im}, n00 = {-u[0][0].re, -u[0][0].im}, n01 = {-u[0][1].re, -u[0][1].im};
+  u[2][0] = conj(cmad(n02, u[1][1], cmul(u[0][1], u[1][2])));
+  u[2][1] = conj(cmad(n00, u[1][2], cmul(u[0][2], u[1][0])));
+  u[2][2] = conj(cmad(n01, u[1][0], cmul(u[0][0], u[1][1])));
 }
 
 template <typename P, int RECON>

@@ -18,6 +18,7 @@
 #pragma once
 
 #include "qpx_common.cuh"
+#include "qpx_lanes.cuh"
 #include "qpx_reduce.cuh"
 
 namespace qpx {
@@ -99,39 +100,44 @@ __device__ __forceinline__ void project(const T *psi, cx<T> h[2][3])
 }
 
 // --- reconstruct-accumulate of (1 + SG gamma_mu) from chi = U h -------------
+// QPX_ADD(k, v): acc[k] += SG v ; QPX_SUB(k, v): acc[k] -= SG v (signs
+// resolved at compile time)
 template <int MU, int SG, typename T>
 __device__ __forceinline__ void recons_add(const cx<T> ch[2][3], T *acc)
 {
-  const T sg = (T)SG;  // +-1: folded into add / subtract by the compiler
+#define QPX_ADD(k, v) (SG > 0 ? (acc[k] = acc[k] + (v)) : (acc[k] = acc[k] - (v)))
+#define QPX_SUB(k, v) (SG > 0 ? (acc[k] = acc[k] - (v)) : (acc[k] = acc[k] + (v)))
 #pragma unroll
   for (int c = 0; c < 3; c++) {
     cx<T> c0 = ch[0][c], c1 = ch[1][c];
-    acc[(0 * 3 + c) * 2] += c0.re;
-    acc[(0 * 3 + c) * 2 + 1] += c0.im;
-    acc[(1 * 3 + c) * 2] += c1.re;
-    acc[(1 * 3 + c) * 2 + 1] += c1.im;
+    acc[(0 * 3 + c) * 2] = acc[(0 * 3 + c) * 2] + c0.re;
+    acc[(0 * 3 + c) * 2 + 1] = acc[(0 * 3 + c) * 2 + 1] + c0.im;
+    acc[(1 * 3 + c) * 2] = acc[(1 * 3 + c) * 2] + c1.re;
+    acc[(1 * 3 + c) * 2 + 1] = acc[(1 * 3 + c) * 2 + 1] + c1.im;
     if (MU == 0) {        // o2 += -SG i c1, o3 += -SG i c0
-      acc[(2 * 3 + c) * 2] += sg * c1.im;
-      acc[(2 * 3 + c) * 2 + 1] -= sg * c1.re;
-      acc[(3 * 3 + c) * 2] += sg * c0.im;
-      acc[(3 * 3 + c) * 2 + 1] -= sg * c0.re;
+      QPX_ADD((2 * 3 + c) * 2, c1.im);
+      QPX_SUB((2 * 3 + c) * 2 + 1, c1.re);
+      QPX_ADD((3 * 3 + c) * 2, c0.im);
+      QPX_SUB((3 * 3 + c) * 2 + 1, c0.re);
     } else if (MU == 1) { // o2 += SG c1, o3 += -SG c0
-      acc[(2 * 3 + c) * 2] += sg * c1.re;
-      acc[(2 * 3 + c) * 2 + 1] += sg * c1.im;
-      acc[(3 * 3 + c) * 2] -= sg * c0.re;
-      acc[(3 * 3 + c) * 2 + 1] -= sg * c0.im;
+      QPX_ADD((2 * 3 + c) * 2, c1.re);
+      QPX_ADD((2 * 3 + c) * 2 + 1, c1.im);
+      QPX_SUB((3 * 3 + c) * 2, c0.re);
+      QPX_SUB((3 * 3 + c) * 2 + 1, c0.im);
     } else if (MU == 2) { // o2 += -SG i c0, o3 += SG i c1
-      acc[(2 * 3 + c) * 2] += sg * c0.im;
-      acc[(2 * 3 + c) * 2 + 1] -= sg * c0.re;
-      acc[(3 * 3 + c) * 2] -= sg * c1.im;
-      acc[(3 * 3 + c) * 2 + 1] += sg * c1.re;
+      QPX_ADD((2 * 3 + c) * 2, c0.im);
+      QPX_SUB((2 * 3 + c) * 2 + 1, c0.re);
+      QPX_SUB((3 * 3 + c) * 2, c1.im);
+      QPX_ADD((3 * 3 + c) * 2 + 1, c1.re);
     } else {              // o2 += SG c0, o3 += SG c1
-      acc[(2 * 3 + c) * 2] += sg * c0.re;
-      acc[(2 * 3 + c) * 2 + 1] += sg * c0.im;
-      acc[(3 * 3 + c) * 2] += sg * c1.re;
-      acc[(3 * 3 + c) * 2 + 1] += sg * c1.im;
+      QPX_ADD((2 * 3 + c) * 2, c0.re);
+      QPX_ADD((2 * 3 + c) * 2 + 1, c0.im);
+      QPX_ADD((3 * 3 + c) * 2, c1.re);
+      QPX_ADD((3 * 3 + c) * 2 + 1, c1.im);
     }
   }
+#undef QPX_ADD
+#undef QPX_SUB
 }
 
 // scale the projected half spinor once by the hop's coefficient x the
@@ -145,12 +151,12 @@ __device__ __forceinline__ void scale_h(cx<T> h[2][3], T coeff, bool tw, cx<T> p
 #pragma unroll
     for (int s = 0; s < 2; s++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) h[s][c] = h[s][c] * f;
+      for (int c = 0; c < 3; c++) h[s][c] = cmul(h[s][c], f);
   } else {
 #pragma unroll
     for (int s = 0; s < 2; s++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) h[s][c] = coeff * h[s][c];
+      for (int c = 0; c < 3; c++) h[s][c] = rmul(coeff, h[s][c]);
   }
 }
 
@@ -164,13 +170,13 @@ __device__ __forceinline__ void link_mult(const cx<T> u[3][3], const cx<T> h[2][
     for (int r = 0; r < 3; r++) {
       cx<T> v;
       if (!ADJ) {
-        v = u[r][0] * h[s][0];
-        v = v + u[r][1] * h[s][1];
-        v = v + u[r][2] * h[s][2];
+        v = cmul(u[r][0], h[s][0]);
+        v = cmad(u[r][1], h[s][1], v);
+        v = cmad(u[r][2], h[s][2], v);
       } else {
-        v = cmulc(u[0][r], h[s][0]);
-        v = v + cmulc(u[1][r], h[s][1]);
-        v = v + cmulc(u[2][r], h[s][2]);
+        v = cmulcf(u[0][r], h[s][0]);
+        v = cmadc(u[1][r], h[s][1], v);
+        v = cmadc(u[2][r], h[s][2], v);
       }
       ch[s][r] = v;
     }
@@ -188,15 +194,15 @@ __device__ __forceinline__ void herm6_apply(const T *blk, const T *in, T *out, i
 #pragma unroll
   for (int i = 0; i < 6; i++) x[i] = {in[((2 * b + i / 3) * 3 + i % 3) * 2], in[((2 * b + i / 3) * 3 + i % 3) * 2 + 1]};
 #pragma unroll
-  for (int i = 0; i < 6; i++) y[i] = blk[i] * x[i];
+  for (int i = 0; i < 6; i++) y[i] = rmul(blk[i], x[i]);
 #pragma unroll
   for (int i = 1; i < 6; i++) {
 #pragma unroll
     for (int j = 0; j < i; j++) {
       int od = i * (i - 1) / 2 + j;
       cx<T> a = {blk[6 + 2 * od], blk[6 + 2 * od + 1]};
-      y[i] = y[i] + a * x[j];
-      y[j] = y[j] + cmulc(a, x[i]);
+      y[i] = cmad(a, x[j], y[i]);
+      y[j] = cmadc(a, x[i], y[j]);
     }
   }
 #pragma unroll
@@ -215,75 +221,136 @@ __device__ __forceinline__ void full6_apply(const T *blk, const T *in, T *out, i
   for (int i = 0; i < 6; i++) x[i] = {in[((2 * b + i / 3) * 3 + i % 3) * 2], in[((2 * b + i / 3) * 3 + i % 3) * 2 + 1]};
 #pragma unroll
   for (int i = 0; i < 6; i++) {
-    cx<T> y = {0, 0};
+    cx<T> y = cmul(cx<T>{blk[i * 12], blk[i * 12 + 1]}, x[0]);
 #pragma unroll
-    for (int j = 0; j < 6; j++) {
+    for (int j = 1; j < 6; j++) {
       cx<T> a = {blk[(i * 6 + j) * 2], blk[(i * 6 + j) * 2 + 1]};
-      y = y + a * x[j];
+      y = cmad(a, x[j], y);
     }
     out[((2 * b + i / 3) * 3 + i % 3) * 2] = y.re;
     out[((2 * b + i / 3) * 3 + i % 3) * 2 + 1] = y.im;
   }
 }
 
+// rows 2j, 2j+1 of a full complex 6x6 block (24 reals, row-major) applied to
+// the block-b half of `in`
+template <typename T>
+__device__ __forceinline__ void full6_rows(const T *rows, const T *in, T *out, int b, int j)
+{
+  cx<T> x[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) x[i] = {in[((2 * b + i / 3) * 3 + i % 3) * 2], in[((2 * b + i / 3) * 3 + i % 3) * 2 + 1]};
+#pragma unroll
+  for (int q = 0; q < 2; q++) {
+    const int i = 2 * j + q;
+    cx<T> y = cmul(cx<T>{rows[q * 12], rows[q * 12 + 1]}, x[0]);
+#pragma unroll
+    for (int k = 1; k < 6; k++) y = cmad(cx<T>{rows[q * 12 + 2 * k], rows[q * 12 + 2 * k + 1]}, x[k], y);
+    out[((2 * b + i / 3) * 3 + i % 3) * 2] = y.re;
+    out[((2 * b + i / 3) * 3 + i % 3) * 2 + 1] = y.im;
+  }
+}
+
+// per-lane values of a lane-generic type from SP doubles
+__device__ __forceinline__ void lanes_set(double &d, const double *v) { d = v[0]; }
+__device__ __forceinline__ void lanes_set(float &d, const double *v) { d = (float)v[0]; }
+__device__ __forceinline__ void lanes_set(f2 &d, const double *v) { d = make_float2((float)v[0], (float)v[1]); }
+
 // ---------------------------------------------------------------------------
-template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN>
+// P      storage precision (arithmetic in P::real, or float2 lanes for SP = 2)
+// RECON  12- or 18-real links
+// EPI, ACHI  the operator epilogue (see the enums above)
+// R      right-hand sides per thread (SP = 1)
+// ISIGN  +1: D, -1: D^dagger
+// SP     lattice sites per thread: 1, or 2 in float2 lanes (FP32 arithmetic)
+// GEN    honour a.dir_mask and twisted boundary phases.  Without GEN every
+//        hop is taken and no phase applied: the hops are then straight-line
+//        code and the compiler can schedule every load early.
+// Blocks cover (site block, rhs tile) pairs with the rhs tile varying
+// fastest, so the blocks that share a site block (and its links) run
+// together and the links of the later right-hand sides come from L2.
+template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN, int SP, bool GEN>
 __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
 {
-  using T = typename P::real;
+  using L = Lanes<P, SP>;
+  using T = typename L::T;
+  static_assert(SP == 1 || R == 1, "two sites per thread take one right-hand side");
   if (a.state && a.state->done) return;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  const int rhs0 = blockIdx.y * R;
-  const bool active = s < a.geom.vh;
+  const int ntiles = a.nrhs / R;
+  const int tile = blockIdx.x % ntiles;
+  const int sblock = blockIdx.x / ntiles;
+  const int rhs0 = tile * R;
+  int s[SP];
+  bool act[SP];
+  if (SP == 1) {
+    s[0] = sblock * QPX_BLOCK + threadIdx.x;
+    act[0] = s[0] < a.geom.vh;
+  } else {
+    // each warp owns 64 consecutive sites: lane l takes sites l and l + 32,
+    // so every load instruction of the warp reads 32 consecutive sites
+    const int base = (sblock * QPX_BLOCK + (threadIdx.x & ~31)) * 2 + (threadIdx.x & 31);
+    s[0] = base;
+    act[0] = base < a.geom.vh;
+    act[SP - 1] = base + 32 < a.geom.vh;
+    s[SP - 1] = act[SP - 1] ? base + 32 : base;
+  }
   double red[R][QPX_MAX_RED];
 #pragma unroll
   for (int r = 0; r < R; r++)
 #pragma unroll
     for (int k = 0; k < QPX_MAX_RED; k++) red[r][k] = 0.0;
 
-  if (active) {
+  if (act[0]) {
     const Geom &g = a.geom;
-    int xh, y, z, t, par;
-    site_coords(g, s, a.cb, xh, y, z, t, par);
-    // neighbour cb indices
     const int sxy = g.nxh;
     const int sxyz = g.nxh * g.ny;
     const int sxyzt = sxyz * g.nz;
-    int nb[4][2];  // [mu][0 back, 1 forward]
-    {
-      int xf = (par == 0) ? xh : ((xh + 1 == g.nxh) ? 0 : xh + 1);
-      int xb = (par == 1) ? xh : ((xh == 0) ? g.nxh - 1 : xh - 1);
-      nb[0][1] = s - xh + xf;
-      nb[0][0] = s - xh + xb;
-      nb[1][1] = s + ((y + 1 == g.ny) ? -(g.ny - 1) * sxy : sxy);
-      nb[1][0] = s + ((y == 0) ? (g.ny - 1) * sxy : -sxy);
-      nb[2][1] = s + ((z + 1 == g.nz) ? -(g.nz - 1) * sxyz : sxyz);
-      nb[2][0] = s + ((z == 0) ? (g.nz - 1) * sxyz : -sxyz);
-      nb[3][1] = s + ((t + 1 == g.nt) ? -(g.nt - 1) * sxyzt : sxyzt);
-      nb[3][0] = s + ((t == 0) ? (g.nt - 1) * sxyzt : -sxyzt);
+    int nb[4][2][SP];  // [mu][0 back, 1 forward][lane]
+    bool tlast[SP], tfirst[SP];
+#pragma unroll
+    for (int l = 0; l < SP; l++) {
+      int xh, y, z, t, par;
+      const int sl = s[l];
+      site_coords(g, sl, a.cb, xh, y, z, t, par);
+      const int xf = (par == 0) ? xh : ((xh + 1 == g.nxh) ? 0 : xh + 1);
+      const int xb = (par == 1) ? xh : ((xh == 0) ? g.nxh - 1 : xh - 1);
+      nb[0][1][l] = sl - xh + xf;
+      nb[0][0][l] = sl - xh + xb;
+      nb[1][1][l] = sl + ((y + 1 == g.ny) ? -(g.ny - 1) * sxy : sxy);
+      nb[1][0][l] = sl + ((y == 0) ? (g.ny - 1) * sxy : -sxy);
+      nb[2][1][l] = sl + ((z + 1 == g.nz) ? -(g.nz - 1) * sxyz : sxyz);
+      nb[2][0][l] = sl + ((z == 0) ? (g.nz - 1) * sxyz : -sxyz);
+      nb[3][1][l] = sl + ((t + 1 == g.nt) ? -(g.nt - 1) * sxyzt : sxyzt);
+      nb[3][0][l] = sl + ((t == 0) ? (g.nt - 1) * sxyzt : -sxyzt);
+      tlast[l] = (t + 1 == g.nt);
+      tfirst[l] = (t == 0);
     }
-    const T sgn = (T)ISIGN;
+    const T zero = splat<T>(0.0);
     T acc[R][24];
 #pragma unroll
     for (int r = 0; r < R; r++)
 #pragma unroll
-      for (int k = 0; k < 24; k++) acc[r][k] = 0;
+      for (int k = 0; k < 24; k++) acc[r][k] = zero;
 
 #define QPX_HOP(MU)                                                                       \
   {                                                                                       \
-    const T cs = (MU == 3) ? (T)0 : (T)a.coeff_s;                                         \
-    const bool tw = (a.tbc_mask >> MU) & 1;                                               \
+    const bool tw = GEN && ((a.tbc_mask >> MU) & 1);                                      \
     /* forward hop: U_mu(x) (1 - isign g) psi(x + mu) */                                  \
-    if (a.dir_mask & (1u << (2 * MU + 1))) {                                              \
+    if (!GEN || (a.dir_mask & (1u << (2 * MU + 1)))) {                                    \
       cx<T> u[3][3];                                                                      \
-      GaugeIO<P, RECON>::load(a.gauge, a.cb, MU, s, u);                                   \
-      T cf = cs;                                                                          \
-      if (MU == 3) cf = (T)((t + 1 == g.nt) ? a.coeff_t_edge : a.coeff_t);                \
-      cx<T> ph = {(T)a.tbc[MU][0], (T)a.tbc[MU][1]};                                      \
+      L::template load_link<RECON>(a.gauge, a.cb, MU, s, u);                              \
+      T cf;                                                                               \
+      {                                                                                   \
+        double c[SP];                                                                     \
+        _Pragma("unroll") for (int l = 0; l < SP; l++) c[l] =                             \
+            (MU < 3) ? a.coeff_s : (tlast[l] ? a.coeff_t_edge : a.coeff_t);               \
+        lanes_set(cf, c);                                                                 \
+      }                                                                                   \
+      const cx<T> ph = {splat<T>(a.tbc[MU][0]), splat<T>(a.tbc[MU][1])};                  \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
         T psi[24], nrm;                                                                   \
-        SpinorIO<P>::load_raw(a.in, rhs0 + r, nb[MU][1], psi, nrm);                      \
+        L::load_raw(a.in, rhs0 + r, nb[MU][1], psi, nrm);                                 \
         cx<T> h[2][3], ch[2][3];                                                          \
         project<MU, -ISIGN>(psi, h);                                                      \
         scale_h(h, cf * nrm, tw, ph);                                                     \
@@ -292,16 +359,21 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
       }                                                                                   \
     }                                                                                     \
     /* backward hop: U_mu(x - mu)^+ (1 + isign g) psi(x - mu) */                          \
-    if (a.dir_mask & (1u << (2 * MU))) {                                                  \
+    if (!GEN || (a.dir_mask & (1u << (2 * MU)))) {                                        \
       cx<T> u[3][3];                                                                      \
-      GaugeIO<P, RECON>::load(a.gauge, 1 - a.cb, MU, nb[MU][0], u);                       \
-      T cf = cs;                                                                          \
-      if (MU == 3) cf = (T)((t == 0) ? a.coeff_t_edge : a.coeff_t);                       \
-      cx<T> ph = {(T)a.tbc[MU][0], -(T)a.tbc[MU][1]};                                     \
+      L::template load_link<RECON>(a.gauge, 1 - a.cb, MU, nb[MU][0], u);                  \
+      T cf;                                                                               \
+      {                                                                                   \
+        double c[SP];                                                                     \
+        _Pragma("unroll") for (int l = 0; l < SP; l++) c[l] =                             \
+            (MU < 3) ? a.coeff_s : (tfirst[l] ? a.coeff_t_edge : a.coeff_t);              \
+        lanes_set(cf, c);                                                                 \
+      }                                                                                   \
+      const cx<T> ph = {splat<T>(a.tbc[MU][0]), splat<T>(-a.tbc[MU][1])};                 \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
         T psi[24], nrm;                                                                   \
-        SpinorIO<P>::load_raw(a.in, rhs0 + r, nb[MU][0], psi, nrm);                      \
+        L::load_raw(a.in, rhs0 + r, nb[MU][0], psi, nrm);                                 \
         cx<T> h[2][3], ch[2][3];                                                          \
         project<MU, ISIGN>(psi, h);                                                       \
         scale_h(h, cf * nrm, tw, ph);                                                     \
@@ -328,20 +400,22 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
 #pragma unroll
         for (int b = 0; b < 2; b++) {
           T blk[36];
-          CloverIO<P, 72>::load(a.clov, s, 36 * b, 36, blk);
+          L::template load_clover<72>(a.clov, s, 36 * b, 36, blk);
 #pragma unroll
           for (int r = 0; r < R; r++) herm6_apply(blk, acc[r], res[r], b);
         }
       } else if (EPI == EPI_FCLOV) {
 #pragma unroll
-        for (int b = 0; b < 2; b++) {
-          T blk[72];
-          CloverIO<P, 144>::load(a.clov, s, 72 * b, 72, blk);
+        for (int b = 0; b < 2; b++)
 #pragma unroll
-          for (int r = 0; r < R; r++) full6_apply(blk, acc[r], res[r], b);
-        }
+          for (int j = 0; j < 3; j++) {
+            T rows[24];
+            L::template load_clover<144>(a.clov, s, 72 * b + 24 * j, 24, rows);
+#pragma unroll
+            for (int r = 0; r < R; r++) full6_rows(rows, acc[r], res[r], b, j);
+          }
       } else {  // EPI_TMINV: mu_inv (1 - i mu isign g5) acc
-        const T m = (T)a.mu * sgn, mi = (T)a.mu_inv;
+        const T m = splat<T>(a.mu * ISIGN), mi = splat<T>(a.mu_inv);
 #pragma unroll
         for (int r = 0; r < R; r++)
 #pragma unroll
@@ -350,31 +424,31 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
 #pragma unroll
             for (int c = 0; c < 3; c++) {
               T re = acc[r][(sp * 3 + c) * 2], im = acc[r][(sp * 3 + c) * 2 + 1];
-              res[r][(sp * 3 + c) * 2] = mi * (re + mm * im);
-              res[r][(sp * 3 + c) * 2 + 1] = mi * (im - mm * re);
+              res[r][(sp * 3 + c) * 2] = mi * mad(mm, im, re);
+              res[r][(sp * 3 + c) * 2 + 1] = mi * mad(-mm, re, im);
             }
           }
       }
     } else {
-      const T beta = (T)a.beta;
+      const T nbeta = splat<T>(-a.beta);
       T chi[R][24];
 #pragma unroll
-      for (int r = 0; r < R; r++) SpinorIO<P>::load(a.chi, rhs0 + r, s, chi[r]);
+      for (int r = 0; r < R; r++) L::load(a.chi, rhs0 + r, s, chi[r]);
       if (ACHI == ACHI_ALPHA) {
-        const T al = (T)a.alpha;
+        const T al = splat<T>(a.alpha);
 #pragma unroll
         for (int r = 0; r < R; r++)
 #pragma unroll
-          for (int k = 0; k < 24; k++) res[r][k] = al * chi[r][k] - beta * acc[r][k];
+          for (int k = 0; k < 24; k++) res[r][k] = mad(nbeta, acc[r][k], al * chi[r][k]);
       } else if (ACHI == ACHI_CLOV) {
 #pragma unroll
         for (int b = 0; b < 2; b++) {
           T blk[36];
-          CloverIO<P, 72>::load(a.clov, s, 36 * b, 36, blk);
+          L::template load_clover<72>(a.clov, s, 36 * b, 36, blk);
 #pragma unroll
           for (int r = 0; r < R; r++) herm6_apply(blk, chi[r], res[r], b);
         }
-        const T rh = (T)a.rho * sgn;
+        const T rh = splat<T>(a.rho * ISIGN);
 #pragma unroll
         for (int r = 0; r < R; r++)
 #pragma unroll
@@ -383,12 +457,13 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
 #pragma unroll
             for (int c = 0; c < 3; c++) {
               int k = (sp * 3 + c) * 2;
-              res[r][k] += -rr * chi[r][k + 1] - beta * acc[r][k];
-              res[r][k + 1] += rr * chi[r][k] - beta * acc[r][k + 1];
+              // res += i rr chi - beta acc
+              res[r][k] = mad(nbeta, acc[r][k], mad(-rr, chi[r][k + 1], res[r][k]));
+              res[r][k + 1] = mad(nbeta, acc[r][k + 1], mad(rr, chi[r][k], res[r][k + 1]));
             }
           }
       } else {  // ACHI_TM: alpha (1 + i mu isign g5) chi - beta acc
-        const T al = (T)a.alpha, m = (T)a.mu * sgn;
+        const T al = splat<T>(a.alpha), m = splat<T>(a.mu * ISIGN);
 #pragma unroll
         for (int r = 0; r < R; r++)
 #pragma unroll
@@ -398,8 +473,8 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
             for (int c = 0; c < 3; c++) {
               int k = (sp * 3 + c) * 2;
               T re = chi[r][k], im = chi[r][k + 1];
-              res[r][k] = al * (re - mm * im) - beta * acc[r][k];
-              res[r][k + 1] = al * (im + mm * re) - beta * acc[r][k + 1];
+              res[r][k] = mad(nbeta, acc[r][k], al * mad(-mm, im, re));
+              res[r][k + 1] = mad(nbeta, acc[r][k + 1], al * mad(mm, re, im));
             }
           }
       }
@@ -409,9 +484,15 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
         for (int r = 0; r < R; r++) {
           double dre = 0, dim = 0;
 #pragma unroll
-          for (int k = 0; k < 24; k += 2) {
-            dre += (double)res[r][k] * chi[r][k] + (double)res[r][k + 1] * chi[r][k + 1];
-            dim += (double)res[r][k] * chi[r][k + 1] - (double)res[r][k + 1] * chi[r][k];
+          for (int l = 0; l < SP; l++) {
+            if (!act[l]) continue;
+#pragma unroll
+            for (int k = 0; k < 24; k += 2) {
+              const double xr = lane(res[r][k], l), xi = lane(res[r][k + 1], l);
+              const double cr = lane(chi[r][k], l), ci = lane(chi[r][k + 1], l);
+              dre += xr * cr + xi * ci;
+              dim += xr * ci - xi * cr;
+            }
           }
           red[r][3] = dre;
           red[r][4] = dim;
@@ -427,55 +508,75 @@ __global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
       if (a.red.mask & RED_NORM_OUT) {
         double n2 = 0;
 #pragma unroll
-        for (int k = 0; k < 24; k++) n2 += (double)res[r][k] * res[r][k];
+        for (int l = 0; l < SP; l++) {
+          if (!act[l]) continue;
+#pragma unroll
+          for (int k = 0; k < 24; k++) n2 += (double)lane(res[r][k], l) * lane(res[r][k], l);
+        }
         red[r][0] = n2;
       }
       if (a.red.mask & RED_DOT_W_OUT) {
         T w[24];
-        SpinorIO<P>::load(a.w, rr, s, w);
+        L::load(a.w, rr, s, w);
         double dre = 0, dim = 0;
 #pragma unroll
-        for (int k = 0; k < 24; k += 2) {
-          dre += (double)w[k] * res[r][k] + (double)w[k + 1] * res[r][k + 1];
-          dim += (double)w[k] * res[r][k + 1] - (double)w[k + 1] * res[r][k];
+        for (int l = 0; l < SP; l++) {
+          if (!act[l]) continue;
+#pragma unroll
+          for (int k = 0; k < 24; k += 2) {
+            const double wr = lane(w[k], l), wi = lane(w[k + 1], l);
+            const double xr = lane(res[r][k], l), xi = lane(res[r][k + 1], l);
+            dre += wr * xr + wi * xi;
+            dim += wr * xi - wi * xr;
+          }
         }
         red[r][1] = dre;
         red[r][2] = dim;
       }
       if (a.post == POST_STORE) {
-        SpinorIO<P>::store(a.out, rr, s, res[r]);
+        L::store(a.out, rr, s, act, res[r]);
       } else if (a.post == POST_RAXPY) {  // r += b mmp ; |r|^2
-        const T cb_ = (T)a.state->v[S_B][rr];
+        const T cb_ = splat<T>(a.state->v[S_B][rr]);
         T rv[24];
-        SpinorIO<P>::load(a.r, rr, s, rv);
+        L::load(a.r, rr, s, rv);
+#pragma unroll
+        for (int k = 0; k < 24; k++) rv[k] = mad(cb_, res[r][k], rv[k]);
         double n2 = 0;
 #pragma unroll
-        for (int k = 0; k < 24; k++) {
-          rv[k] += cb_ * res[r][k];
-          n2 += (double)rv[k] * rv[k];
+        for (int l = 0; l < SP; l++) {
+          if (!act[l]) continue;
+#pragma unroll
+          for (int k = 0; k < 24; k++) n2 += (double)lane(rv[k], l) * lane(rv[k], l);
         }
-        SpinorIO<P>::store(a.r, rr, s, rv);
+        L::store(a.r, rr, s, act, rv);
         red[r][5] = n2;
       } else {  // POST_CG: r -= a mmp ; x += a p ; |r|^2
-        const T ca = (T)a.state->v[S_A][rr];
+        const T ca = splat<T>(a.state->v[S_A][rr]), nca = splat<T>(-a.state->v[S_A][rr]);
         T rv[24], xv[24], pv[24];
-        SpinorIO<P>::load(a.r, rr, s, rv);
-        SpinorIO<P>::load(a.x, rr, s, xv);
-        SpinorIO<P>::load(a.p, rr, s, pv);
-        double n2 = 0;
+        L::load(a.r, rr, s, rv);
+        L::load(a.x, rr, s, xv);
+        L::load(a.p, rr, s, pv);
 #pragma unroll
         for (int k = 0; k < 24; k++) {
-          rv[k] -= ca * res[r][k];
-          xv[k] += ca * pv[k];
-          n2 += (double)rv[k] * rv[k];
+          rv[k] = mad(nca, res[r][k], rv[k]);
+          xv[k] = mad(ca, pv[k], xv[k]);
         }
-        SpinorIO<P>::store(a.r, rr, s, rv);
-        SpinorIO<P>::store(a.x, rr, s, xv);
+        double n2 = 0;
+#pragma unroll
+        for (int l = 0; l < SP; l++) {
+          if (!act[l]) continue;
+#pragma unroll
+          for (int k = 0; k < 24; k++) n2 += (double)lane(rv[k], l) * lane(rv[k], l);
+        }
+        L::store(a.r, rr, s, act, rv);
+        L::store(a.x, rr, s, act, xv);
         red[r][5] = n2;
       }
     }
   }
-  if (a.red.mask) reduce_epilogue<R>(a.red, a.state, a.nrhs, rhs0, red_slots(a.red.mask), red);
+  if (a.red.mask)
+    reduce_epilogue<R>(a.red, a.state, a.nrhs, rhs0, red_slots(a.red.mask), red, sblock,
+                       (int)(gridDim.x / ntiles));
 }
 
 }  // namespace qpx

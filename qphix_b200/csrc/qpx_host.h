@@ -56,6 +56,11 @@ struct qphix_gpu_lattice_s {
   cudaStream_t stream = nullptr;
   bool owns_stream = false;
   int refs = 1;  // the creator's reference plus one per live field
+  // fields of a lattice with a memory pool are allocated and freed in stream
+  // order on its stream (no device-wide synchronisation); nullptr: cudaMalloc
+  cudaMemPool_t mempool = nullptr;
+  size_t field_bytes = 0;  // bytes of the live fields (pool temporaries included)
+  size_t field_bytes_peak = 0;
   // reduction workspace (one in-flight reduction per stream at a time)
   double *partials = nullptr;
   size_t partials_len = 0;
@@ -93,6 +98,7 @@ struct qphix_gpu_field_s {
   void *data = nullptr;
   float *norm = nullptr;
   size_t bytes = 0;
+  bool pooled = false;  // allocated from the lattice's memory pool
   qpx::SpinorArg sarg() const
   {
     qpx::SpinorArg a;
@@ -128,8 +134,30 @@ struct qphix_gpu_eo_op_s {
 
 namespace qpx {
 
+}  // namespace qpx
+
+// records `msg` as the calling thread's last error and returns `code`
+int qpx_set_last_error(const char *msg, int code);
+
+namespace qpx {
+
+// ---- lattices for the serving layer ----------------------------------------
+// A lattice whose fields come from `pool` in stream order (own stream).
+int lattice_create_pooled(const int latt[4], cudaMemPool_t pool, qphix_gpu_lattice_s **out);
+// Wait for the lattice's stream, then free its pooled solver temporaries and
+// staging buffer and drop its cached iteration graphs.
+void lattice_trim(qphix_gpu_lattice_s *L);
+
 // ---- dispatch (implemented per precision) ----------------------------------
-void launch_dslash(int prec, int recon, int epi, int achi, int R, const DslashArgs &a, dim3 grid,
+// Launch shape of the Dslash kernel: R right-hand sides per thread, SP
+// lattice sites per thread, gen = the general path (direction mask, twisted
+// boundary phases).  Grid: ceil(Vh / (QPX_BLOCK SP)) site blocks x nrhs / R.
+struct DslashShape {
+  int R = 1, SP = 1;
+  bool gen = false;
+};
+// a == nullptr: report only whether the shape is built for (prec, recon)
+bool launch_dslash(int prec, int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
                    cudaStream_t st);
 void launch_blas(int prec, const BlasArgs &a, dim3 grid, cudaStream_t st);
 void launch_convert(int pdst, int psrc, int vh, SpinorArg src, SpinorArg dst, Coef scale, SolverState *state,
@@ -152,7 +180,5 @@ void launch_clover_invert(int prec_in, int prec_out, Geom geo, const void *in, l
 void launch_clover_convert(int prec_in, int prec_out, Geom geo, const void *in, int vpc_in, void *out, int vpc_out,
                            long long stride, int nr, dim3 grid, cudaStream_t st);
 
-// tile sizes compiled for each precision
-bool dslash_tile_ok(int prec, int R);
 
 }  // namespace qpx

@@ -97,14 +97,21 @@ __device__ inline void finalize(int fin, SolverState *st, const double *res, int
 // producing kernel, translated by it into a slot bit set) says which slots
 // are live, and they are packed in slot order into nval doubles per rhs.
 // rhs0 = first rhs of the block's tile.  The last block runs the finalize.
+// The block's partials are stored under site-block index `sblock` of
+// `nsblocks` (default: blockIdx.x of gridDim.x; kernels whose blocks cover
+// (site block, rhs tile) pairs in one grid dimension pass their own).
 template <int R>
 __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, SolverState *st, int nrhs, int rhs0,
-                                                int slots, const double val[R][QPX_MAX_RED])
+                                                int slots, const double val[R][QPX_MAX_RED], int sblock = -1,
+                                                int nsblocks = -1)
 {
   __shared__ double smem[32];
   __shared__ bool am_last;
+  if (sblock < 0) {
+    sblock = blockIdx.x;
+    nsblocks = gridDim.x;
+  }
   const long long nblocks = (long long)gridDim.x * gridDim.y;
-  const long long bid = (long long)blockIdx.y * gridDim.x + blockIdx.x;
 #pragma unroll
   for (int r = 0; r < R; r++) {
     int o = 0;
@@ -113,7 +120,7 @@ __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, SolverState
       if (slots & (1 << k)) {
         double s = block_sum(val[r][k], smem);
         if (threadIdx.x == 0 && rhs0 + r < nrhs)
-          ra.partials[((long long)blockIdx.x * nrhs + rhs0 + r) * ra.nval + o] = s;
+          ra.partials[((long long)sblock * nrhs + rhs0 + r) * ra.nval + o] = s;
         o++;
       }
     }
@@ -125,11 +132,10 @@ __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, SolverState
     am_last = (t == (unsigned int)(nblocks - 1));
   }
   __syncthreads();
-  (void)bid;
   if (!am_last) return;
   __threadfence();
-  // last block: fold the partials of every x-block, in block order
-  const int gx = gridDim.x;
+  // last block: fold the partials of every site block, in block order
+  const int gx = nsblocks;
   for (int idx = 0; idx < nrhs * ra.nval; idx++) {
     double acc = 0;
     for (int b = threadIdx.x; b < gx; b += blockDim.x)

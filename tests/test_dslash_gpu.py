@@ -174,3 +174,76 @@ def test_half_error_is_stated(api, oracle, setup):
         errs[prec] = rel_l2(gr.download(), ref)
     print("relative L2 vs FP64 oracle:", errs)
     assert errs["f32"] < 1e-6 and errs["f16"] < 4e-3 and errs["bf16"] < 3e-2
+
+
+SHAPES = [("sp1", {"QPHIX_GPU_SITES_PER_THREAD": "1", "QPHIX_GPU_RHS_TILE": "1"}),
+          ("sp2", {"QPHIX_GPU_SITES_PER_THREAD": "2", "QPHIX_GPU_RHS_TILE": "1"}),
+          ("r2", {"QPHIX_GPU_SITES_PER_THREAD": "1", "QPHIX_GPU_RHS_TILE": "2"})]
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda s: s[0])
+@pytest.mark.parametrize("prec", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("dims", [(6, 4, 4, 6), (8, 8, 8, 8)], ids=lambda d: "x".join(map(str, d)))
+def test_launch_shapes(api, oracle, monkeypatch, shape, prec, dims):
+    """Every built kernel shape (sites per thread, right-hand sides per
+    thread) against the oracle with two right-hand sides; 6x4x4x6 has 288
+    sites per checkerboard, so its last warp is only partly filled."""
+    for k, v in shape[1].items():
+        monkeypatch.setenv(k, v)
+    s = make_setup(dims)
+    lat = api.Lattice(dims)
+    u = lat.gauge(prec, 12).upload(s["gauge"])
+    u18 = lat.gauge(prec, 18).upload(s["gauge"])
+    L = oracle.make_lattice(dims, -1.0, 1.0, 1.0)
+    psi = [F.gaussian_spinor(dims, 40 + i) for i in range(2)]
+    chi = [F.gaussian_spinor(dims, 50 + i) for i in range(2)]
+    gp = lat.spinor(prec, 2).upload(np.stack(psi))
+    gc = lat.spinor(prec, 2).upload(np.stack(chi))
+    gr = lat.spinor(prec, 2)
+    D = api.Dslash(lat, -1.0, 1.0, 1.0)
+    Cd = api.ClovDslash(lat, -1.0, 1.0, 1.0, prec_mass_rho=0.11)
+    T = api.TMClovDslash(lat, -1.0, 1.0, 1.0, prec_mass_rho=s["mu"])
+    for cb in (0, 1):
+        A = lat.clover(prec).upload(s["clov"][cb])
+        Ai = lat.clover(prec).upload(s["invclov"][cb])
+        f0, f1 = s["finv"][cb]
+        g0 = lat.full_clover(prec).upload(f0)
+        g1 = lat.full_clover(prec).upload(f1)
+        for isign in (1, -1):
+            for links in (u, u18):
+                D.dslash(gr, gp, links, isign, cb)
+                out = gr.download()
+                for i in range(2):
+                    ref = oracle.dslash(L, psi[i], s["gauge"], isign, cb)
+                    assert rel_l2(out[i], ref) < TOL[prec], ("wilson", cb, isign, i)
+            Cd.dslash(gr, gp, u, Ai, isign, cb)
+            out = gr.download()
+            for i in range(2):
+                ref = oracle.clov_dslash(L, psi[i], s["gauge"], s["invclov"][cb], isign, cb)
+                assert rel_l2(out[i], ref) < TOL[prec], ("clover", cb, isign, i)
+            Cd.dslashAChiMinusBDPsi(gr, gp, gc, u, A, 0.25, isign, cb)
+            out = gr.download()
+            for i in range(2):
+                ref = oracle.clov_achimbdpsi(L, psi[i], chi[i], s["gauge"], s["clov"][cb], 0.25, 0.11, isign, cb)
+                assert rel_l2(out[i], ref) < TOL[prec], ("achi", cb, isign, i)
+            T.dslash(gr, gp, u, (g0, g1), isign, cb)
+            out = gr.download()
+            for i in range(2):
+                ref = oracle.tmclov_dslash(L, psi[i], s["gauge"], f0, f1, isign, cb)
+                assert rel_l2(out[i], ref) < TOL[prec], ("tmclover", cb, isign, i)
+
+
+def test_autotuner_records_shapes(api, setup):
+    """The tuner keeps one entry per Dslash configuration it has timed, with a
+    built shape and a positive launch time."""
+    dims = setup["dims"]
+    lat = api.Lattice(dims)
+    u = lat.gauge("f16", 12).upload(setup["gauge"])
+    gp = lat.spinor("f16", 2).upload(np.stack([F.gaussian_spinor(dims, 1), F.gaussian_spinor(dims, 2)]))
+    gr = lat.spinor("f16", 2)
+    api.Dslash(lat, -1.0, 1.0, 1.0).dslash(gr, gp, u, 1, 0)
+    entries = api.tune_entries()
+    key = "dslash p2 r12 e0 a0 %dx%dx%dx%d n2" % tuple(dims)
+    assert key in entries, entries
+    R, SP, us = entries[key]
+    assert (R, SP) in [(1, 1), (1, 2), (2, 1)] and us > 0
