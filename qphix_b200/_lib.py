@@ -133,11 +133,13 @@ class QPhiXGPUError(RuntimeError):
 
 
 def load(path: str | None = None):
-    """Load (once) and return the C library; raises if it is missing."""
+    """Load (once) and return the C library; raises if it is missing.
+    QPHIX_B200_LIBRARY names another build of it (e.g. a variant with other
+    kernel register budgets) to load instead of the in-tree one."""
     global _lib
     if _lib is not None:
         return _lib
-    path = path or LIB_PATH
+    path = path or os.environ.get("QPHIX_B200_LIBRARY") or LIB_PATH
     if not os.path.exists(path):
         raise ImportError(f"{path} is missing: build it with `python -m qphix_b200.build` "
                           "(there is no CPU fallback)")

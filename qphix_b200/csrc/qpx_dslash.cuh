@@ -21,6 +21,23 @@
 #include "qpx_lanes.cuh"
 #include "qpx_reduce.cuh"
 
+// Register budget of the Dslash kernels, as the minimum resident 128-thread
+// blocks per SM the compiler must allow for (registers per thread capped at
+// 65536 / (128 x that)).  Measured on B200 (FP16 clover, 32^3x64 and
+// 16^3x32 x 8 rhs): one site per thread runs best with the compiler free to
+// use ~125 registers (1); two sites or two right-hand sides per thread with
+// at most 168 (3).
+#ifndef QPX_MINB1
+#define QPX_MINB1 1
+#endif
+#ifndef QPX_MINB2
+#define QPX_MINB2 3
+#endif
+#ifndef QPX_MINBR
+#define QPX_MINBR 3
+#endif
+#define QPX_DSLASH_BOUNDS __launch_bounds__(QPX_BLOCK, (SP == 2 ? QPX_MINB2 : (R == 2 ? QPX_MINBR : QPX_MINB1)))
+
 namespace qpx {
 
 enum Epi : int { EPI_NONE = 0, EPI_CLOV = 1, EPI_TMINV = 2, EPI_FCLOV = 3 };
@@ -270,7 +287,7 @@ __device__ __forceinline__ void lanes_set(f2 &d, const double *v) { d = make_flo
 // fastest, so the blocks that share a site block (and its links) run
 // together and the links of the later right-hand sides come from L2.
 template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN, int SP, bool GEN>
-__global__ void __launch_bounds__(QPX_BLOCK) dslash_kernel(const DslashArgs a)
+__global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
 {
   using L = Lanes<P, SP>;
   using T = typename L::T;

@@ -130,6 +130,7 @@ struct qphix_gpu_eo_op_s {
   qphix_gpu_op_params p;
   qphix_gpu_field_s *gauge, *clov, *invclov, *finv0, *finv1;
   std::map<int, qphix_gpu_field_s *> tmp;  // by nrhs
+  std::vector<int> pretuned;                // nrhs values whose Dslash shapes were tuned
 };
 
 namespace qpx {
