@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--inner", default="f16", choices=["f16", "bf16", "f32"])
+    ap.add_argument("--inner-recon", type=int, default=12, choices=[12, 18],
+                    help="link storage of the inner operator (12- or 18-real)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--solver", default="ru", choices=["ru", "richardson"],
                     help="ru: BiCGStab with reliable updates; richardson: InvRichardsonMultiPrec")
@@ -176,9 +178,9 @@ def run_reference(args, rank, world):
 METRIC = "Clover solves/s @1e-10 mixed vs FP64 plain, 1 B200; Dslash HBM GB/s; p99 ms"
 
 
-def config_dict(batch, inner, solver="ru"):
+def config_dict(batch, inner, solver="ru", inner_recon=12):
     how = ("BiCGStab with reliable updates (FP64 true residual / solution, iterations in "
-           f"{inner} storage + FP32 arithmetic)" if solver == "ru" else
+           f"{inner} storage ({inner_recon}-real links) + FP32 arithmetic)" if solver == "ru" else
            f"InvRichardsonMultiPrec (FP64 outer, BiCGStab inner in {inner} storage + FP32 arithmetic)")
     return {"workload": ("clover even-odd 16^3x32, kappa=0.1360, csw=1.0, links exp(i 0.3 H) "
                          f"(H GUE) 12-real, antiperiodic t; {how} to 1e-10 true residual"),
@@ -218,7 +220,7 @@ def main():
     A64 = lat.clover("f64").upload(inputs["clov_odd"])
     Ai64 = lat.clover("f64").upload(inputs["invclov_even"])
     M64 = api.EvenOddCloverOperator(u64, A64, Ai64)
-    ui = lat.gauge(args.inner, 12).upload(inputs["gauge"])
+    ui = lat.gauge(args.inner, args.inner_recon).upload(inputs["gauge"])
     Ai = lat.clover(args.inner).upload(inputs["clov_odd"])
     Aii = lat.clover(args.inner).upload(inputs["invclov_even"])
     Mi = api.EvenOddCloverOperator(ui, Ai, Aii)
@@ -427,7 +429,7 @@ def main():
             "ms_per_step": round(total_s * 1e3 / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": f"mixed: f64 outer, f32 arithmetic on {args.inner} storage inner",
-            "data": "synthetic (seeded)", "config": config_dict(B, args.inner, args.solver),
+            "data": "synthetic (seeded)", "config": config_dict(B, args.inner, args.solver, args.inner_recon),
             "e2e": {"value": round(e2e_value, 3), "unit": "solves/s", "h2d_bytes_per_step": bytes_io,
                     "d2h_bytes_per_step": bytes_io},
             "roofline": roof, "roofline_large_lattice": roof_big,

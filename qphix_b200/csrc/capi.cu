@@ -596,12 +596,18 @@ DslashShape default_shape(int prec, bool gen)
   return sh;
 }
 
-std::string tune_key(const qphix_gpu_lattice_s *lat, int prec, int recon, int epi, int achi, int nrhs)
+// the fused reductions that are timed with a configuration (the CG update's
+// |r|^2 goes with its post op, which is not replayed when tuning)
+int tuned_reductions(const DslashArgs &a) { return a.red.mask & ~RED_NORM_R; }
+
+std::string tune_key(const qphix_gpu_lattice_s *lat, int prec, int recon, int epi, int achi, int nrhs, int red)
 {
   char buf[160];
   snprintf(buf, sizeof(buf), "dslash p%d r%d e%d a%d %dx%dx%dx%d n%d", prec, recon, epi, achi, lat->dims[0],
            lat->dims[1], lat->dims[2], lat->dims[3], nrhs);
-  return buf;
+  std::string k = buf;
+  if (red) k += " red" + std::to_string(red);
+  return k;
 }
 }  // namespace
 
@@ -628,7 +634,8 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
       if (shape_built(prec, recon, epi, achi, sh, a.nrhs)) cands.push_back(sh);
     }
   if (cands.size() <= 1) return cands.empty() ? default_shape(prec, false) : cands[0];
-  const std::string key = tune_key(lat, prec, recon, epi, achi, a.nrhs);
+  const int red = tuned_reductions(a);
+  const std::string key = tune_key(lat, prec, recon, epi, achi, a.nrhs, red);
   {
     std::lock_guard<std::mutex> g(g_tune_mu);
     auto it = g_tune.find(key);
@@ -638,14 +645,20 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
   QPX_CUDA(cudaStreamIsCapturing(lat->stream, &cap));
   if (!tune_enabled() || cap != cudaStreamCaptureStatusNone) return default_shape(prec, false);
 
-  // time every candidate writing a scratch field; no fused updates, no
-  // reductions, no solver state
+  // time every candidate writing a scratch field, with the configuration's
+  // reductions (into the lattice's workspace) but no finalize, no fused
+  // solver update and no solver state
   Tmp scratch(lat, prec, a.nrhs);
   DslashArgs t = a;
   t.out = static_cast<qphix_gpu_field_s *>(scratch)->sarg();
   t.post = POST_STORE;
-  t.red.mask = 0;
   t.state = nullptr;
+  t.red.mask = red;
+  t.red.nval = red_nval(red);
+  t.red.fin = FIN_NONE;
+  t.red.partials = lat->partials;
+  t.red.ticket = lat->ticket;
+  t.red.result = lat->result;
   cudaEvent_t e0, e1;
   QPX_CUDA(cudaEventCreate(&e0));
   QPX_CUDA(cudaEventCreate(&e1));
@@ -1089,17 +1102,28 @@ static void eo_apply(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *res, qphix_gpu_fi
 }
 
 // Times the operator's Dslash shapes (autotuner) outside stream capture, on
-// scratch fields, once per operator and nrhs: an operator whose first
-// application would otherwise happen inside a captured solver iteration.
-static void pretune_op(qphix_gpu_eo_op_s *op, qphix_gpu_lattice_s *lat, int nrhs, int isign, int cb)
+// scratch fields, once per operator, nrhs and set of fused reductions: for an
+// operator whose first applications would otherwise happen inside a captured
+// solver iteration.  `opts` are the applications' options; their finalize
+// steps and solver state are dropped (reductions land in the workspace only).
+static void pretune_op(qphix_gpu_eo_op_s *op, qphix_gpu_lattice_s *lat, int nrhs, int isign, int cb,
+                       std::vector<ApplyOpts> opts)
 {
   if (!tune_enabled()) return;
+  int tag = nrhs;
+  for (size_t i = 0; i < opts.size(); i++) tag = tag * 64 + opts[i].red_mask;
   for (int n : op->pretuned)
-    if (n == nrhs) return;
+    if (n == tag) return;
   // the input's values do not matter for timing (pool fields hold finite data)
   Tmp a(lat, op->gauge->prec, nrhs), b(lat, op->gauge->prec, nrhs);
-  eo_apply(op, b, a, isign, cb, ApplyOpts());
-  op->pretuned.push_back(nrhs);
+  for (auto o : opts) {
+    o.fin = FIN_NONE;
+    o.state = nullptr;
+    o.post = POST_STORE;
+    eo_apply(op, b, a, isign, cb, o);
+  }
+  QPX_CUDA(cudaStreamSynchronize(lat->stream));
+  op->pretuned.push_back(tag);
 }
 
 extern "C" int qphix_gpu_eo_op_apply(qphix_gpu_eo_op op, qphix_gpu_field res, qphix_gpu_field in, int isign,
@@ -1977,7 +2001,13 @@ void solve_bicgstab_mixed(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opl, qphix_g
       blas_launch(latl, lp, nr, rx);
     };
     op_tmp(opl, nr, latl);  // the operator's temporary must exist before graph capture
-    pretune_op(opl, latl, nr, isign, cb);
+    {
+      ApplyOpts t1, t2;
+      t1.red_mask = RED_DOT_W_OUT;
+      t1.w = r0;
+      t2.red_mask = RED_NORM_OUT | RED_DOT_OUT_CHI;
+      pretune_op(opl, latl, nr, isign, cb, {t1, t2});
+    }
     std::string key = "bicg-ru/" + std::to_string(opl->serial) + "/" + fkey(xl) + fkey(r0) + fkey(r) + fkey(p) +
                       fkey(v) + fkey(t) + "/" + std::to_string(isign) + std::to_string(cb);
     while (true) {
