@@ -587,13 +587,27 @@ class Server:
         return eid.value
 
     @staticmethod
-    def _request(ensemble, kind, rhs, mass, csw, mu, t_boundary, rsd_target, max_iters):
+    def interleave(rhs):
+        """complex [(nrhs,) Vh, 4, 3] -> the C layout float64 [nrhs, Vh, 4, 3, 2]"""
         b = np.asarray(rhs)
         if b.ndim == 3:
             b = b[None]
-        nrhs = b.shape[0]
-        bb = np.ascontiguousarray(np.stack([b.real, b.imag], axis=-1), dtype=np.float64)
-        xx = np.zeros_like(bb)
+        return np.ascontiguousarray(np.stack([b.real, b.imag], axis=-1), dtype=np.float64)
+
+    @staticmethod
+    def _request(ensemble, kind, rhs, mass, csw, mu, t_boundary, rsd_target, max_iters, out=None):
+        b = np.asarray(rhs)
+        if b.dtype == np.float64 and b.ndim == 5 and b.shape[-1] == 2 and b.flags.c_contiguous:
+            bb = b  # already in the C layout
+        else:
+            bb = Server.interleave(b)
+        nrhs = bb.shape[0]
+        if out is None:
+            xx = np.zeros_like(bb)
+        else:
+            if out.shape != bb.shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+                raise ValueError("out must be a C-contiguous float64 array shaped like the interleaved rhs")
+            xx = out
         req = L.Request(int(ensemble), OP_KINDS[kind], float(mass), float(csw), float(mu), float(t_boundary),
                         int(nrhs), float(rsd_target), int(max_iters), bb.ctypes.data, xx.ctypes.data)
         return req, bb, xx
@@ -605,9 +619,12 @@ class Server:
         return n.value
 
     def submit(self, ensemble, kind, rhs, mass, csw=1.0, mu=0.0, t_boundary=-1.0, rsd_target=1e-10,
-               max_iters=5000):
-        """rhs: complex [(nrhs,) Vh, 4, 3] odd-checkerboard spinors; returns a ticket."""
-        req, bb, xx = self._request(ensemble, kind, rhs, mass, csw, mu, t_boundary, rsd_target, max_iters)
+               max_iters=5000, out=None):
+        """rhs: complex [(nrhs,) Vh, 4, 3] odd-checkerboard spinors (or already
+        interleaved, see interleave()); out: optional caller-owned float64
+        buffer of the interleaved shape for the solution.  Returns a ticket;
+        both buffers must stay alive until wait()."""
+        req, bb, xx = self._request(ensemble, kind, rhs, mass, csw, mu, t_boundary, rsd_target, max_iters, out)
         t = C.c_longlong(0)
         check(L._lib.qphix_gpu_server_submit(self.h, C.byref(req), C.byref(t)))
         self._pending[t.value] = (bb, xx, req)
@@ -618,8 +635,9 @@ class Server:
         check(L._lib.qphix_gpu_server_poll(self.h, C.c_longlong(ticket), C.byref(d)))
         return bool(d.value)
 
-    def wait(self, ticket, raise_on_error=True):
-        """(x complex [nrhs, Vh, 4, 3], result dict) of a submitted request."""
+    def wait(self, ticket, raise_on_error=True, as_complex=True):
+        """(x, result dict) of a submitted request; x is complex [nrhs, Vh, 4, 3]
+        (as_complex) or the interleaved float64 buffer it was written to."""
         res = L.RequestResult()
         rc = L._lib.qphix_gpu_server_wait(self.h, C.c_longlong(ticket), C.byref(res))
         bb, xx, _ = self._pending.pop(ticket)
@@ -628,7 +646,7 @@ class Server:
             out["error"] = L._lib.qphix_gpu_last_error().decode()
             if raise_on_error:
                 check(rc)
-        return xx[..., 0] + 1j * xx[..., 1], out
+        return (xx[..., 0] + 1j * xx[..., 1] if as_complex else xx), out
 
     def stats(self):
         st = L.ServerStats()

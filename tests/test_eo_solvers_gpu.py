@@ -220,3 +220,86 @@ def test_bicgstab_reliable_update(api, oracle, setup, low, nrhs):
         r = bs[i] - O.apply(xs[i], 1)
         assert np.linalg.norm(r) / np.linalg.norm(bs[i]) < 1e-10
         assert infos[i]["status"] == 0 and infos[i]["true_rel_resid"] < 1e-10
+
+
+def _low_op(api, lat, s, kind, low, target_cb=1):
+    other = 1 - target_cb
+    u = lat.gauge(low, 12).upload(s["gauge"])
+    keep = [u]
+    if kind == "wilson":
+        M = api.EvenOddWilsonOperator(s["mass"], u)
+    elif kind == "tm":
+        M = api.EvenOddTMWilsonOperator(s["mass"], s["mu"], u)
+    elif kind == "clover":
+        A = lat.clover(low).upload(s["clov"][target_cb])
+        Ai = lat.clover(low).upload(s["invclov"][other])
+        keep += [A, Ai]
+        M = api.EvenOddCloverOperator(u, A, Ai)
+    else:
+        A = lat.clover(low).upload(s["clov"][target_cb])
+        f0 = lat.full_clover(low).upload(s["finv"][other][0])
+        f1 = lat.full_clover(low).upload(s["finv"][other][1])
+        keep += [A, f0, f1]
+        M = api.EvenOddTMCloverOperator(u, A, (f0, f1), prec_mass_rho=s["mu"])
+    M._keep = keep
+    return M
+
+
+@pytest.mark.parametrize("kind", ["wilson", "tm", "tmclover"])
+@pytest.mark.parametrize("low", ["f16", "bf16"])
+def test_bicgstab_reliable_update_kinds(api, oracle, setup, kind, low):
+    """The batched mixed solve for every operator kind (two right-hand sides,
+    16-bit inner iterations): each reaches 1e-10 in the FP64 true residual,
+    recomputed with the oracle's operator."""
+    s = setup
+    lat, M, O = build_ops(api, oracle, s, kind)
+    Ml = _low_op(api, lat, s, kind, low)
+    bs = [F.gaussian_spinor(s["dims"], 90 + i) for i in range(2)]
+    gb = lat.spinor("f64", 2).upload(np.stack(bs))
+    gx = lat.spinor("f64", 2)
+    infos = api.InvBiCGStabMixed(M, Ml, delta=0.1)(gx, gb, 1e-10)
+    xs = gx.download()
+    for i in range(2):
+        r = bs[i] - O.apply(xs[i], 1)
+        assert np.linalg.norm(r) / np.linalg.norm(bs[i]) < 1e-10, (kind, low, i)
+        assert infos[i]["status"] == 0
+
+
+def test_multishift_fp32_with_fp64_refinement(api, oracle, setup):
+    """FP32 multishift CG on M^+M followed by FP64 defect correction of each
+    shift (FP64 residual, FP32 single-shift corrections): every shift's
+    solution meets 1e-9 in the FP64 true residual of (M^+M + shift),
+    recomputed with the oracle."""
+    s = setup
+    lat, M64, O = build_ops(api, oracle, s, "wilson")
+    M32 = _low_op(api, lat, s, "wilson", "f32")
+    shifts = [1e-3, 1e-2, 0.1, 1.0]
+    tol = 1e-9
+    b = F.gaussian_spinor(s["dims"], 123)
+    b64, b32 = lat.spinor("f64").upload(b), lat.spinor("f32").upload(b)
+    xs32 = [lat.spinor("f32") for _ in shifts]
+    api.MInvCG(M32, 2000)(xs32, b32, shifts, [tol] * len(shifts))
+    r64, t64, o64, d64 = (lat.spinor("f64") for _ in range(4))
+    r32, d32 = lat.spinor("f32"), lat.spinor("f32")
+    one = api.MInvCG(M32, 2000, max_shifts=1)
+    bn = np.linalg.norm(b)
+    for k, sh in enumerate(shifts):
+        x64 = lat.spinor("f64")
+        x64.convert_from(xs32[k])
+        for _ in range(10):
+            M64(t64, x64, 1)
+            M64(o64, t64, -1)
+            api.caxpby(sh, x64, 1.0, o64)
+            api.copy(r64, b64)
+            api.caxpby(-1.0, o64, 1.0, r64)
+            rn = float(np.sqrt(api.norm2(r64)[0]))
+            if rn / bn < tol:
+                break
+            r32.convert_from(r64, 1.0 / rn)
+            api.zero(d32)
+            one([d32], r32, [sh], [max(1e-5, 0.3 * tol * bn / rn)])
+            d64.convert_from(d32, rn)
+            api.caxpby(1.0, d64, 1.0, x64)
+        x = x64.download()
+        r = b - (O.apply(O.apply(x, 1), -1) + sh * x)
+        assert np.linalg.norm(r) / bn < tol, (sh, np.linalg.norm(r) / bn)
