@@ -43,7 +43,9 @@ extern "C" {
 #define QPHIX_GPU_EUNSUPPORTED (-6)
 
 /* ---- enums ------------------------------------------------------------- */
-enum { QPHIX_GPU_F64 = 0, QPHIX_GPU_F32 = 1, QPHIX_GPU_F16 = 2, QPHIX_GPU_BF16 = 3 };
+/* Q16: spinors as 16-bit fixed point (q / 32767 of the site's largest |value|,
+ * with that value stored per site); links and clover terms in FP16 */
+enum { QPHIX_GPU_F64 = 0, QPHIX_GPU_F32 = 1, QPHIX_GPU_F16 = 2, QPHIX_GPU_BF16 = 3, QPHIX_GPU_Q16 = 4 };
 enum { QPHIX_GPU_SPINOR = 0, QPHIX_GPU_GAUGE = 1, QPHIX_GPU_CLOVER = 2, QPHIX_GPU_FULLCLOVER = 3 };
 enum { QPHIX_GPU_WILSON = 0, QPHIX_GPU_CLOVER_OP = 1, QPHIX_GPU_TM = 2, QPHIX_GPU_TMCLOVER = 3 };
 enum { QPHIX_GPU_HOST_CANONICAL = 0, QPHIX_GPU_HOST_QPHIX = 1 };

@@ -45,6 +45,7 @@ ChunkSpec clover_spec(int prec, int nreal)
   case PREC_F32: { using P = F32; CALL; } break;                   \
   case PREC_F16: { using P = F16; CALL; } break;                   \
   case PREC_BF16: { using P = BF16; CALL; } break;                 \
+  case PREC_Q16: { using P = Q16; CALL; } break;                   \
   default: throw Error(QPHIX_GPU_EINVAL, "bad precision");         \
   }
 
@@ -62,6 +63,7 @@ static void conv_from(int pdst, int vh, SpinorArg src, SpinorArg dst, Coef scale
   case PREC_F32: convert_kernel<P, F32><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
   case PREC_F16: convert_kernel<P, F16><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
   case PREC_BF16: convert_kernel<P, BF16><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
+  case PREC_Q16: convert_kernel<P, Q16><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
   default: throw Error(QPHIX_GPU_EINVAL, "bad precision");
   }
 }
@@ -116,6 +118,8 @@ bool launch_dslash_f16(int recon, int epi, int achi, const DslashShape &sh, cons
                       cudaStream_t st);
 bool launch_dslash_bf16(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
                        cudaStream_t st);
+bool launch_dslash_q16(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
+                      cudaStream_t st);
 
 bool launch_dslash(int prec, int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
                    cudaStream_t st)
@@ -125,6 +129,7 @@ bool launch_dslash(int prec, int recon, int epi, int achi, const DslashShape &sh
   case PREC_F32: return launch_dslash_f32(recon, epi, achi, sh, a, grid, st);
   case PREC_F16: return launch_dslash_f16(recon, epi, achi, sh, a, grid, st);
   case PREC_BF16: return launch_dslash_bf16(recon, epi, achi, sh, a, grid, st);
+  case PREC_Q16: return launch_dslash_q16(recon, epi, achi, sh, a, grid, st);
   }
   return false;
 }

@@ -20,7 +20,7 @@
 
 namespace qpx {
 
-enum Prec : int { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2, PREC_BF16 = 3 };
+enum Prec : int { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2, PREC_BF16 = 3, PREC_Q16 = 4 };
 
 // ---------------------------------------------------------------------------
 // complex arithmetic on plain structs (kept in registers)
@@ -135,8 +135,52 @@ struct BF16 {
   static constexpr int prec = PREC_BF16;
   static constexpr bool has_norm = true;
 };
+// 16-bit fixed-point spinors with a per-site scale (links and clover terms
+// stay FP16): a spinor value is q * norm with q an integer in [-32767, 32767]
+// and norm = (max |value| of the site) / 32767, so every component is held to
+// 1/65534 of the site's largest one (FP16: ~1/4096)
+struct Q16 {
+  using real = float;
+  static constexpr int prec = PREC_Q16;
+  static constexpr bool has_norm = true;
+};
+
+// the per-site norm stored for a site whose largest |value| is m
+template <typename H>
+__host__ __device__ constexpr float site_norm_scale() { return 1.0f; }
+template <>
+__host__ __device__ constexpr float site_norm_scale<Q16>() { return 1.0f / 32767.0f; }
+
+// Q16 words hold u = q + 32768 in each 16-bit half.  As the low 16 mantissa
+// bits of a float with exponent 2^23 they give 2^23 + u exactly, so one byte
+// permute and one subtraction recover q as a float (and one fused
+// multiply-add plus a byte permute store it).
+constexpr float QPX_Q16_BIAS = 8421376.0f;  // 2^23 + 32768
+__device__ __forceinline__ float q16_lo(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B00u, 0x5410)) - QPX_Q16_BIAS; }
+__device__ __forceinline__ float q16_hi(uint32_t w) { return __uint_as_float(__byte_perm(w, 0x4B00u, 0x5432)) - QPX_Q16_BIAS; }
+// a and b in [-1, 1] (already divided by the site's max): the word of
+// round(32767 a), round(32767 b) (round to nearest even)
+__device__ __forceinline__ uint32_t q16_pack(float a, float b)
+{
+  const uint32_t ua = __float_as_uint(fmaf(a, 32767.0f, QPX_Q16_BIAS));
+  const uint32_t ub = __float_as_uint(fmaf(b, 32767.0f, QPX_Q16_BIAS));
+  return __byte_perm(ua, ub, 0x5410);
+}
 
 // 16-bit conversions --------------------------------------------------------
+__device__ __forceinline__ void unpack8(const uint4 &v, float out[8], Q16)
+{
+  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    out[2 * i] = q16_lo(w[i]);
+    out[2 * i + 1] = q16_hi(w[i]);
+  }
+}
+__device__ __forceinline__ uint4 pack8(const float in[8], Q16)
+{
+  return make_uint4(q16_pack(in[0], in[1]), q16_pack(in[2], in[3]), q16_pack(in[4], in[5]), q16_pack(in[6], in[7]));
+}
 __device__ __forceinline__ void unpack8(const uint4 &v, float out[8], F16)
 {
   const __half2 *h = reinterpret_cast<const __half2 *>(&v);
@@ -339,13 +383,15 @@ struct SpinorIO16 {
     uint4 *p = reinterpret_cast<uint4 *>(f.data) + rhs * f.rhs_stride_chunks + s;
 #pragma unroll
     for (int k = 0; k < 3; k++) p[k * f.stride] = pack8(w + 8 * k, H());
-    f.norm[rhs * f.stride + s] = m;
+    f.norm[rhs * f.stride + s] = m * site_norm_scale<H>();
   }
 };
 template <>
 struct SpinorIO<F16> : SpinorIO16<F16> {};
 template <>
 struct SpinorIO<BF16> : SpinorIO16<BF16> {};
+template <>
+struct SpinorIO<Q16> : SpinorIO16<Q16> {};
 
 // ---------------------------------------------------------------------------
 // gauge links
@@ -469,6 +515,11 @@ template <>
 struct GaugeIO<BF16, 18> : GaugeIO16_18<BF16> {};
 template <>
 struct GaugeIO<BF16, 12> : GaugeIO16_12<BF16> {};
+// Q16 keeps links (and clover terms) in FP16
+template <>
+struct GaugeIO<Q16, 18> : GaugeIO16_18<F16> {};
+template <>
+struct GaugeIO<Q16, 12> : GaugeIO16_12<F16> {};
 
 // ---------------------------------------------------------------------------
 // clover fields (NR = 72 packed Hermitian, NR = 144 full blocks)
@@ -534,6 +585,8 @@ template <int NR>
 struct CloverIO<F16, NR> : CloverIO16<F16, NR> {};
 template <int NR>
 struct CloverIO<BF16, NR> : CloverIO16<BF16, NR> {};
+template <int NR>
+struct CloverIO<Q16, NR> : CloverIO16<F16, NR> {};
 
 // ---------------------------------------------------------------------------
 // lattice geometry as seen by a kernel

@@ -3,8 +3,8 @@
 // SP = 1: one site, arithmetic in P::real (double or float).
 // SP = 2: two sites (lanes), arithmetic in f2 = float2 whose .x holds the
 //         value of site s[0] and .y the value of site s[1]; only for the
-//         FP32-arithmetic precisions (F32 storage, F16 / BF16 storage with
-//         per-site norms).  Each lane's data is loaded with the same
+//         FP32-arithmetic precisions (F32 storage, F16 / BF16 / Q16 storage
+//         with per-site norms).  Each lane's data is loaded with the same
 //         coalesced per-site loads as the one-site path and converted
 //         straight into its lane.
 // A lane whose site lies past the end of the checkerboard is given a copy of
@@ -54,6 +54,8 @@ __device__ __forceinline__ float lo_f(uint32_t w, F16) { return __low2float(*rei
 __device__ __forceinline__ float hi_f(uint32_t w, F16) { return __high2float(*reinterpret_cast<const __half2 *>(&w)); }
 __device__ __forceinline__ float lo_f(uint32_t w, BF16) { return __uint_as_float(w << 16); }
 __device__ __forceinline__ float hi_f(uint32_t w, BF16) { return __uint_as_float(w & 0xffff0000u); }
+__device__ __forceinline__ float lo_f(uint32_t w, Q16) { return q16_lo(w); }
+__device__ __forceinline__ float hi_f(uint32_t w, Q16) { return q16_hi(w); }
 
 // v[0] = (a.lo, b.lo), v[1] = (a.hi, b.hi): the same element of sites A and B
 template <typename H>
@@ -63,7 +65,8 @@ __device__ __forceinline__ void lanes_from_words(uint32_t a, uint32_t b, f2 *v)
   v[1] = make_float2(hi_f(a, H()), hi_f(b, H()));
 }
 
-template <typename H>
+// S: spinor storage (F16, BF16, Q16); H: link and clover storage (F16, BF16)
+template <typename S, typename H>
 struct Lanes16 {
   using T = f2;
   __device__ __forceinline__ static void load_raw(const SpinorArg &f, int rhs, const int *s, f2 v[24], f2 &nrm)
@@ -74,10 +77,10 @@ struct Lanes16 {
     for (int k = 0; k < 3; k++) {
       uint4 da = __ldg(p + k * f.stride + s[0]);
       uint4 db = __ldg(p + k * f.stride + s[1]);
-      lanes_from_words<H>(da.x, db.x, v + 8 * k);
-      lanes_from_words<H>(da.y, db.y, v + 8 * k + 2);
-      lanes_from_words<H>(da.z, db.z, v + 8 * k + 4);
-      lanes_from_words<H>(da.w, db.w, v + 8 * k + 6);
+      lanes_from_words<S>(da.x, db.x, v + 8 * k);
+      lanes_from_words<S>(da.y, db.y, v + 8 * k + 2);
+      lanes_from_words<S>(da.z, db.z, v + 8 * k + 4);
+      lanes_from_words<S>(da.w, db.w, v + 8 * k + 6);
     }
   }
   __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, const int *s, f2 v[24])
@@ -109,9 +112,9 @@ struct Lanes16 {
         float q[8];
 #pragma unroll
         for (int i = 0; i < 8; i++) q[i] = lane(w[8 * k + i], l);
-        p[k * f.stride + s[l]] = pack8(q, H());
+        p[k * f.stride + s[l]] = pack8(q, S());
       }
-      f.norm[rhs * f.stride + s[l]] = l ? mb : ma;
+      f.norm[rhs * f.stride + s[l]] = (l ? mb : ma) * site_norm_scale<S>();
     }
   }
   template <int RECON>
@@ -163,9 +166,11 @@ struct Lanes16 {
 };
 
 template <>
-struct Lanes<F16, 2> : Lanes16<F16> {};
+struct Lanes<F16, 2> : Lanes16<F16, F16> {};
 template <>
-struct Lanes<BF16, 2> : Lanes16<BF16> {};
+struct Lanes<BF16, 2> : Lanes16<BF16, BF16> {};
+template <>
+struct Lanes<Q16, 2> : Lanes16<Q16, F16> {};
 
 template <>
 struct Lanes<F32, 2> {

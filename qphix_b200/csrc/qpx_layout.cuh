@@ -105,7 +105,7 @@ __device__ __forceinline__ void dev_store_real(void *base, long long stride, int
     reinterpret_cast<double *>(base)[e] = val;
   else if (P::prec == PREC_F32)
     reinterpret_cast<float *>(base)[e] = (float)val;
-  else if (P::prec == PREC_F16)
+  else if (P::prec == PREC_F16 || P::prec == PREC_Q16)  // Q16 links / clover terms are FP16
     reinterpret_cast<__half *>(base)[e] = __float2half((float)val);
   else
     reinterpret_cast<__nv_bfloat16 *>(base)[e] = __float2bfloat16((float)val);
@@ -118,7 +118,7 @@ __device__ __forceinline__ double dev_load_real(const void *base, long long stri
   long long e = (chunk * stride + s) * vpc + within;
   if (P::prec == PREC_F64) return reinterpret_cast<const double *>(base)[e];
   if (P::prec == PREC_F32) return reinterpret_cast<const float *>(base)[e];
-  if (P::prec == PREC_F16) return __half2float(reinterpret_cast<const __half *>(base)[e]);
+  if (P::prec == PREC_F16 || P::prec == PREC_Q16) return __half2float(reinterpret_cast<const __half *>(base)[e]);
   return __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(base)[e]);
 }
 

@@ -17,12 +17,12 @@ import json
 
 import numpy as np
 
-BYTES = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}
+BYTES = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2, "q16": 2}
 
 
 def algorithmic_bytes(prec, recon, kind, nrhs, achi=False):
     e = BYTES[prec]
-    spinor = 24 * e + (4 if prec in ("f16", "bf16") else 0)
+    spinor = 24 * e + (4 if prec in ("f16", "bf16", "q16") else 0)
     links = 8 * recon * e
     extra = {"wilson": 0, "tm": 0, "clover": 72 * e, "tmclover": 144 * e}[kind]
     if achi and kind == "tmclover":
