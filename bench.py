@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--batch", type=int, default=8)
-    ap.add_argument("--inner", default="f16", choices=["f16", "bf16", "q16", "f32"])
+    ap.add_argument("--inner", default="f16", choices=["f16", "bf16", "q16", "q16f32", "f32"])
     ap.add_argument("--inner-recon", type=int, default=12, choices=[12, 18],
                     help="link storage of the inner operator (12- or 18-real)")
     ap.add_argument("--no-fp64", action="store_true")
@@ -389,9 +389,10 @@ def main():
             torch.cuda.synchronize()
             durs.append(e0.elapsed_time(e1) / 1e3)
         vh = F.vh(dims)
-        esize = {"f16": 2, "bf16": 2, "q16": 2, "f32": 4, "f64": 8}[prec]
-        norm = 4 if prec in ("f16", "bf16", "q16") else 0
-        per_site = nrhs * 2 * (24 * esize + norm) + 8 * 12 * esize + 72 * esize
+        esize = {"f16": 2, "bf16": 2, "q16": 2, "q16f32": 2, "f32": 4, "f64": 8}[prec]
+        lsize = 4 if prec == "q16f32" else esize  # links and clover
+        norm = 4 if prec in ("f16", "bf16", "q16", "q16f32") else 0
+        per_site = nrhs * 2 * (24 * esize + norm) + 8 * 12 * lsize + 72 * lsize
         t = statistics.mean(durs)
         return per_site, vh, t
 

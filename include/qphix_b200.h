@@ -44,8 +44,10 @@ extern "C" {
 
 /* ---- enums ------------------------------------------------------------- */
 /* Q16: spinors as 16-bit fixed point (q / 32767 of the site's largest |value|,
- * with that value stored per site); links and clover terms in FP16 */
-enum { QPHIX_GPU_F64 = 0, QPHIX_GPU_F32 = 1, QPHIX_GPU_F16 = 2, QPHIX_GPU_BF16 = 3, QPHIX_GPU_Q16 = 4 };
+ * with that value stored per site); links and clover terms in FP16.
+ * Q16F32: the same spinors with FP32 links and clover terms. */
+enum { QPHIX_GPU_F64 = 0, QPHIX_GPU_F32 = 1, QPHIX_GPU_F16 = 2, QPHIX_GPU_BF16 = 3, QPHIX_GPU_Q16 = 4,
+       QPHIX_GPU_Q16F32 = 5 };
 enum { QPHIX_GPU_SPINOR = 0, QPHIX_GPU_GAUGE = 1, QPHIX_GPU_CLOVER = 2, QPHIX_GPU_FULLCLOVER = 3 };
 enum { QPHIX_GPU_WILSON = 0, QPHIX_GPU_CLOVER_OP = 1, QPHIX_GPU_TM = 2, QPHIX_GPU_TMCLOVER = 3 };
 enum { QPHIX_GPU_HOST_CANONICAL = 0, QPHIX_GPU_HOST_QPHIX = 1 };

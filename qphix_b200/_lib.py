@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libqphix_b200.so")
 
 OK, EINVAL, ENOMEM, ECUDA, ENOTCONV, EBREAKDOWN, EUNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
-F64, F32, F16, BF16, Q16 = 0, 1, 2, 3, 4
+F64, F32, F16, BF16, Q16, Q16F32 = 0, 1, 2, 3, 4, 5
 SPINOR, GAUGE, CLOVER, FULLCLOVER = 0, 1, 2, 3
 WILSON, CLOVER_OP, TM, TMCLOVER = 0, 1, 2, 3
 HOST_CANONICAL, HOST_QPHIX = 0, 1

@@ -24,7 +24,7 @@ import numpy as np
 from . import _lib as L
 from ._lib import check
 
-PREC = {"f64": L.F64, "f32": L.F32, "f16": L.F16, "bf16": L.BF16, "q16": L.Q16,
+PREC = {"f64": L.F64, "f32": L.F32, "f16": L.F16, "bf16": L.BF16, "q16": L.Q16, "q16f32": L.Q16F32,
         "double": L.F64, "float": L.F32, "half": L.F16}
 
 

@@ -16,6 +16,7 @@ ChunkSpec spinor_spec(int prec)
 
 ChunkSpec gauge_spec(int prec, int recon)
 {
+  if (prec == PREC_Q16F32) prec = PREC_F32;  // FP32 links
   if (recon == 18) {
     switch (prec) {
     case PREC_F64: return {9, 16, 2};
@@ -32,6 +33,7 @@ ChunkSpec gauge_spec(int prec, int recon)
 
 ChunkSpec clover_spec(int prec, int nreal)
 {
+  if (prec == PREC_Q16F32) prec = PREC_F32;  // FP32 clover terms
   switch (prec) {
   case PREC_F64: return {nreal / 2, 16, 2};
   case PREC_F32: return {nreal / 4, 16, 4};
@@ -46,6 +48,7 @@ ChunkSpec clover_spec(int prec, int nreal)
   case PREC_F16: { using P = F16; CALL; } break;                   \
   case PREC_BF16: { using P = BF16; CALL; } break;                 \
   case PREC_Q16: { using P = Q16; CALL; } break;                   \
+  case PREC_Q16F32: { using P = Q16F32; CALL; } break;             \
   default: throw Error(QPHIX_GPU_EINVAL, "bad precision");         \
   }
 
@@ -64,6 +67,7 @@ static void conv_from(int pdst, int vh, SpinorArg src, SpinorArg dst, Coef scale
   case PREC_F16: convert_kernel<P, F16><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
   case PREC_BF16: convert_kernel<P, BF16><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
   case PREC_Q16: convert_kernel<P, Q16><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
+  case PREC_Q16F32: convert_kernel<P, Q16F32><<<grid, QPX_BLOCK, 0, st>>>(vh, src, dst, scale, state, acc); break;
   default: throw Error(QPHIX_GPU_EINVAL, "bad precision");
   }
 }
@@ -120,6 +124,8 @@ bool launch_dslash_bf16(int recon, int epi, int achi, const DslashShape &sh, con
                        cudaStream_t st);
 bool launch_dslash_q16(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
                       cudaStream_t st);
+bool launch_dslash_q16f32(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
+                         cudaStream_t st);
 
 bool launch_dslash(int prec, int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
                    cudaStream_t st)
@@ -130,6 +136,7 @@ bool launch_dslash(int prec, int recon, int epi, int achi, const DslashShape &sh
   case PREC_F16: return launch_dslash_f16(recon, epi, achi, sh, a, grid, st);
   case PREC_BF16: return launch_dslash_bf16(recon, epi, achi, sh, a, grid, st);
   case PREC_Q16: return launch_dslash_q16(recon, epi, achi, sh, a, grid, st);
+  case PREC_Q16F32: return launch_dslash_q16f32(recon, epi, achi, sh, a, grid, st);
   }
   return false;
 }

@@ -237,7 +237,7 @@ extern "C" int qphix_gpu_field_create(qphix_gpu_lattice L, int kind, int prec, i
 {
   return guard([&] {
     QPX_REQUIRE(L && out, "null argument");
-    QPX_REQUIRE(prec >= PREC_F64 && prec <= PREC_Q16, "bad precision");
+    QPX_REQUIRE(prec >= PREC_F64 && prec <= PREC_Q16F32, "bad precision");
     auto *f = new qphix_gpu_field_s();
     f->lat = L;
     f->serial = g_serial++;

@@ -254,6 +254,7 @@ __global__ void clover_convert_kernel(Geom geo, const void *in, int vpc_in, void
   case PREC_F16: { using Q = F16; CALL; } break;            \
   case PREC_BF16: { using Q = BF16; CALL; } break;          \
   case PREC_Q16: { using Q = F16; CALL; } break;            \
+  case PREC_Q16F32: { using Q = F32; CALL; } break;         \
   default: throw Error(QPHIX_GPU_EINVAL, "bad precision");  \
   }
 #define QPX_IN_SWITCH(prec, CALL)                           \
@@ -263,6 +264,7 @@ __global__ void clover_convert_kernel(Geom geo, const void *in, int vpc_in, void
   case PREC_F16: { using Pin = F16; CALL; } break;          \
   case PREC_BF16: { using Pin = BF16; CALL; } break;        \
   case PREC_Q16: { using Pin = F16; CALL; } break;          \
+  case PREC_Q16F32: { using Pin = F32; CALL; } break;       \
   default: throw Error(QPHIX_GPU_EINVAL, "bad precision");  \
   }
 

@@ -20,7 +20,7 @@
 
 namespace qpx {
 
-enum Prec : int { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2, PREC_BF16 = 3, PREC_Q16 = 4 };
+enum Prec : int { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2, PREC_BF16 = 3, PREC_Q16 = 4, PREC_Q16F32 = 5 };
 
 // ---------------------------------------------------------------------------
 // complex arithmetic on plain structs (kept in registers)
@@ -142,6 +142,14 @@ struct BF16 {
 struct Q16 {
   using real = float;
   static constexpr int prec = PREC_Q16;
+  static constexpr bool has_norm = true;
+};
+// Q16 spinors with FP32 links and clover terms: the operator at FP32
+// accuracy, the Krylov vectors at 16 bits (for many right-hand sides, whose
+// spinor traffic outweighs the shared links and clover terms)
+struct Q16F32 {
+  using real = float;
+  static constexpr int prec = PREC_Q16F32;
   static constexpr bool has_norm = true;
 };
 
@@ -392,6 +400,8 @@ template <>
 struct SpinorIO<BF16> : SpinorIO16<BF16> {};
 template <>
 struct SpinorIO<Q16> : SpinorIO16<Q16> {};
+template <>
+struct SpinorIO<Q16F32> : SpinorIO16<Q16> {};
 
 // ---------------------------------------------------------------------------
 // gauge links
@@ -520,6 +530,8 @@ template <>
 struct GaugeIO<Q16, 18> : GaugeIO16_18<F16> {};
 template <>
 struct GaugeIO<Q16, 12> : GaugeIO16_12<F16> {};
+template <int RECON>
+struct GaugeIO<Q16F32, RECON> : GaugeIO<F32, RECON> {};
 
 // ---------------------------------------------------------------------------
 // clover fields (NR = 72 packed Hermitian, NR = 144 full blocks)
@@ -587,6 +599,8 @@ template <int NR>
 struct CloverIO<BF16, NR> : CloverIO16<BF16, NR> {};
 template <int NR>
 struct CloverIO<Q16, NR> : CloverIO16<F16, NR> {};
+template <int NR>
+struct CloverIO<Q16F32, NR> : CloverIO<F32, NR> {};
 
 // ---------------------------------------------------------------------------
 // lattice geometry as seen by a kernel

@@ -246,4 +246,33 @@ struct Lanes<F32, 2> {
   }
 };
 
+// Q16 spinors, FP32 links and clover terms
+template <>
+struct Lanes<Q16F32, 2> {
+  using T = f2;
+  __device__ __forceinline__ static void load_raw(const SpinorArg &f, int rhs, const int *s, f2 v[24], f2 &nrm)
+  {
+    Lanes16<Q16, F16>::load_raw(f, rhs, s, v, nrm);
+  }
+  __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, const int *s, f2 v[24])
+  {
+    Lanes16<Q16, F16>::load(f, rhs, s, v);
+  }
+  __device__ __forceinline__ static void store(const SpinorArg &f, int rhs, const int *s, const bool *act,
+                                               const f2 v[24])
+  {
+    Lanes16<Q16, F16>::store(f, rhs, s, act, v);
+  }
+  template <int RECON>
+  __device__ __forceinline__ static void load_link(const GaugeArg &g, int cb, int mu, const int *s, cx<f2> u[3][3])
+  {
+    Lanes<F32, 2>::load_link<RECON>(g, cb, mu, s, u);
+  }
+  template <int NR>
+  __device__ __forceinline__ static void load_clover(const CloverArg &c, const int *s, int k0, int n, f2 *v)
+  {
+    Lanes<F32, 2>::load_clover<NR>(c, s, k0, n, v);
+  }
+};
+
 }  // namespace qpx

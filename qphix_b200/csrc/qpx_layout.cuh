@@ -103,7 +103,7 @@ __device__ __forceinline__ void dev_store_real(void *base, long long stride, int
   long long e = (chunk * stride + s) * vpc + within;
   if (P::prec == PREC_F64)
     reinterpret_cast<double *>(base)[e] = val;
-  else if (P::prec == PREC_F32)
+  else if (P::prec == PREC_F32 || P::prec == PREC_Q16F32)  // Q16F32 links / clover terms are FP32
     reinterpret_cast<float *>(base)[e] = (float)val;
   else if (P::prec == PREC_F16 || P::prec == PREC_Q16)  // Q16 links / clover terms are FP16
     reinterpret_cast<__half *>(base)[e] = __float2half((float)val);
@@ -117,7 +117,7 @@ __device__ __forceinline__ double dev_load_real(const void *base, long long stri
   long long chunk = k / vpc, within = k % vpc;
   long long e = (chunk * stride + s) * vpc + within;
   if (P::prec == PREC_F64) return reinterpret_cast<const double *>(base)[e];
-  if (P::prec == PREC_F32) return reinterpret_cast<const float *>(base)[e];
+  if (P::prec == PREC_F32 || P::prec == PREC_Q16F32) return reinterpret_cast<const float *>(base)[e];
   if (P::prec == PREC_F16 || P::prec == PREC_Q16) return __half2float(reinterpret_cast<const __half *>(base)[e]);
   return __bfloat162float(reinterpret_cast<const __nv_bfloat16 *>(base)[e]);
 }

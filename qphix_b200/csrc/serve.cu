@@ -84,7 +84,7 @@ size_t spinor_bytes(int prec, long long stride, int nrhs)
 {
   ChunkSpec c = spinor_spec(prec);
   size_t b = (size_t)c.nchunk * c.chunk_bytes * stride;
-  if (prec == PREC_F16 || prec == PREC_BF16 || prec == PREC_Q16) b += sizeof(float) * stride;
+  if (prec == PREC_F16 || prec == PREC_BF16 || prec == PREC_Q16 || prec == PREC_Q16F32) b += sizeof(float) * stride;
   return b * nrhs;
 }
 
@@ -338,8 +338,8 @@ extern "C" int qphix_gpu_server_create(const qphix_gpu_server_config *cfg, qphix
     if (!cfg || !out) throw Error(QPHIX_GPU_EINVAL, "null argument");
     if (cfg->slots < 1 || cfg->slots > 64) throw Error(QPHIX_GPU_EINVAL, "slots must be in [1, 64]");
     if (cfg->low_prec != PREC_F32 && cfg->low_prec != PREC_F16 && cfg->low_prec != PREC_BF16 &&
-        cfg->low_prec != PREC_Q16)
-      throw Error(QPHIX_GPU_EINVAL, "low_prec must be F32, F16, BF16 or Q16");
+        cfg->low_prec != PREC_Q16 && cfg->low_prec != PREC_Q16F32)
+      throw Error(QPHIX_GPU_EINVAL, "low_prec must be F32, F16, BF16, Q16 or Q16F32");
     if (!(cfg->delta > 0.0 && cfg->delta < 1.0)) throw Error(QPHIX_GPU_EINVAL, "delta must be in (0, 1)");
     S = new qphix_gpu_server_s();
     S->cfg = *cfg;

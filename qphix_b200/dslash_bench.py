@@ -17,16 +17,19 @@ import json
 
 import numpy as np
 
-BYTES = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2, "q16": 2}
+BYTES = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2, "q16": 2, "q16f32": 2}
+# links and clover terms, where they differ from the spinors
+LINK_BYTES = {"q16f32": 4}
 
 
 def algorithmic_bytes(prec, recon, kind, nrhs, achi=False):
     e = BYTES[prec]
-    spinor = 24 * e + (4 if prec in ("f16", "bf16", "q16") else 0)
-    links = 8 * recon * e
-    extra = {"wilson": 0, "tm": 0, "clover": 72 * e, "tmclover": 144 * e}[kind]
+    el = LINK_BYTES.get(prec, e)
+    spinor = 24 * e + (4 if prec in ("f16", "bf16", "q16", "q16f32") else 0)
+    links = 8 * recon * el
+    extra = {"wilson": 0, "tm": 0, "clover": 72 * el, "tmclover": 144 * el}[kind]
     if achi and kind == "tmclover":
-        extra = 72 * e
+        extra = 72 * el
     return nrhs * (2 * spinor + (spinor if achi else 0)) + links + extra
 
 

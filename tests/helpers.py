@@ -18,4 +18,4 @@ def make_setup(dims, seed=11, gauge_kind="gaussian", mass=0.1, csw=1.0, mu=0.05)
     return dict(dims=dims, gauge=g, clov=cl, invclov=inv, finv=finv, mass=mass, mu=mu)
 
 
-TOL = {"f64": 1e-13, "f32": 1e-6, "f16": 4e-3, "bf16": 3e-2, "q16": 1e-3}
+TOL = {"f64": 1e-13, "f32": 1e-6, "f16": 4e-3, "bf16": 3e-2, "q16": 1e-3, "q16f32": 1e-4}

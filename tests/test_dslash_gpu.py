@@ -2,8 +2,9 @@
 
 Tolerances (relative L2 over the output checkerboard): FP64 1e-13, FP32 1e-6;
 16-bit storage (FP32 arithmetic) is held to the stated bounds 4e-3 (FP16 +
-per-site norm), 3e-2 (BF16 + per-site norm) and 1e-3 (Q16: 16-bit fixed-point
-spinors with per-site scale, FP16 links and clover) against the FP64 oracle.
+per-site norm), 3e-2 (BF16 + per-site norm), 1e-3 (Q16: 16-bit fixed-point
+spinors with per-site scale, FP16 links and clover) and 1e-4 (Q16F32: the same
+spinors, FP32 links and clover) against the FP64 oracle.
 Mirrors tests/testDslashFull.cc:110-168 (every isign, cb and t boundary).
 """
 import numpy as np
@@ -33,7 +34,7 @@ def _fields(api, lat, s, prec, recon):
     return u
 
 
-@pytest.mark.parametrize("prec", ["f64", "f32", "f16", "bf16", "q16"])
+@pytest.mark.parametrize("prec", ["f64", "f32", "f16", "bf16", "q16", "q16f32"])
 @pytest.mark.parametrize("recon", [18, 12])
 @pytest.mark.parametrize("t_bc", [1.0, -1.0])
 def test_wilson_dslash(api, oracle, setup, prec, recon, t_bc):
@@ -84,7 +85,7 @@ def test_twisted_boundary_and_dir(api, oracle, setup, prec):
         assert rel_l2(gr.download(), ref) < TOL[prec], d
 
 
-@pytest.mark.parametrize("prec", ["f64", "f32", "f16", "q16"])
+@pytest.mark.parametrize("prec", ["f64", "f32", "f16", "q16", "q16f32"])
 @pytest.mark.parametrize("recon", [18, 12])
 def test_clover_dslash(api, oracle, setup, prec, recon):
     dims = setup["dims"]
@@ -139,7 +140,7 @@ def test_tm_dslash(api, oracle, setup, prec):
                 assert rel_l2(gr.download(), ref) < TOL[prec]
 
 
-@pytest.mark.parametrize("prec", ["f64", "f32", "f16", "q16"])
+@pytest.mark.parametrize("prec", ["f64", "f32", "f16", "q16", "q16f32"])
 def test_tmclover_dslash(api, oracle, setup, prec):
     dims = setup["dims"]
     lat = api.Lattice(dims)
@@ -166,7 +167,7 @@ def test_half_error_is_stated(api, oracle, setup):
     psi = F.gaussian_spinor(dims, 13)
     ref = oracle.dslash(L, psi, setup["gauge"], 1, 0)
     errs = {}
-    for prec in ("f32", "f16", "bf16", "q16"):
+    for prec in ("f32", "f16", "bf16", "q16", "q16f32"):
         lat = api.Lattice(dims)
         u = lat.gauge(prec, 12).upload(setup["gauge"])
         gp = lat.spinor(prec).upload(psi)
@@ -174,7 +175,7 @@ def test_half_error_is_stated(api, oracle, setup):
         api.Dslash(lat, -1.0, 1.0, 1.0).dslash(gr, gp, u, 1, 0)
         errs[prec] = rel_l2(gr.download(), ref)
     print("relative L2 vs FP64 oracle:", errs)
-    assert errs["f32"] < 1e-6 and errs["f16"] < 4e-3 and errs["bf16"] < 3e-2 and errs["q16"] < 1e-3
+    assert errs["f32"] < 1e-6 and errs["f16"] < 4e-3 and errs["bf16"] < 3e-2 and errs["q16"] < 1e-3 and errs["q16f32"] < 1e-4
 
 
 SHAPES = [("sp1", {"QPHIX_GPU_SITES_PER_THREAD": "1", "QPHIX_GPU_RHS_TILE": "1"}),
@@ -183,7 +184,7 @@ SHAPES = [("sp1", {"QPHIX_GPU_SITES_PER_THREAD": "1", "QPHIX_GPU_RHS_TILE": "1"}
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda s: s[0])
-@pytest.mark.parametrize("prec", ["f32", "f16", "bf16", "q16"])
+@pytest.mark.parametrize("prec", ["f32", "f16", "bf16", "q16", "q16f32"])
 @pytest.mark.parametrize("dims", [(6, 4, 4, 6), (8, 8, 8, 8)], ids=lambda d: "x".join(map(str, d)))
 def test_launch_shapes(api, oracle, monkeypatch, shape, prec, dims):
     """Every built kernel shape (sites per thread, right-hand sides per

@@ -197,7 +197,7 @@ def test_minvcg(api, oracle, setup, kind, prec):
             assert rel_l2(x.download(), xr) < 1e-7
 
 
-@pytest.mark.parametrize("low", ["f16", "bf16", "q16", "f32"])
+@pytest.mark.parametrize("low", ["f16", "bf16", "q16", "q16f32", "f32"])
 @pytest.mark.parametrize("nrhs", [1, 3])
 def test_bicgstab_reliable_update(api, oracle, setup, low, nrhs):
     """BiCGStab with reliable updates (FP64 true residuals, low-precision
@@ -246,7 +246,7 @@ def _low_op(api, lat, s, kind, low, target_cb=1):
 
 
 @pytest.mark.parametrize("kind", ["wilson", "tm", "tmclover"])
-@pytest.mark.parametrize("low", ["f16", "bf16", "q16"])
+@pytest.mark.parametrize("low", ["f16", "bf16", "q16", "q16f32"])
 def test_bicgstab_reliable_update_kinds(api, oracle, setup, kind, low):
     """The batched mixed solve for every operator kind (two right-hand sides,
     16-bit inner iterations): each reaches 1e-10 in the FP64 true residual,
