@@ -58,7 +58,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--solver", default="ru", choices=["ru", "richardson"],
                     help="ru: BiCGStab with reliable updates; richardson: InvRichardsonMultiPrec")
-    ap.add_argument("--delta", type=float, default=0.1)
+    ap.add_argument("--delta", type=float, default=0.03)
     return ap.parse_args()
 
 
