@@ -157,6 +157,48 @@ __device__ __forceinline__ void recons_add(const cx<T> ch[2][3], T *acc)
 #undef QPX_SUB
 }
 
+// the same with the hop's real coefficient c folded in: acc += c x (the
+// reconstruction of ch), as fused multiply-adds (no separate scaling pass)
+template <int MU, int SG, typename T>
+__device__ __forceinline__ void recons_add_c(const cx<T> ch[2][3], T *acc, T c)
+{
+  const T cp = (SG > 0) ? c : -c;  // +SG c
+  const T cn = -cp;                // -SG c
+#define QPX_ADD(k, v) (acc[k] = mad(cp, (v), acc[k]))
+#define QPX_SUB(k, v) (acc[k] = mad(cn, (v), acc[k]))
+#pragma unroll
+  for (int cc = 0; cc < 3; cc++) {
+    cx<T> c0 = ch[0][cc], c1 = ch[1][cc];
+    acc[(0 * 3 + cc) * 2] = mad(c, c0.re, acc[(0 * 3 + cc) * 2]);
+    acc[(0 * 3 + cc) * 2 + 1] = mad(c, c0.im, acc[(0 * 3 + cc) * 2 + 1]);
+    acc[(1 * 3 + cc) * 2] = mad(c, c1.re, acc[(1 * 3 + cc) * 2]);
+    acc[(1 * 3 + cc) * 2 + 1] = mad(c, c1.im, acc[(1 * 3 + cc) * 2 + 1]);
+    if (MU == 0) {        // o2 += -SG i c1, o3 += -SG i c0
+      QPX_ADD((2 * 3 + cc) * 2, c1.im);
+      QPX_SUB((2 * 3 + cc) * 2 + 1, c1.re);
+      QPX_ADD((3 * 3 + cc) * 2, c0.im);
+      QPX_SUB((3 * 3 + cc) * 2 + 1, c0.re);
+    } else if (MU == 1) { // o2 += SG c1, o3 += -SG c0
+      QPX_ADD((2 * 3 + cc) * 2, c1.re);
+      QPX_ADD((2 * 3 + cc) * 2 + 1, c1.im);
+      QPX_SUB((3 * 3 + cc) * 2, c0.re);
+      QPX_SUB((3 * 3 + cc) * 2 + 1, c0.im);
+    } else if (MU == 2) { // o2 += -SG i c0, o3 += SG i c1
+      QPX_ADD((2 * 3 + cc) * 2, c0.im);
+      QPX_SUB((2 * 3 + cc) * 2 + 1, c0.re);
+      QPX_SUB((3 * 3 + cc) * 2, c1.im);
+      QPX_ADD((3 * 3 + cc) * 2 + 1, c1.re);
+    } else {              // o2 += SG c0, o3 += SG c1
+      QPX_ADD((2 * 3 + cc) * 2, c0.re);
+      QPX_ADD((2 * 3 + cc) * 2 + 1, c0.im);
+      QPX_ADD((3 * 3 + cc) * 2, c1.re);
+      QPX_ADD((3 * 3 + cc) * 2 + 1, c1.im);
+    }
+  }
+#undef QPX_ADD
+#undef QPX_SUB
+}
+
 // scale the projected half spinor once by the hop's coefficient x the
 // spinor's per-site norm (x the twisted-boundary phase): the link multiply is
 // linear, so this equals scaling its result
@@ -370,9 +412,14 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
         L::load_raw(a.in, rhs0 + r, nb[MU][1], psi, nrm);                                 \
         cx<T> h[2][3], ch[2][3];                                                          \
         project<MU, -ISIGN>(psi, h);                                                      \
-        scale_h(h, cf * nrm, tw, ph);                                                     \
-        link_mult<false>(u, h, ch);                                                       \
-        recons_add<MU, -ISIGN>(ch, acc[r]);                                               \
+        if (tw || SP == 2) { /* SP = 2: the folded form costs registers (spills) */       \
+          scale_h(h, cf * nrm, tw, ph);                                                   \
+          link_mult<false>(u, h, ch);                                                     \
+          recons_add<MU, -ISIGN>(ch, acc[r]);                                             \
+        } else {                                                                          \
+          link_mult<false>(u, h, ch);                                                     \
+          recons_add_c<MU, -ISIGN>(ch, acc[r], cf * nrm);                                 \
+        }                                                                                 \
       }                                                                                   \
     }                                                                                     \
     /* backward hop: U_mu(x - mu)^+ (1 + isign g) psi(x - mu) */                          \
@@ -393,9 +440,14 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
         L::load_raw(a.in, rhs0 + r, nb[MU][0], psi, nrm);                                 \
         cx<T> h[2][3], ch[2][3];                                                          \
         project<MU, ISIGN>(psi, h);                                                       \
-        scale_h(h, cf * nrm, tw, ph);                                                     \
-        link_mult<true>(u, h, ch);                                                        \
-        recons_add<MU, ISIGN>(ch, acc[r]);                                                \
+        if (tw || SP == 2) { /* SP = 2: the folded form costs registers (spills) */       \
+          scale_h(h, cf * nrm, tw, ph);                                                   \
+          link_mult<true>(u, h, ch);                                                      \
+          recons_add<MU, ISIGN>(ch, acc[r]);                                              \
+        } else {                                                                          \
+          link_mult<true>(u, h, ch);                                                      \
+          recons_add_c<MU, ISIGN>(ch, acc[r], cf * nrm);                                  \
+        }                                                                                 \
       }                                                                                   \
     }                                                                                     \
   }
