@@ -58,12 +58,16 @@ class AbstractMultiSolver
 namespace gpu
 {
 // relative target for a possibly absolute request
+// the library's targets are relative; an absolute target is divided by the
+// norm of the whole right-hand side (both flavours of a two-flavour field)
 inline double relative_target(qphix_gpu_field rhs, double rsd, ResiduumType t)
 {
   if (t == RELATIVE) return rsd;
-  double n2 = 0;
-  check(qphix_gpu_blas_norm2(rhs, &n2), "norm2");
-  return n2 > 0 ? rsd / std::sqrt(n2) : rsd;
+  double n2[32] = {0};
+  check(qphix_gpu_blas_norm2(rhs, n2), "norm2");
+  double s = 0;
+  for (int i = 0; i < 32; i++) s += n2[i];
+  return s > 0 ? rsd / std::sqrt(s) : rsd;
 }
 }  // namespace gpu
 

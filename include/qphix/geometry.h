@@ -149,6 +149,20 @@ class Geometry
     auto l = host_layout();
     gpu::check(qphix_gpu_field_download(f.get(), h, &l, -1), "spinor download");
   }
+  // a two-flavour spinor (up, down host arrays) as the device field of two
+  // right-hand sides, and back
+  gpu::Field upload_flavours(const FourSpinorBlock *const h[2]) const
+  {
+    gpu::Field f(lat_, QPHIX_GPU_SPINOR, device_prec(), 0, 2);
+    auto l = host_layout();
+    for (int fl = 0; fl < 2; fl++) gpu::check(qphix_gpu_field_upload(f.get(), h[fl], &l, -1, fl), "spinor upload");
+    return f;
+  }
+  void download_flavours(const gpu::Field &f, FourSpinorBlock *const h[2]) const
+  {
+    auto l = host_layout();
+    for (int fl = 0; fl < 2; fl++) gpu::check(qphix_gpu_field_download(f.get(), h[fl], &l, fl), "spinor download");
+  }
   // one gauge field from the two checkerboard arrays QPhiX packs
   gpu::Field upload_gauge(const SU3MatrixBlock *u0, const SU3MatrixBlock *u1) const
   {

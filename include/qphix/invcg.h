@@ -11,36 +11,43 @@ namespace QPhiX
 
 namespace gpu
 {
+// Op::num_flav = 2 (two-flavour operators): x and rhs are (up, down) pairs,
+// solved as one system on a device field of two right-hand sides
 template <typename FT, int V, int S, bool C, typename Op>
-class DeviceSolver : public AbstractSolver<FT, V, S, C, 1>
+class DeviceSolver : public AbstractSolver<FT, V, S, C, Op::num_flav>
 {
  public:
+  static constexpr int NF = Op::num_flav;
   typedef typename Geometry<FT, V, S, C>::FourSpinorBlock Spinor;
   DeviceSolver(Op &M_, int MaxIters_, int kind_, double omega_ = 1.0)
       : M(M_), MaxIters(MaxIters_), kind(kind_), omega(omega_)
   {
   }
-  using AbstractSolver<FT, V, S, C, 1>::operator();
+  using AbstractSolver<FT, V, S, C, NF>::operator();
 
-  void operator()(Spinor *const x[1], const Spinor *const rhs[1], const double RsdTarget, int &n_iters,
+  void operator()(Spinor *const x[NF], const Spinor *const rhs[NF], const double RsdTarget, int &n_iters,
                   double &rsd_sq_final, unsigned long &site_flops, unsigned long &mv_apps, int isign, bool verbose,
                   int cb = 1, ResiduumType residType = RELATIVE) const override
   {
     (void)verbose;
     auto &g = M.getGeometry();
-    auto dx = g.upload_spinor(x[0]);
-    auto db = g.upload_spinor(rhs[0]);
+    auto dx = NF == 1 ? g.upload_spinor(x[0]) : g.upload_flavours(x);
+    auto db = NF == 1 ? g.upload_spinor(rhs[0]) : g.upload_flavours(rhs);
     double rsd = relative_target(db.get(), RsdTarget, residType);
-    qphix_gpu_solve_info info;
+    qphix_gpu_solve_info infos[NF];  // one per right-hand side (the flavours of a pair agree)
+    const qphix_gpu_solve_info &info = infos[0];
     int rc;
     if (kind == QPHIX_GPU_SOLVER_CG)
-      rc = qphix_gpu_solve_cg(M.gpu_op(), dx.get(), db.get(), rsd, MaxIters, isign, cb, &info);
+      rc = qphix_gpu_solve_cg(M.gpu_op(), dx.get(), db.get(), rsd, MaxIters, isign, cb, infos);
     else if (kind == QPHIX_GPU_SOLVER_BICGSTAB)
-      rc = qphix_gpu_solve_bicgstab(M.gpu_op(), dx.get(), db.get(), rsd, MaxIters, isign, cb, &info);
+      rc = qphix_gpu_solve_bicgstab(M.gpu_op(), dx.get(), db.get(), rsd, MaxIters, isign, cb, infos);
     else
-      rc = qphix_gpu_solve_mr(M.gpu_op(), dx.get(), db.get(), rsd, MaxIters, omega, isign, cb, &info);
+      rc = qphix_gpu_solve_mr(M.gpu_op(), dx.get(), db.get(), rsd, MaxIters, omega, isign, cb, infos);
     check(rc, "solver");
-    g.download_spinor(dx, x[0]);
+    if (NF == 1)
+      g.download_spinor(dx, x[0]);
+    else
+      g.download_flavours(dx, x);
     n_iters = info.n_iters;
     rsd_sq_final = info.rsd_sq_final;
     site_flops = info.site_flops;

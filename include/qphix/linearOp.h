@@ -31,6 +31,24 @@ class EvenOddLinearOperator
   virtual qphix_gpu_eo_op gpu_op() const = 0;
 };
 
+// reference: include/qphix/linearOp.h (TwoFlavEvenOddLinearOperator): the
+// operator on two-flavour spinors res[2], in[2] (up, down)
+template <typename FT, int veclen, int soalen, bool compress>
+class TwoFlavEvenOddLinearOperator
+{
+ public:
+  virtual ~TwoFlavEvenOddLinearOperator() {}
+  typedef typename Geometry<FT, veclen, soalen, compress>::FourSpinorBlock FourSpinorBlock;
+  static constexpr int num_flav = 2;
+
+  virtual void operator()(FourSpinorBlock *const res[2], FourSpinorBlock const *const in[2], int isign,
+                          int target_cb = 1) = 0;
+  virtual Geometry<FT, veclen, soalen, compress> &getGeometry() = 0;
+
+  // the device operator (not part of QPhiX's interface)
+  virtual qphix_gpu_eo_op gpu_op() const = 0;
+};
+
 namespace gpu
 {
 // shared body of the four even-odd operators

@@ -49,7 +49,14 @@ extern "C" {
 enum { QPHIX_GPU_F64 = 0, QPHIX_GPU_F32 = 1, QPHIX_GPU_F16 = 2, QPHIX_GPU_BF16 = 3, QPHIX_GPU_Q16 = 4,
        QPHIX_GPU_Q16F32 = 5 };
 enum { QPHIX_GPU_SPINOR = 0, QPHIX_GPU_GAUGE = 1, QPHIX_GPU_CLOVER = 2, QPHIX_GPU_FULLCLOVER = 3 };
-enum { QPHIX_GPU_WILSON = 0, QPHIX_GPU_CLOVER_OP = 1, QPHIX_GPU_TM = 2, QPHIX_GPU_TMCLOVER = 3 };
+/* QPHIX_GPU_NDTM: the two-flavour (non-degenerate) twisted-mass Wilson
+ * operator (include/qphix/ndtm_reuse_operator.h:16-110, parameters mass,
+ * twisted_mass = mu and epsilon).  Its fields hold flavour pairs: right-hand
+ * side 2k is the up, 2k + 1 the down flavour.  As a Dslash kind it is the
+ * Wilson hop followed by mu_inv [(alpha - i isign mu g5 tau3) + eps tau1];
+ * solved with CG (flavour-coupled: the pair is one system). */
+enum { QPHIX_GPU_WILSON = 0, QPHIX_GPU_CLOVER_OP = 1, QPHIX_GPU_TM = 2, QPHIX_GPU_TMCLOVER = 3,
+       QPHIX_GPU_NDTM = 4 };
 enum { QPHIX_GPU_HOST_CANONICAL = 0, QPHIX_GPU_HOST_QPHIX = 1 };
 enum { QPHIX_GPU_HOST_F64 = 0, QPHIX_GPU_HOST_F32 = 1, QPHIX_GPU_HOST_F16 = 2 };
 enum { QPHIX_GPU_SOLVER_CG = 0, QPHIX_GPU_SOLVER_BICGSTAB = 1, QPHIX_GPU_SOLVER_MR = 2 };
@@ -88,6 +95,7 @@ typedef struct {
   double mass;              /* Wilson / TM bare mass (alpha = 4 + mass)      */
   double twisted_mass;      /* TM mu                                         */
   double prec_mass_rho;     /* clover / TM clover i rho gamma_5 term         */
+  double epsilon;           /* two-flavour twisted mass: flavour splitting   */
 } qphix_gpu_op_params;
 
 typedef struct {

@@ -42,7 +42,7 @@ class Operator(C.Structure):
     _fields_ = [("kind", C.c_int), ("L", Lattice), ("gauge", C.c_void_p),
                 ("clov", C.c_void_p), ("invclov", C.c_void_p),
                 ("finv", C.c_void_p * 2), ("mass", C.c_double),
-                ("twisted_mass", C.c_double), ("rho", C.c_double)]
+                ("twisted_mass", C.c_double), ("rho", C.c_double), ("epsilon", C.c_double)]
 
 
 class SolveInfo(C.Structure):
@@ -118,10 +118,10 @@ def make_lattice(dims, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0, tbc=None):
 class OracleOp:
     """Keeps the numpy buffers alive for an or_operator."""
 
-    KINDS = {"wilson": 0, "clover": 1, "tm": 2, "tmclover": 3}
+    KINDS = {"wilson": 0, "clover": 1, "tm": 2, "tmclover": 3, "ndtm": 4}
 
     def __init__(self, kind, L, gauge, clov=None, invclov=None, finv=None,
-                 mass=0.0, twisted_mass=0.0, rho=0.0):
+                 mass=0.0, twisted_mass=0.0, rho=0.0, epsilon=0.0):
         self.bufs = []
         op = Operator()
         op.kind = self.KINDS[kind]
@@ -145,14 +145,17 @@ class OracleOp:
         op.mass = mass
         op.twisted_mass = twisted_mass
         op.rho = rho
+        op.epsilon = epsilon
         self.op = op
         self.vh = int(np.prod(L.dims[:])) // 2
+        # two-flavour operators act on [flavour][Vh][4][3]
+        self.shape = (2, self.vh, 4, 3) if kind == "ndtm" else (self.vh, 4, 3)
 
     def apply(self, x, isign=1, target_cb=1):
         xi = _r(x)
         out = np.empty_like(xi)
         lib().or_eo_apply(C.byref(self.op), _p(out), _p(xi), isign, target_cb)
-        return _c(out, (self.vh, 4, 3))
+        return _c(out, self.shape)
 
 
 def dslash(L, psi, gauge, isign, cb):
@@ -231,7 +234,7 @@ def _solve(fn, op, rhs, x0, *args):
     b = _r(rhs)
     info = SolveInfo()
     fn(C.byref(op.op), _p(x), _p(b), *args, C.byref(info))
-    return _c(x, (op.vh, 4, 3)), info
+    return _c(x, op.shape), info
 
 
 def cg(op, rhs, rsd, max_iters=1000, isign=1, cb=1, x0=None):

@@ -369,9 +369,60 @@ static const double *gauge_cb(const or_operator *op, int cb)
   return op->gauge; /* both checkerboards live in one array */
 }
 
+long or_op_len(const or_operator *op)
+{
+  return 24 * or_vh(&op->L) * (op->kind == OR_OP_NDTM ? 2 : 1);
+}
+
+/* include/qphix/ndtm_reuse_operator.h:68-110 (EvenOddNDTMWilsonReuseOperator):
+   t_f = D_{other,target} in_f (Wilson hop, both flavours);
+   t' = mu_inv [(alpha - i isign mu g5 tau3) + eps tau1] t
+        (two_flav_twisted_mass, include/qphix/complex_functors.h:467-541 with
+         include/qphix/blas_utils.h:77-113; mu_inv = 1/(alpha^2 + mu^2 - eps^2));
+   res_f = alpha (1 + i s_f isign (mu/alpha) g5) in_f - 0.25 D t'_f - eps in_{1-f},
+   s_up = +1, s_dn = -1 (two_flav_AChiMinusBDPsi, include/qphix/tm_dslash_body.h:1174-1207) */
+static void ndtm_apply(const or_operator *op, double *res, const double *in, int isign, int target_cb)
+{
+  const or_lattice *L = &op->L;
+  long vh = or_vh(L), n1 = 24 * vh;
+  int other = 1 - target_cb;
+  double alpha = 4.0 + op->mass, mu = op->twisted_mass, eps = op->epsilon;
+  double mu_inv = 1.0 / (alpha * alpha + mu * mu - eps * eps);
+  double *t = (double *)malloc(sizeof(double) * 2 * n1);
+  double *tp = (double *)malloc(sizeof(double) * 2 * n1);
+  for (int f = 0; f < 2; f++) or_dslash(L, t + f * n1, in + f * n1, gauge_cb(op, other), isign, other);
+  double a = alpha * mu_inv, b = -isign * mu * mu_inv, e = eps * mu_inv;
+#pragma omp parallel for schedule(static)
+  for (long s = 0; s < vh; s++) {
+    cplx up[4][3], dn[4][3], ou[4][3], od[4][3];
+    load_spinor(t, s, up);
+    load_spinor(t + n1, s, dn);
+    for (int sp = 0; sp < 4; sp++) {
+      double g5 = (sp < 2) ? 1.0 : -1.0;
+      for (int c = 0; c < 3; c++) {
+        ou[sp][c] = (a + I * b * g5) * up[sp][c] + e * dn[sp][c];
+        od[sp][c] = (a - I * b * g5) * dn[sp][c] + e * up[sp][c];
+      }
+    }
+    store_spinor(tp, s, ou);
+    store_spinor(tp + n1, s, od);
+  }
+  for (int f = 0; f < 2; f++) {
+    or_tm_achimbdpsi(L, res + f * n1, tp + f * n1, in + f * n1, op->gauge, alpha, 0.25, op->mass, mu, isign,
+                     target_cb, f == 0 ? 1.0 : -1.0);
+    for (long i = 0; i < n1; i++) res[f * n1 + i] -= eps * in[(1 - f) * n1 + i];
+  }
+  free(t);
+  free(tp);
+}
+
 void or_eo_apply(const or_operator *op, double *res, const double *in,
                  int isign, int target_cb)
 {
+  if (op->kind == OR_OP_NDTM) {
+    ndtm_apply(op, res, in, isign, target_cb);
+    return;
+  }
   const or_lattice *L = &op->L;
   long vh = or_vh(L);
   int other = 1 - target_cb;
@@ -451,7 +502,7 @@ static inline void cmul(double r[2], const double a[2], const double b[2])
 void or_cg(const or_operator *op, double *x, const double *rhs, double rsd,
            int max_iters, int isign, int cb, or_solve_info *info)
 {
-  long n = 24 * or_vh(&op->L);
+  long n = or_op_len(op);
   double *r = malloc(sizeof(double) * n), *p = malloc(sizeof(double) * n);
   double *mp = malloc(sizeof(double) * n), *mmp = malloc(sizeof(double) * n);
   unsigned long mv = 0;
@@ -510,7 +561,7 @@ void or_bicgstab(const or_operator *op, double *x, const double *rhs,
                  double rsd, int max_iters, int isign, int cb,
                  or_solve_info *info)
 {
-  long n = 24 * or_vh(&op->L);
+  long n = or_op_len(op);
   double *r0 = malloc(sizeof(double) * n), *r = malloc(sizeof(double) * n);
   double *p = calloc(n, sizeof(double)), *v = calloc(n, sizeof(double));
   double *t = malloc(sizeof(double) * n);
@@ -607,7 +658,7 @@ done:
 void or_mr(const or_operator *op, double *x, const double *rhs, double rsd,
            int max_iters, double omega, int isign, int cb, or_solve_info *info)
 {
-  long n = 24 * or_vh(&op->L);
+  long n = or_op_len(op);
   double *r = malloc(sizeof(double) * n), *Mr = malloc(sizeof(double) * n);
   unsigned long mv = 0;
   int k = 0;
@@ -661,7 +712,7 @@ void or_minvcg(const or_operator *op, double **x, const double *rhs,
                int max_iters, int isign, int cb, int *n_iters,
                double *rsd_sq_final, unsigned long *mv_apps)
 {
-  long n = 24 * or_vh(&op->L);
+  long n = or_op_len(op);
   double *r = malloc(sizeof(double) * n), *p0 = malloc(sizeof(double) * n);
   double *mp = malloc(sizeof(double) * n), *mmp = malloc(sizeof(double) * n);
   double **p = malloc(sizeof(double *) * n_shift);
@@ -745,7 +796,7 @@ void or_richardson_bicgstab(const or_operator *op, double *x,
                             int max_iters, int inner_max_iters, int isign,
                             int cb, or_solve_info *info)
 {
-  long n = 24 * or_vh(&op->L);
+  long n = or_op_len(op);
   double *r = malloc(sizeof(double) * n), *tmp = malloc(sizeof(double) * n);
   double *rin = malloc(sizeof(double) * n), *dx = malloc(sizeof(double) * n);
   unsigned long mv = 0;

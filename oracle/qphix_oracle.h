@@ -82,7 +82,9 @@ void or_tmclov_dslash(const or_lattice *L, double *res, const double *psi,
                       const double *finv1, int isign, int cb);
 
 /* ---- even-odd operators ------------------------------------------------- */
-enum { OR_OP_WILSON = 0, OR_OP_CLOVER = 1, OR_OP_TM = 2, OR_OP_TMCLOVER = 3 };
+/* OR_OP_NDTM: two-flavour (non-degenerate) twisted-mass Wilson, vectors
+   [flavour up, down][Vh][24] (include/qphix/ndtm_reuse_operator.h) */
+enum { OR_OP_WILSON = 0, OR_OP_CLOVER = 1, OR_OP_TM = 2, OR_OP_TMCLOVER = 3, OR_OP_NDTM = 4 };
 typedef struct {
   int kind;
   or_lattice L;
@@ -93,7 +95,11 @@ typedef struct {
   double mass;              /* Wilson bare mass (wilson, tm)             */
   double twisted_mass;      /* tm                                        */
   double rho;               /* prec_mass_rho (clover, tm clover)         */
+  double epsilon;           /* flavour splitting (ndtm)                  */
 } or_operator;
+
+/* reals in one vector the operator acts on (24 Vh, twice that for ndtm) */
+long or_op_len(const or_operator *op);
 
 void or_eo_apply(const or_operator *op, double *res, const double *in,
                  int isign, int target_cb);

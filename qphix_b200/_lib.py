@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libqphix_b200.so")
 OK, EINVAL, ENOMEM, ECUDA, ENOTCONV, EBREAKDOWN, EUNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
 F64, F32, F16, BF16, Q16, Q16F32 = 0, 1, 2, 3, 4, 5
 SPINOR, GAUGE, CLOVER, FULLCLOVER = 0, 1, 2, 3
-WILSON, CLOVER_OP, TM, TMCLOVER = 0, 1, 2, 3
+WILSON, CLOVER_OP, TM, TMCLOVER, NDTM = 0, 1, 2, 3, 4
 HOST_CANONICAL, HOST_QPHIX = 0, 1
 HOST_F64, HOST_F32, HOST_F16 = 0, 1, 2
 SOLVER_CG, SOLVER_BICGSTAB, SOLVER_MR = 0, 1, 2
@@ -28,7 +28,7 @@ class OpParams(C.Structure):
     _fields_ = [("kind", C.c_int), ("t_boundary", C.c_double), ("aniso_s", C.c_double),
                 ("aniso_t", C.c_double), ("use_tbc", C.c_int * 4),
                 ("tbc_phases", (C.c_double * 2) * 4), ("mass", C.c_double),
-                ("twisted_mass", C.c_double), ("prec_mass_rho", C.c_double)]
+                ("twisted_mass", C.c_double), ("prec_mass_rho", C.c_double), ("epsilon", C.c_double)]
 
 
 class SolveInfo(C.Structure):

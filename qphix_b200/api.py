@@ -168,7 +168,7 @@ class Field:
 
 
 def op_params(kind, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0, use_tbc=None, tbc_phases=None,
-              mass=0.0, twisted_mass=0.0, prec_mass_rho=0.0):
+              mass=0.0, twisted_mass=0.0, prec_mass_rho=0.0, epsilon=0.0):
     p = L.OpParams()
     p.kind = kind
     p.t_boundary = t_boundary
@@ -185,6 +185,7 @@ def op_params(kind, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0, use_tbc=None, tbc
     p.mass = mass
     p.twisted_mass = twisted_mass
     p.prec_mass_rho = prec_mass_rho
+    p.epsilon = epsilon
     return p
 
 
@@ -350,6 +351,17 @@ class EvenOddTMWilsonOperator(EvenOddLinearOperator):
                  use_tbc=None, tbc_phases=None):
         super().__init__(op_params(L.TM, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases,
                                    mass=mass, twisted_mass=twisted_mass), u)
+
+
+class EvenOddNDTMWilsonOperator(EvenOddLinearOperator):
+    """include/qphix/ndtm_reuse_operator.h:16-110 (EvenOddNDTMWilsonReuseOperator):
+    the two-flavour twisted-mass operator.  Its fields hold (up, down) pairs
+    as right-hand sides 2k, 2k + 1 (a spinor field of nrhs = 2 is one doublet);
+    InvCG solves each pair as one system."""
+
+    def __init__(self, mass, twisted_mass, epsilon, u, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0):
+        super().__init__(op_params(L.NDTM, t_boundary, aniso_s, aniso_t, None, None, mass=mass,
+                                   twisted_mass=twisted_mass, epsilon=epsilon), u)
 
 
 class EvenOddTMCloverOperator(EvenOddLinearOperator):

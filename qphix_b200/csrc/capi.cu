@@ -615,6 +615,12 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
                                 const DslashArgs &a)
 {
   const bool gen = a.dir_mask != 0xFFu || a.tbc_mask != 0;
+  if (epi == EPI_NDTM || achi == ACHI_NDTM) {  // both flavours of a site in one thread
+    QPX_REQUIRE(!gen, "two-flavour twisted mass takes all hops without twisted boundary phases");
+    DslashShape sh;
+    sh.R = 2;
+    return sh;
+  }
   if (gen) return default_shape(prec, true);
   // forced shapes (experiments)
   const char *fr = getenv("QPHIX_GPU_RHS_TILE"), *fs = getenv("QPHIX_GPU_SITES_PER_THREAD");
@@ -815,6 +821,16 @@ static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qp
     epi = EPI_FCLOV;
     break;
   }
+  case QPHIX_GPU_NDTM: {  // include/qphix/ndtm_reuse_operator.h:76-96
+    QPX_REQUIRE(res->nrhs % 2 == 0, "two-flavour fields hold an even number of right-hand sides (up, down pairs)");
+    const double alpha = 4.0 + p.mass, mu = p.twisted_mass, eps = p.epsilon;
+    const double mu_inv = 1.0 / (alpha * alpha + mu * mu - eps * eps);
+    a.alpha = alpha * mu_inv;
+    a.mu = -isign * mu * mu_inv;
+    a.eps = eps * mu_inv;
+    epi = EPI_NDTM;
+    break;
+  }
   default:
     throw Error(QPHIX_GPU_EINVAL, "bad operator kind");
   }
@@ -872,6 +888,12 @@ static void achi_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphi
     achi = ACHI_TM;
     break;
   }
+  case QPHIX_GPU_NDTM:  // include/qphix/tm_dslash_body.h:1174-1207
+    QPX_REQUIRE(res->nrhs % 2 == 0, "two-flavour fields hold an even number of right-hand sides (up, down pairs)");
+    a.mu = p.twisted_mass / (4.0 + p.mass);
+    a.eps = p.epsilon;
+    achi = ACHI_NDTM;
+    break;
   default:
     throw Error(QPHIX_GPU_EINVAL, "bad operator kind");
   }
@@ -1092,6 +1114,10 @@ static void eo_apply(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *res, qphix_gpu_fi
     achi_core(p, res, tmp, in, op->gauge, nullptr, alpha, 0.25, isign, target_cb, 1.0, o);
     break;
   }
+  case QPHIX_GPU_NDTM:  // include/qphix/ndtm_reuse_operator.h:68-110
+    dslash_core(p, tmp, in, op->gauge, nullptr, nullptr, isign, other);
+    achi_core(p, res, tmp, in, op->gauge, nullptr, 4.0 + p.mass, 0.25, isign, target_cb, 1.0, o);
+    break;
   case QPHIX_GPU_TMCLOVER:  // include/qphix/twisted_mass_clover.h:92-102
     dslash_core(p, tmp, in, op->gauge, op->finv0, op->finv1, isign, other);
     achi_core(p, res, tmp, in, op->gauge, op->clov, 0.0, 0.25, isign, target_cb, 1.0, o);
@@ -1430,9 +1456,12 @@ void sync_op_fields(const qphix_gpu_eo_op_s *op, const qphix_gpu_lattice_s *lat)
   }
 }
 
-void check_solver_fields(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs)
+void check_solver_fields(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs,
+                         bool two_flavour_ok = false)
 {
   QPX_REQUIRE(op, "null operator");
+  QPX_REQUIRE(two_flavour_ok || op->p.kind != QPHIX_GPU_NDTM,
+              "two-flavour operators are solved with CG (the flavour pair as one system)");
   require_spinor(x, "x");
   require_spinor(rhs, "rhs");
   require_same(x, rhs);
@@ -1467,15 +1496,26 @@ void true_residual(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_
 
 // ---------------------------------------------------------------------------
 // CG on M^dag M (include/qphix/invcg.h:88-456)
+// two-flavour systems: the values of right-hand sides 2k and 2k+1 summed
+void pair_sum(std::vector<double> &v)
+{
+  for (size_t r = 0; r + 1 < v.size(); r += 2) v[r] = v[r + 1] = v[r] + v[r + 1];
+}
+
 void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs, const double *rsd,
               int max_iters, int isign, int cb, qphix_gpu_solve_info *info, bool final_resid = true)
 {
-  check_solver_fields(op, x, rhs);
+  check_solver_fields(op, x, rhs, true);
   auto *lat = x->lat;
   const int nr = x->nrhs, prec = x->prec;
+  // two-flavour operator: each (up, down) pair is one system whose inner
+  // products sum over both flavours (include/qphix/invcg.h with num_flav = 2)
+  const bool coupled = op->p.kind == QPHIX_GPU_NDTM;
+  QPX_REQUIRE(!coupled || nr % 2 == 0, "two-flavour fields hold (up, down) pairs");
   Timer timer(lat);
   Tmp mp(lat, prec, nr), mmp(lat, prec, nr), r(lat, prec, nr), p(lat, prec, nr);
   std::vector<double> chi = norm2_host(rhs);
+  if (coupled) pair_sum(chi);
   eo_apply(op, mp, x, isign, cb, ApplyOpts());
   eo_apply(op, mmp, mp, -isign, cb, ApplyOpts());
   BlasCall c;
@@ -1487,7 +1527,9 @@ void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
   blas_launch(lat, prec, nr, c);
   const double *h = fetch_result(lat, nr, 1);
   std::vector<double> cp(h, h + nr);
+  if (coupled) pair_sum(cp);
   SolverState &S = state_reset(lat, nr, max_iters + 1);
+  S.coupled = coupled ? 1 : 0;
   bool all = true;
   for (int i = 0; i < nr; i++) {
     S.v[S_RSD][i] = rsd[i] * rsd[i] * chi[i];
@@ -1540,7 +1582,13 @@ void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
   // true residual (not counted in mv_apps: the reference's own recompute is
   // compiled out, include/qphix/invcg.h:342-403)
   std::vector<double> abs2(nr, -1.0), rel(nr, -1.0);
-  if (final_resid) true_residual(op, x, rhs, mmp, r, isign, cb, true, chi, abs2, rel);
+  if (final_resid) {
+    true_residual(op, x, rhs, mmp, r, isign, cb, true, chi, abs2, rel);
+    if (coupled) {
+      pair_sum(abs2);
+      for (int i = 0; i < nr; i++) rel[i] = chi[i] > 0 ? std::sqrt(abs2[i] / chi[i]) : 0.0;
+    }
+  }
   const SolverState &H = *lat->h_state;
   double secs = timer.stop();
   for (int i = 0; i < nr; i++) {

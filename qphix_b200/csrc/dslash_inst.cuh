@@ -30,6 +30,19 @@ void launch_dslash_k(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStre
   throw Error(QPHIX_GPU_EINVAL, "unsupported dslash epilogue combination");
 }
 
+// the two-flavour twisted-mass kernels (two right-hand sides per thread)
+template <typename P, int RECON, int S>
+void launch_dslash_nd(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStream_t st)
+{
+  dim3 block(QPX_BLOCK);
+  if (achi == ACHI_NONE && epi == EPI_NDTM)
+    dslash_kernel<P, RECON, EPI_NDTM, ACHI_NONE, 2, S, 1, false><<<grid, block, 0, st>>>(a);
+  else if (epi == EPI_NONE && achi == ACHI_NDTM)
+    dslash_kernel<P, RECON, EPI_NONE, ACHI_NDTM, 2, S, 1, false><<<grid, block, 0, st>>>(a);
+  else
+    throw Error(QPHIX_GPU_EINVAL, "unsupported two-flavour dslash combination");
+}
+
 // isign is a template parameter: the projector signs become adds / subtracts
 template <typename P, int RECON, int R, int SP, bool GEN>
 void launch_dslash_s(int epi, int achi, const DslashArgs *a, dim3 grid, cudaStream_t st)
@@ -52,6 +65,16 @@ bool launch_dslash_p(int recon, int epi, int achi, const DslashShape &sh, const 
 {
   constexpr bool fp32 = std::is_same<typename P::real, float>::value;
   if (recon != 12 && recon != 18) return false;
+  if (epi == EPI_NDTM || achi == ACHI_NDTM) {  // two-flavour twisted mass: R = 2 only
+    if (sh.R != 2 || sh.SP != 1 || sh.gen) return false;
+    if (!a) return true;
+    const bool plus = a->isign == 1;
+    if (recon == 12)
+      plus ? launch_dslash_nd<P, 12, 1>(epi, achi, *a, grid, st) : launch_dslash_nd<P, 12, -1>(epi, achi, *a, grid, st);
+    else
+      plus ? launch_dslash_nd<P, 18, 1>(epi, achi, *a, grid, st) : launch_dslash_nd<P, 18, -1>(epi, achi, *a, grid, st);
+    return true;
+  }
   if (sh.gen) {
     if (sh.R != 1 || sh.SP != 1) return false;
     if (recon == 12)

@@ -40,8 +40,18 @@
 
 namespace qpx {
 
-enum Epi : int { EPI_NONE = 0, EPI_CLOV = 1, EPI_TMINV = 2, EPI_FCLOV = 3 };
-enum Achi : int { ACHI_NONE = 0, ACHI_ALPHA = 1, ACHI_CLOV = 2, ACHI_TM = 3 };
+// EPI_NDTM / ACHI_NDTM: the two flavours of a non-degenerate twisted-mass
+// doublet are right-hand sides 2k (up) and 2k + 1 (down) and are only built
+// with two right-hand sides per thread (R = 2), so both flavours of a site
+// sit in one thread:
+//   EPI_NDTM:  out_up = (a + i b g5) acc_up + e acc_dn,
+//              out_dn = (a - i b g5) acc_dn + e acc_up   (a = alpha, b = mu,
+//              e = eps of the args; include/qphix/blas_utils.h:77-113)
+//   ACHI_NDTM: out_f = alpha (1 + i s_f isign mu g5) chi_f - beta acc_f
+//              - eps chi_{1-f}, s_up = +1, s_dn = -1
+//              (include/qphix/tm_dslash_body.h:1174-1207)
+enum Epi : int { EPI_NONE = 0, EPI_CLOV = 1, EPI_TMINV = 2, EPI_FCLOV = 3, EPI_NDTM = 4 };
+enum Achi : int { ACHI_NONE = 0, ACHI_ALPHA = 1, ACHI_CLOV = 2, ACHI_TM = 3, ACHI_NDTM = 4 };
 enum Post : int {
   POST_STORE = 0,  // store out
   POST_CG = 1,     // r -= a out ; x += a p ; |r|^2   (a = state S_A[rhs]); out not stored
@@ -84,6 +94,7 @@ struct DslashArgs {
   double alpha, beta;   // a chi - b D psi
   double mu, mu_inv;    // twisted mass
   double rho;           // i rho gamma_5 term
+  double eps;           // flavour splitting of the two-flavour twisted mass
   int post;
   SpinorArg r, x, p, w; // extra vectors for POST_CG and RED_DOT_W_OUT
   ReduceArg red;
@@ -483,6 +494,24 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
 #pragma unroll
             for (int r = 0; r < R; r++) full6_rows(rows, acc[r], res[r], b, j);
           }
+      } else if (EPI == EPI_NDTM) {
+        if constexpr (R == 2) {
+          const T ca = splat<T>(a.alpha), cb = splat<T>(a.mu), ce = splat<T>(a.eps);
+#pragma unroll
+          for (int sp = 0; sp < 4; sp++) {
+            const T bb = (sp < 2) ? cb : -cb;
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+              const int k = (sp * 3 + c) * 2;
+              const T ur = acc[0][k], ui = acc[0][k + 1], dr = acc[1][k], di = acc[1][k + 1];
+              // up: (a + i bb) u + e d ; down: (a - i bb) d + e u
+              res[0][k] = mad(ce, dr, mad(ca, ur, -(bb * ui)));
+              res[0][k + 1] = mad(ce, di, mad(ca, ui, bb * ur));
+              res[1][k] = mad(ce, ur, mad(ca, dr, bb * di));
+              res[1][k + 1] = mad(ce, ui, mad(ca, di, -(bb * dr)));
+            }
+          }
+        }
       } else {  // EPI_TMINV: mu_inv (1 - i mu isign g5) acc
         const T m = splat<T>(a.mu * ISIGN), mi = splat<T>(a.mu_inv);
 #pragma unroll
@@ -531,6 +560,25 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
               res[r][k + 1] = mad(nbeta, acc[r][k + 1], mad(rr, chi[r][k], res[r][k + 1]));
             }
           }
+      } else if (ACHI == ACHI_NDTM) {
+        if constexpr (R == 2) {
+          const T al = splat<T>(a.alpha), m = splat<T>(a.mu * ISIGN), ne = splat<T>(-a.eps);
+#pragma unroll
+          for (int f = 0; f < 2; f++) {
+#pragma unroll
+            for (int sp = 0; sp < 4; sp++) {
+              // s_f g5 isign mu
+              const T mm = ((sp < 2) == (f == 0)) ? m : -m;
+#pragma unroll
+              for (int c = 0; c < 3; c++) {
+                const int k = (sp * 3 + c) * 2;
+                const T re = chi[f][k], im = chi[f][k + 1];
+                res[f][k] = mad(ne, chi[1 - f][k], mad(nbeta, acc[f][k], al * mad(-mm, im, re)));
+                res[f][k + 1] = mad(ne, chi[1 - f][k + 1], mad(nbeta, acc[f][k + 1], al * mad(mm, re, im)));
+              }
+            }
+          }
+        }
       } else {  // ACHI_TM: alpha (1 + i mu isign g5) chi - beta acc
         const T al = splat<T>(a.alpha), m = splat<T>(a.mu * ISIGN);
 #pragma unroll

@@ -36,7 +36,8 @@ struct SolverState {
   int max_iter;
   int status;     // 0 converged / running, 1 max iterations, 2 breakdown
   int nrhs;
-  int pad[3];
+  int coupled;    // 1: right-hand sides 2k, 2k+1 are one two-flavour system
+  int pad[2];
   int rhs_done[QPX_MAX_RHS];
   int rhs_iter[QPX_MAX_RHS];
   double v[QPX_NSLOT][QPX_MAX_RHS];
@@ -146,6 +147,15 @@ __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, SolverState
   if (threadIdx.x == 0) {
     *ra.ticket = 0u;
     __threadfence();
+    // two-flavour systems: each flavour pair's reductions are one sum (the
+    // reference's num_flav = 2 BLAS), so both get the same solver scalars
+    if (st && st->coupled)
+      for (int r = 0; r + 1 < nrhs; r += 2)
+        for (int k = 0; k < ra.nval; k++) {
+          const double s = ra.result[r * ra.nval + k] + ra.result[(r + 1) * ra.nval + k];
+          ra.result[r * ra.nval + k] = s;
+          ra.result[(r + 1) * ra.nval + k] = s;
+        }
     if (ra.fin != FIN_NONE && st) finalize(ra.fin, st, ra.result, nrhs, ra.nval);
   }
 }

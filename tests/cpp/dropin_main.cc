@@ -16,6 +16,7 @@
 #include "qphix/invbicgstab.h"
 #include "qphix/invcg.h"
 #include "qphix/minvcg.h"
+#include "qphix/ndtm_reuse_operator.h"
 #include "qphix/wilson.h"
 
 using namespace QPhiX;
@@ -136,6 +137,25 @@ int main(int argc, char **argv)
     MInvCG<double, 4, 2, true> mcg(M, 2000, ns);
     mcg(xs, psi, ns, shifts, rsd, n_iters, fin, flops, mv, 1, false, 1);
     for (int s = 0; s < ns; s++) write_from("out_minv_x" + std::to_string(s), xs[s], sbytes);
+
+    // 7. two-flavour twisted mass: the operator on (psi, chi) and InvCG on the pair
+    auto *chi = geom.allocCBFourSpinor();
+    read_into("d_chi", chi, sbytes);
+    double nd[3];
+    read_into("ndtm", nd, sizeof(nd));
+    EvenOddNDTMWilsonReuseOperator<double, 4, 2, true> N(nd[0], nd[1], nd[2], F.u, &geom, -1.0, 1.0, 1.0);
+    Geometry<double, 4, 2, true>::FourSpinorBlock *nres[2] = {geom.allocCBFourSpinor(), geom.allocCBFourSpinor()};
+    const Geometry<double, 4, 2, true>::FourSpinorBlock *nin[2] = {psi, chi};
+    N(nres, nin, 1, 1);
+    write_from("out_nd_up", nres[0], sbytes);
+    write_from("out_nd_dn", nres[1], sbytes);
+    InvCG<double, 4, 2, true, EvenOddNDTMWilsonReuseOperator<double, 4, 2, true>> ncg(N, 2000);
+    ncg(nres, nin, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
+    write_from("out_ndcg_up", nres[0], sbytes);
+    write_from("out_ndcg_dn", nres[1], sbytes);
+    geom.free(nres[0]);
+    geom.free(nres[1]);
+    geom.free(chi);
 
     for (int s = 0; s < ns; s++) geom.free(xs[s]);
     geom.free(psi);

@@ -4,7 +4,8 @@ the library, fed QPhiX-layout host arrays (Geometry<double,4,2,true> with
 padding, and Geometry<float,8,2,true> for the inner solver of
 InvRichardsonMultiPrec) packed from seeded fields, and its outputs -- a
 Dslash, the clover operator, BiCGStab, CG, Richardson and multishift-CG
-solves -- are checked against the CPU oracle."""
+solves, the two-flavour twisted-mass operator and its CG solve -- are
+checked against the CPU oracle."""
 import os
 import subprocess
 
@@ -39,6 +40,10 @@ def test_cpp_dropin(tmp_path, oracle):
     lay = F.QPhiXLayout(dims, 4, 2, True, pad_xy=1, pad_xyz=1)
     psi = F.gaussian_spinor(dims, 32)
     lay.pack_spinor(psi)[1:].tofile(d / "d_psi")  # block 0 = what allocCBFourSpinor returns
+    chi = F.gaussian_spinor(dims, 33)
+    lay.pack_spinor(chi)[1:].tofile(d / "d_chi")
+    nd = (s["mass"], 0.3, 0.2)  # mass, mu, epsilon of the two-flavour operator
+    np.array(nd, dtype=np.float64).tofile(d / "ndtm")
     out = subprocess.run([str(exe), str(d)], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr + out.stdout
 
@@ -66,3 +71,10 @@ def test_cpp_dropin(tmp_path, oracle):
         xs = load(f"out_minv_x{i}")
         r = psi - (O.apply(O.apply(xs, 1), -1) + sh * xs)
         assert np.linalg.norm(r) / np.linalg.norm(psi) < 3e-9
+    N = oracle.OracleOp("ndtm", L, s["gauge"], mass=nd[0], twisted_mass=nd[1], epsilon=nd[2])
+    pair = np.stack([psi, chi])
+    got = np.stack([load("out_nd_up"), load("out_nd_dn")])
+    assert rel_l2(got, N.apply(pair, 1, 1)) < 1e-13
+    xn = np.stack([load("out_ndcg_up"), load("out_ndcg_dn")])
+    r = pair - N.apply(N.apply(xn, 1), -1)
+    assert np.linalg.norm(r) / np.linalg.norm(pair) < 2e-10

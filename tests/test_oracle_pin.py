@@ -168,3 +168,29 @@ def test_dslash_free_field_plane_wave(oracle, isign, t_bc):
 def test_gamma5_is_product_of_gammas():
     g5 = G[0] @ G[1] @ G[2] @ G[3]
     assert np.allclose(g5, np.diag([1, 1, -1, -1]))
+
+
+def test_ndtm_oracle_structure(oracle):
+    """The two-flavour twisted-mass operator of the oracle
+    (include/qphix/ndtm_reuse_operator.h:68-110): with epsilon = 0 it is the
+    twisted-mass operator with +mu on the up and -mu on the down flavour
+    (pinning it to the single-flavour operator), and its isign = -1
+    application is its adjoint."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__)))
+    from helpers import make_setup
+    from qphix_b200 import fields as F
+    dims = (4, 4, 4, 8)
+    s = make_setup(dims, seed=21, gauge_kind="weak", mass=0.1, mu=0.1)
+    L = oracle.make_lattice(dims, -1.0)
+    x = np.stack([F.gaussian_spinor(dims, 1), F.gaussian_spinor(dims, 2)])
+    y = np.stack([F.gaussian_spinor(dims, 3), F.gaussian_spinor(dims, 4)])
+    op0 = oracle.OracleOp("ndtm", L, s["gauge"], mass=0.1, twisted_mass=0.3, epsilon=0.0)
+    up = oracle.OracleOp("tm", L, s["gauge"], mass=0.1, twisted_mass=0.3)
+    dn = oracle.OracleOp("tm", L, s["gauge"], mass=0.1, twisted_mass=-0.3)
+    r = op0.apply(x, 1)
+    assert np.array_equal(r[0], up.apply(x[0], 1)) and np.array_equal(r[1], dn.apply(x[1], 1))
+    op = oracle.OracleOp("ndtm", L, s["gauge"], mass=0.1, twisted_mass=0.3, epsilon=0.2)
+    a = np.vdot(y, op.apply(x, 1))
+    b = np.vdot(op.apply(y, -1), x)
+    assert abs(a - b) / abs(a) < 1e-13
