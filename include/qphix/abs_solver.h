@@ -6,6 +6,7 @@
 
 #include <cmath>
 
+#include "qphix/full_spinor.h"
 #include "qphix/linearOp.h"
 
 namespace QPhiX
@@ -53,6 +54,52 @@ class AbstractMultiSolver
                           const double *RsdTarget, int &niters, double *rsd_sq_final, unsigned long &site_flops,
                           unsigned long &mv_apps, int isign, bool verboseP, int cb = 1) const = 0;
   virtual Geometry<FT, V, S, compress12> &getGeometry() = 0;
+};
+
+// reference: include/qphix/abs_solver.h:271-438 (AbstractUnprecSolver): solves the
+// unpreconditioned system M x = b on both checkerboards with an even-odd
+// solver: prepare the source, solve on solve_cb, reconstruct the other
+// checkerboard
+template <typename FT, int V, int S, bool compress12, int num_flav = 1>
+class AbstractUnprecSolver
+{
+ public:
+  using Spinor = FullSpinor<FT, V, S, compress12>;
+  using CBSpinor = typename Spinor::CBSpinor;
+
+  virtual ~AbstractUnprecSolver() {}
+  virtual AbstractSolver<FT, V, S, compress12> &getEOSolver() const = 0;
+  virtual void SourcePrepare(CBSpinor *const out[num_flav], CBSpinor const *const in_cb[num_flav],
+                             CBSpinor const *const in_other_cb[num_flav], int isign, int solve_cb) const = 0;
+  virtual void SolutionReconstruct(CBSpinor *const out_other_cb[num_flav], CBSpinor const *const in_other_cb[num_flav],
+                                   CBSpinor const *const out_cb[num_flav], int isign, int solve_cb) const = 0;
+
+  virtual void operator()(Spinor *x, const Spinor *rhs, const double RsdTarget, int &niters, double &rsd_sq_final,
+                          unsigned long &site_flops, unsigned long &mv_apps, int isign, bool verboseP,
+                          int solve_cb = 1, ResiduumType residType = RELATIVE) const
+  {
+    Spinor *xa[1] = {x};
+    const Spinor *ra[1] = {rhs};
+    (*this)(xa, ra, RsdTarget, niters, rsd_sq_final, site_flops, mv_apps, isign, verboseP, solve_cb, residType);
+  }
+
+  virtual void operator()(Spinor *const x[num_flav], const Spinor *const rhs[num_flav], const double RsdTarget,
+                          int &niters, double &rsd_sq_final, unsigned long &site_flops, unsigned long &mv_apps,
+                          int isign, bool verboseP, int solve_cb = 1, ResiduumType residType = RELATIVE) const
+  {
+    CBSpinor *in_cb[num_flav], *in_other_cb[num_flav], *out_cb[num_flav], *out_other_cb[num_flav];
+    for (int f = 0; f < num_flav; ++f) {
+      in_cb[f] = rhs[f]->getCBData(solve_cb);
+      in_other_cb[f] = rhs[f]->getCBData(1 - solve_cb);
+      out_cb[f] = x[f]->getCBData(solve_cb);
+      out_other_cb[f] = x[f]->getCBData(1 - solve_cb);
+    }
+    // the prepared source is kept in the solution's other checkerboard
+    SourcePrepare(out_other_cb, in_cb, in_other_cb, isign, solve_cb);
+    getEOSolver()(out_cb, out_other_cb, RsdTarget, niters, rsd_sq_final, site_flops, mv_apps, isign, verboseP,
+                  solve_cb, residType);
+    SolutionReconstruct(out_other_cb, in_other_cb, out_cb, isign, solve_cb);
+  }
 };
 
 namespace gpu

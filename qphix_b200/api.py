@@ -314,6 +314,24 @@ class EvenOddLinearOperator:
     def __call__(self, res, inp, isign=1, target_cb=1):
         check(L._lib.qphix_gpu_eo_op_apply(self.h, res.h, inp.h, isign, target_cb))
 
+    def M_offdiag(self, res, inp, isign, target_cb):
+        """checkerboard off-diagonal block; only the Wilson and clover operators
+        have it (the reference's twisted-mass operators print "not yet
+        implemented", twisted_mass.h:79-87)"""
+        raise NotImplementedError(f"M_offdiag not implemented for {type(self).__name__}")
+
+    def M_diag_inv(self, res, inp, isign, cb=0):
+        """inverse of the checkerboard-diagonal block (Wilson and clover only)"""
+        raise NotImplementedError(f"M_diag_inv not implemented for {type(self).__name__}")
+
+    def _offdiag(self, res, inp, isign, target_cb):
+        # -1/2 D onto target_cb (wilson.h:68-77, clover.h:175-184)
+        w = L.OpParams.from_buffer_copy(self.p)
+        w.kind = L.WILSON
+        check(L._lib.qphix_gpu_dslash(C.byref(w), res.h, inp.h, self.fields[0].h, None, None, isign,
+                                      target_cb))
+        caxpby(0.0, res, -0.5, res)
+
     def close(self):
         if getattr(self, "h", None):
             L._lib.qphix_gpu_eo_op_destroy(self.h)
@@ -333,15 +351,36 @@ class EvenOddWilsonOperator(EvenOddLinearOperator):
                  tbc_phases=None):
         super().__init__(op_params(L.WILSON, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases,
                                    mass=mass), u)
+        self.mass = mass
+
+    def M_offdiag(self, res, inp, isign, target_cb):
+        self._offdiag(res, inp, isign, target_cb)
+
+    def M_diag_inv(self, res, inp, isign, cb=0):
+        """1 / (4 + m) (wilson.h:79-86)"""
+        copy(res, inp)
+        caxpby(0.0, res, 1.0 / (4.0 + self.mass), res)
 
 
 class EvenOddCloverOperator(EvenOddLinearOperator):
-    """include/qphix/clover.h:31-102 (clov = A_oo, invclov = A_ee^-1)"""
+    """include/qphix/clover.h:31-102 (clov = A_oo, invclov = A_ee^-1; invclov_odd =
+    A_oo^-1, needed only by M_diag_inv on the odd checkerboard)"""
 
     def __init__(self, u, clov, invclov, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0, use_tbc=None,
-                 tbc_phases=None, prec_mass_rho=0.0):
+                 tbc_phases=None, prec_mass_rho=0.0, invclov_odd=None):
         super().__init__(op_params(L.CLOVER_OP, t_boundary, aniso_s, aniso_t, use_tbc, tbc_phases,
                                    prec_mass_rho=prec_mass_rho), u, clov, invclov)
+        self.invclov = (invclov, invclov_odd)
+
+    def M_offdiag(self, res, inp, isign, target_cb):
+        self._offdiag(res, inp, isign, target_cb)
+
+    def M_diag_inv(self, res, inp, isign, cb=0):
+        """A^-1 of checkerboard cb (clover.h:186-192)"""
+        ai = self.invclov[cb]
+        if ai is None:
+            raise ValueError("M_diag_inv: no inverse clover term for this checkerboard")
+        check(L._lib.qphix_gpu_clover_apply(res.h, inp.h, ai.h))
 
 
 class EvenOddTMWilsonOperator(EvenOddLinearOperator):
@@ -460,6 +499,63 @@ class InvRichardsonMultiPrec:
                                                     rsd_target, self.delta, self.max_iters,
                                                     self.inner_max, isign, cb, inf))
         return _as_dicts(inf)
+
+
+class FullSpinor:
+    """include/qphix/full_spinor.h: both checkerboards of a spinor field"""
+
+    def __init__(self, lat, prec="f64", nrhs=1):
+        self.cbs = (lat.spinor(prec, nrhs), lat.spinor(prec, nrhs))
+
+    def getCBData(self, cb):
+        return self.cbs[cb]
+
+
+class UnprecSolverWrapper:
+    """include/qphix/unprec_solver_wrapper.h:17-99 with the driver of
+    include/qphix/abs_solver.h:271-438 (AbstractUnprecSolver): solves the
+    unpreconditioned M x = b with an even-odd solver on solve_cb.
+
+      b'      = b_cb - M_offdiag(M_diag_inv(b_other), solve_cb)
+      x_cb    = eo_solver(b')
+      x_other = M_diag_inv(b_other - M_offdiag(x_cb, other))
+
+    The prepared source lives in x's other checkerboard, as in the reference.
+    M_diag_inv is called with its default checkerboard (unprec_solver_wrapper.h:
+    54,84): the inverse diagonal block M was built with, i.e. that of the
+    checkerboard not solved for (an operator for solve_cb = 0 holds A_ee as
+    clov and A_oo^-1 as invclov)."""
+
+    def __init__(self, eo_solver, M):
+        self.solver, self.M = eo_solver, M
+
+    def getEOSolver(self):
+        return self.solver
+
+    @staticmethod
+    def _tmp(like):
+        return Field(like.lat, L.SPINOR, like.prec, 0, like.nrhs)
+
+    def SourcePrepare(self, out, in_cb, in_other_cb, isign, solve_cb):
+        t1, t2 = self._tmp(in_cb), self._tmp(in_cb)
+        self.M.M_diag_inv(t1, in_other_cb, isign)
+        self.M.M_offdiag(t2, t1, isign, solve_cb)
+        copy(out, in_cb)
+        caxpby(-1.0, t2, 1.0, out)
+
+    def SolutionReconstruct(self, out_other_cb, in_other_cb, out_cb, isign, solve_cb):
+        t1, t2 = self._tmp(out_cb), self._tmp(out_cb)
+        self.M.M_offdiag(t1, out_cb, isign, 1 - solve_cb)
+        copy(t2, in_other_cb)
+        caxpby(-1.0, t1, 1.0, t2)
+        self.M.M_diag_inv(out_other_cb, t2, isign)
+
+    def __call__(self, x, rhs, rsd_target, isign=1, solve_cb=1):
+        o = 1 - solve_cb
+        self.SourcePrepare(x.getCBData(o), rhs.getCBData(solve_cb), rhs.getCBData(o), isign, solve_cb)
+        infos = self.solver(x.getCBData(solve_cb), x.getCBData(o), rsd_target, isign, solve_cb)
+        self.SolutionReconstruct(x.getCBData(o), rhs.getCBData(o), x.getCBData(solve_cb), isign, solve_cb)
+        return infos
 
 
 class InvBiCGStabMixed:

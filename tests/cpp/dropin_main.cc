@@ -17,6 +17,7 @@
 #include "qphix/invcg.h"
 #include "qphix/minvcg.h"
 #include "qphix/ndtm_reuse_operator.h"
+#include "qphix/unprec_solver_wrapper.h"
 #include "qphix/wilson.h"
 
 using namespace QPhiX;
@@ -156,6 +157,18 @@ int main(int argc, char **argv)
     geom.free(nres[0]);
     geom.free(nres[1]);
     geom.free(chi);
+
+    // 8. unpreconditioned clover solve: b = (chi on even, psi on odd) through
+    // UnprecSolverWrapper around InvBiCGStab on cb 1
+    {
+      FullSpinor<double, 4, 2, true> fb(geom), fx(geom);
+      read_into("d_chi", fb.getCBData(0), sbytes);
+      read_into("d_psi", fb.getCBData(1), sbytes);
+      UnprecSolverWrapper<double, 4, 2, true, EvenOddCloverOperator<double, 4, 2, true>> unprec(bicg, M);
+      unprec(&fx, &fb, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
+      write_from("out_unprec_e", fx.getCBData(0), sbytes);
+      write_from("out_unprec_o", fx.getCBData(1), sbytes);
+    }
 
     for (int s = 0; s < ns; s++) geom.free(xs[s]);
     geom.free(psi);

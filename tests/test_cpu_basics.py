@@ -59,6 +59,17 @@ def test_library_exports_every_header_symbol():
     assert declared == set(_lib.EXPORTED)
 
 
+def test_dropin_headers_compile_and_link(tmp_path):
+    """The drop-in headers (include/qphix/) compile as a QPhiX caller uses them
+    and every C-ABI call they make resolves in the library."""
+    exe = tmp_path / "dropin"
+    subprocess.check_call(["g++", "-std=c++14", "-O0", "-Wall", "-Werror", "-Wno-unused-variable",
+                           "-I", os.path.join(ROOT, "include"),
+                           os.path.join(ROOT, "tests", "cpp", "dropin_main.cc"),
+                           "-L", os.path.join(ROOT, "qphix_b200"), "-lqphix_b200", "-o", str(exe)])
+    assert exe.exists()
+
+
 def test_library_fails_loudly_without_gpu():
     import torch
     if torch.cuda.is_available():

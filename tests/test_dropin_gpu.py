@@ -5,7 +5,8 @@ padding, and Geometry<float,8,2,true> for the inner solver of
 InvRichardsonMultiPrec) packed from seeded fields, and its outputs -- a
 Dslash, the clover operator, BiCGStab, CG, Richardson and multishift-CG
 solves, the two-flavour twisted-mass operator and its CG solve -- are
-checked against the CPU oracle."""
+checked against the CPU oracle.  An UnprecSolverWrapper solve of the full
+(unpreconditioned) clover system is checked through its full residual."""
 import os
 import subprocess
 
@@ -78,3 +79,10 @@ def test_cpp_dropin(tmp_path, oracle):
     xn = np.stack([load("out_ndcg_up"), load("out_ndcg_dn")])
     r = pair - N.apply(N.apply(xn, 1), -1)
     assert np.linalg.norm(r) / np.linalg.norm(pair) < 2e-10
+    # unpreconditioned clover system: [[A_ee, -D_eo/2], [-D_oe/2, A_oo]] x = (chi, psi)
+    xe, xo = load("out_unprec_e"), load("out_unprec_o")
+    re = oracle.clover_apply(xe, s["clov"][0]) - 0.5 * oracle.dslash(L, xo, s["gauge"], 1, 0) - chi
+    ro = oracle.clover_apply(xo, s["clov"][1]) - 0.5 * oracle.dslash(L, xe, s["gauge"], 1, 1) - psi
+    rel = np.sqrt((np.linalg.norm(re) ** 2 + np.linalg.norm(ro) ** 2)
+                  / (np.linalg.norm(chi) ** 2 + np.linalg.norm(psi) ** 2))
+    assert rel < 2e-10
