@@ -57,7 +57,7 @@ enum { QPHIX_GPU_SPINOR = 0, QPHIX_GPU_GAUGE = 1, QPHIX_GPU_CLOVER = 2, QPHIX_GP
  * solved with CG (flavour-coupled: the pair is one system). */
 enum { QPHIX_GPU_WILSON = 0, QPHIX_GPU_CLOVER_OP = 1, QPHIX_GPU_TM = 2, QPHIX_GPU_TMCLOVER = 3,
        QPHIX_GPU_NDTM = 4 };
-enum { QPHIX_GPU_HOST_CANONICAL = 0, QPHIX_GPU_HOST_QPHIX = 1 };
+enum { QPHIX_GPU_HOST_CANONICAL = 0, QPHIX_GPU_HOST_QPHIX = 1, QPHIX_GPU_HOST_QDP = 2 };
 enum { QPHIX_GPU_HOST_F64 = 0, QPHIX_GPU_HOST_F32 = 1, QPHIX_GPU_HOST_F16 = 2 };
 enum { QPHIX_GPU_SOLVER_CG = 0, QPHIX_GPU_SOLVER_BICGSTAB = 1, QPHIX_GPU_SOLVER_MR = 2 };
 
@@ -73,15 +73,27 @@ typedef struct qphix_gpu_eo_op_s *qphix_gpu_eo_op;
  * qphix: the reference's Geometry<FT,V,S,compress12> arrays with padding
  *   pad_xy / pad_xyz (include/qphix/geometry.h:130-175); spinor pointers are
  *   the ones allocCBFourSpinor returns (block 0 = first site), gauge arrays
- *   are one checkerboard each (8 links per site, stored transposed). */
+ *   are one checkerboard each (8 links per site, stored transposed).
+ * qdp: QDP++ / Chroma full-lattice arrays in QDP++'s checkerboarded (CB2)
+ *   site order, the order the reference's packers read
+ *   (include/qphix/qdp_packer_parscalar.h:51-129,150-230): site
+ *   cb * Vh + (x/2 + Nx/2 (y + Ny (z + Nz t))); FP64 or FP32.
+ *   spinor [nrhs][V][4 spin][3 col][2] (LatticeFermion), gauge
+ *   [4 mu][V][3][3][2] (multi1d<LatticeColorMatrix> u, row-major U_mu(x),
+ *   the four directions contiguous), clover [V][72] (Chroma's
+ *   PrimitiveClovTriang: diag[2][6], then offd[2][15][2]).  Spinor and
+ *   clover transfers touch only checkerboard `cb` of the array (the rest is
+ *   neither read nor written); gauge uploads take both checkerboards. */
 typedef struct {
-  int kind;        /* QPHIX_GPU_HOST_CANONICAL / _QPHIX                 */
+  int kind;        /* QPHIX_GPU_HOST_CANONICAL / _QPHIX / _QDP          */
   int ft;          /* QPHIX_GPU_HOST_F64 / _F32 / _F16                  */
   int veclen;      /* qphix only                                         */
   int soalen;
   int compress12;
   int pad_xy;
   int pad_xyz;
+  int cb;          /* qdp only: the checkerboard a spinor / clover
+                      transfer reads or writes (0 even, 1 odd)            */
 } qphix_gpu_host_layout;
 
 /* Operator parameters: the constructor arguments of Dslash / ClovDslash /

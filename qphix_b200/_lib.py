@@ -14,14 +14,14 @@ OK, EINVAL, ENOMEM, ECUDA, ENOTCONV, EBREAKDOWN, EUNSUPPORTED = 0, -1, -2, -3, -
 F64, F32, F16, BF16, Q16, Q16F32 = 0, 1, 2, 3, 4, 5
 SPINOR, GAUGE, CLOVER, FULLCLOVER = 0, 1, 2, 3
 WILSON, CLOVER_OP, TM, TMCLOVER, NDTM = 0, 1, 2, 3, 4
-HOST_CANONICAL, HOST_QPHIX = 0, 1
+HOST_CANONICAL, HOST_QPHIX, HOST_QDP = 0, 1, 2
 HOST_F64, HOST_F32, HOST_F16 = 0, 1, 2
 SOLVER_CG, SOLVER_BICGSTAB, SOLVER_MR = 0, 1, 2
 
 
 class HostLayout(C.Structure):
     _fields_ = [("kind", C.c_int), ("ft", C.c_int), ("veclen", C.c_int), ("soalen", C.c_int),
-                ("compress12", C.c_int), ("pad_xy", C.c_int), ("pad_xyz", C.c_int)]
+                ("compress12", C.c_int), ("pad_xy", C.c_int), ("pad_xyz", C.c_int), ("cb", C.c_int)]
 
 
 class OpParams(C.Structure):

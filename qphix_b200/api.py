@@ -48,6 +48,25 @@ def qphix_layout(veclen, soalen, compress12, ft="f64", pad_xy=0, pad_xyz=0):
     return h
 
 
+def qdp_layout(cb=0, ft="f64"):
+    """QDP++ / Chroma CB2 full-lattice arrays (the order the reference's
+    qdp_pack_* read, include/qphix/qdp_packer_parscalar.h:51-230); spinor and
+    clover transfers touch checkerboard cb only."""
+    h = L.HostLayout()
+    h.kind = L.HOST_QDP
+    h.ft = {"f64": L.HOST_F64, "f32": L.HOST_F32}[ft]
+    h.cb = cb
+    return h
+
+
+def _qdp_ft(a):
+    if a.dtype in (np.complex128, np.float64):
+        return "f64"
+    if a.dtype in (np.complex64, np.float32):
+        return "f32"
+    raise TypeError(f"QDP arrays are FP64 or FP32, not {a.dtype}")
+
+
 class Lattice:
     """One lattice (Geometry) with its own CUDA stream and reduction workspace."""
 
@@ -155,6 +174,24 @@ class Field:
         assert out.flags["C_CONTIGUOUS"]
         check(L._lib.qphix_gpu_field_download(self.h, out.ctypes.data_as(C.c_void_p),
                                               C.byref(layout), rhs))
+        return out
+
+    # ---- QDP++ / Chroma CB2 full-lattice arrays ---------------------------------
+    def upload_qdp(self, arr, cb=0, rhs=-1):
+        """spinor complex [(nrhs,) V, 4, 3] (checkerboard cb of it), gauge complex
+        [4, V, 3, 3] (both checkerboards), clover float [V, 72] in Chroma's
+        triangle order (checkerboard cb); complex128 / float64 or complex64 /
+        float32."""
+        a = np.ascontiguousarray(arr)
+        lay = qdp_layout(cb if self.kind != L.GAUGE else 0, _qdp_ft(a))
+        check(L._lib.qphix_gpu_field_upload(self.h, a.ctypes.data_as(C.c_void_p), C.byref(lay), -1, rhs))
+        return self
+
+    def download_qdp(self, out, cb, rhs=-1):
+        """write checkerboard cb of a full-lattice spinor / clover array in place"""
+        assert out.flags["C_CONTIGUOUS"]
+        check(L._lib.qphix_gpu_field_download(self.h, out.ctypes.data_as(C.c_void_p),
+                                              C.byref(qdp_layout(cb, _qdp_ft(out))), rhs))
         return out
 
     def convert_from(self, src, scale=1.0):

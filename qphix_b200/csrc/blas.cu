@@ -103,10 +103,10 @@ void launch_clover_in(int prec, Geom g, HostLayout L, const void *host, void *de
   QPX_PREC_SWITCH(prec, (clover_in_kernel<P><<<grid, QPX_BLOCK, 0, st>>>(g, L, host, dev, stride, vpc, nr)));
 }
 
-void launch_clover_out(int prec, Geom g, void *host, const void *dev, long long stride, int vpc, int nr,
-                       dim3 grid, cudaStream_t st)
+void launch_clover_out(int prec, Geom g, HostLayout L, void *host, const void *dev, long long stride, int vpc,
+                       int nr, dim3 grid, cudaStream_t st)
 {
-  QPX_PREC_SWITCH(prec, (clover_out_kernel<P><<<grid, QPX_BLOCK, 0, st>>>(g, host, dev, stride, vpc, nr)));
+  QPX_PREC_SWITCH(prec, (clover_out_kernel<P><<<grid, QPX_BLOCK, 0, st>>>(g, L, host, dev, stride, vpc, nr)));
 }
 
 void launch_mshift(int prec, const MShiftArgs &a, dim3 grid, cudaStream_t st)

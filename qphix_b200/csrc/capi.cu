@@ -340,6 +340,13 @@ static HostLayout make_layout(const qphix_gpu_field_s *f, const qphix_gpu_host_l
     QPX_REQUIRE(L.ft == HFT_F64, "canonical host arrays are FP64");
     return L;
   }
+  if (L.kind == HOST_QDP) {
+    QPX_REQUIRE(L.ft == HFT_F64 || L.ft == HFT_F32, "qdp host arrays are FP64 or FP32");
+    QPX_REQUIRE(f->kind != QPHIX_GPU_FULLCLOVER, "qdp layout: full clover fields are not supported");
+    L.cb = hl->cb;
+    QPX_REQUIRE(f->kind == QPHIX_GPU_GAUGE || L.cb == 0 || L.cb == 1, "qdp layout: cb must be 0 or 1");
+    return L;
+  }
   QPX_REQUIRE(L.kind == HOST_QPHIX, "bad host layout kind");
   const auto *lat = f->lat;
   L.V = hl->veclen;
@@ -362,7 +369,7 @@ static size_t host_elems(const qphix_gpu_field_s *f, const HostLayout &L, int nr
 {
   const auto *lat = f->lat;
   size_t vh = lat->vh;
-  if (L.kind == HOST_CANONICAL) {
+  if (L.kind != HOST_QPHIX) {  // canonical, or the compacted qdp staging
     switch (f->kind) {
     case QPHIX_GPU_SPINOR: return (size_t)nrhs * vh * 24;
     case QPHIX_GPU_GAUGE: return 2 * 4 * vh * 18;
@@ -376,6 +383,23 @@ static size_t host_elems(const qphix_gpu_field_s *f, const HostLayout &L, int nr
   case QPHIX_GPU_GAUGE: return (size_t)L.pxyz * nt * L.S / L.V * 8 * (L.c12 ? 2 : 3) * 3 * 2 * L.V;
   case QPHIX_GPU_CLOVER: return (size_t)L.pxyz * nt * L.S / L.V * 72 * L.V;
   default: return (size_t)L.pxyz * nt * L.S / L.V * 144 * L.V;
+  }
+}
+
+// qdp layout: spinor and clover transfers move checkerboard L.cb of each
+// full-lattice host array ([V] sites = 2 halves of vh) to / from a compacted
+// staging buffer, one contiguous copy per right-hand side
+static void qdp_half_copies(const qphix_gpu_field_s *f, const HostLayout &L, int nr, void *host, void *st,
+                            bool to_device)
+{
+  size_t per = (f->kind == QPHIX_GPU_SPINOR ? 24 : 72) * (size_t)f->lat->vh * host_elem_bytes(L.ft);
+  for (int i = 0; i < nr; i++) {
+    char *h = (char *)host + (2 * (size_t)i + L.cb) * per;
+    char *d = (char *)st + (size_t)i * per;
+    if (to_device)
+      QPX_CUDA(cudaMemcpyAsync(d, h, per, cudaMemcpyHostToDevice, f->lat->stream));
+    else
+      QPX_CUDA(cudaMemcpyAsync(h, d, per, cudaMemcpyDeviceToHost, f->lat->stream));
   }
 }
 
@@ -401,7 +425,12 @@ extern "C" int qphix_gpu_field_upload(qphix_gpu_field f, const void *host, const
     QPX_REQUIRE(rhs < f->nrhs, "rhs index out of range");
     size_t bytes = host_elems(f, L, nr) * host_elem_bytes(L.ft);
     void *st = staging(lat, bytes);
-    QPX_CUDA(cudaMemcpyAsync(st, host, bytes, cudaMemcpyHostToDevice, lat->stream));
+    if (L.kind == HOST_QDP && f->kind != QPHIX_GPU_GAUGE) {
+      QPX_REQUIRE(cb == -1 || cb == L.cb, "qdp layout: the checkerboard is given by layout->cb");
+      qdp_half_copies(f, L, nr, const_cast<void *>(host), st, true);
+    } else {
+      QPX_CUDA(cudaMemcpyAsync(st, host, bytes, cudaMemcpyHostToDevice, lat->stream));
+    }
     switch (f->kind) {
     case QPHIX_GPU_SPINOR: {
       SpinorArg a = rhs_view(f, rhs < 0 ? 0 : rhs);
@@ -410,8 +439,8 @@ extern "C" int qphix_gpu_field_upload(qphix_gpu_field f, const void *host, const
     }
     case QPHIX_GPU_GAUGE: {
       long long slab = (long long)f->spec.nchunk * f->spec.chunk_bytes * lat->stride;
-      if (L.kind == HOST_CANONICAL) {
-        QPX_REQUIRE(cb == -1, "canonical gauge arrays hold both checkerboards (cb = -1)");
+      if (L.kind != HOST_QPHIX) {
+        QPX_REQUIRE(cb == -1, "canonical / qdp gauge arrays hold both checkerboards (cb = -1)");
         for (int c = 0; c < 2; c++)
           launch_gauge_in(f->prec, g, L, st, f->data, lat->stride, slab, f->spec.vpc, f->recon, c, 0,
                           dim3(nblocks_for(lat->vh), 4), lat->stream);
@@ -453,14 +482,17 @@ extern "C" int qphix_gpu_field_download(qphix_gpu_field f, void *host, const qph
       SpinorArg a = rhs_view(f, rhs < 0 ? 0 : rhs);
       launch_spinor_out(f->prec, g, L, st, a, nr, dim3(nblocks_for(lat->vh), nr), lat->stream);
     } else if (f->kind == QPHIX_GPU_CLOVER || f->kind == QPHIX_GPU_FULLCLOVER) {
-      QPX_REQUIRE(L.kind == HOST_CANONICAL, "clover download supports the canonical layout only");
-      launch_clover_out(f->prec, g, st, f->data, lat->stride, f->spec.vpc, f->kind == QPHIX_GPU_CLOVER ? 72 : 144,
+      QPX_REQUIRE(L.kind != HOST_QPHIX, "clover download supports the canonical and qdp layouts");
+      launch_clover_out(f->prec, g, L, st, f->data, lat->stride, f->spec.vpc, f->kind == QPHIX_GPU_CLOVER ? 72 : 144,
                         dim3(nblocks_for(lat->vh)), lat->stream);
     } else {
       throw Error(QPHIX_GPU_EUNSUPPORTED, "gauge download is not supported");
     }
     check_launch();
-    QPX_CUDA(cudaMemcpyAsync(host, st, bytes, cudaMemcpyDeviceToHost, lat->stream));
+    if (L.kind == HOST_QDP)
+      qdp_half_copies(f, L, nr, host, st, false);
+    else
+      QPX_CUDA(cudaMemcpyAsync(host, st, bytes, cudaMemcpyDeviceToHost, lat->stream));
     QPX_CUDA(cudaStreamSynchronize(lat->stream));
   });
 }

@@ -171,8 +171,8 @@ void launch_gauge_in(int prec, Geom g, HostLayout L, const void *host, void *dev
                      long long slab_bytes, int vpc, int recon, int cb, int back, dim3 grid, cudaStream_t st);
 void launch_clover_in(int prec, Geom g, HostLayout L, const void *host, void *dev, long long stride, int vpc,
                       int nr, dim3 grid, cudaStream_t st);
-void launch_clover_out(int prec, Geom g, void *host, const void *dev, long long stride, int vpc, int nr,
-                       dim3 grid, cudaStream_t st);
+void launch_clover_out(int prec, Geom g, HostLayout L, void *host, const void *dev, long long stride, int vpc,
+                       int nr, dim3 grid, cudaStream_t st);
 void launch_mshift(int prec, const MShiftArgs &a, dim3 grid, cudaStream_t st);
 void launch_clover_build(int recon, int prec_out, Geom geo, GaugeArg g, void *out, long long stride, int vpc, int cb,
                          double diag_mass, double cr, double ct, dim3 grid, cudaStream_t st);

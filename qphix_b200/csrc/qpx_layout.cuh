@@ -8,13 +8,19 @@
 //   qphix      the reference's blocked SoA host layout
 //              (include/qphix_codegen/decl_common.h:9-62, geometry.h:156-175,
 //               qdp_packer_parscalar.h:51-129,150-230,232-328)
+//   qdp        QDP++ CB2 full-lattice arrays (site = cb Vh + cb index, the
+//              order qdp_packer_parscalar.h:94-110 reads); spinor and clover
+//              halves of one checkerboard arrive compacted in the staging
+//              buffer ([rhs][Vh][24], [Vh][72]), gauge arrays whole
+//              [4][2][Vh][18]; clover sites in Chroma's triangle order
+//              (diag[2][6], offd[2][15][2])
 #pragma once
 
 #include "qpx_common.cuh"
 
 namespace qpx {
 
-enum HostKind : int { HOST_CANONICAL = 0, HOST_QPHIX = 1 };
+enum HostKind : int { HOST_CANONICAL = 0, HOST_QPHIX = 1, HOST_QDP = 2 };
 enum HostFT : int { HFT_F64 = 0, HFT_F32 = 1, HFT_F16 = 2 };
 
 struct HostLayout {
@@ -22,7 +28,16 @@ struct HostLayout {
   int ft;
   int V, S, c12;
   int nvecs, ngy, pxy, pxyz;
+  int cb;  // qdp: checkerboard of the full-lattice spinor / clover array
 };
+
+// qdp clover: offset within a site of canonical value k (block b = k / 36:
+// diag[6] then offd[15][2]) in Chroma's PrimitiveClovTriang order
+__host__ __device__ __forceinline__ int qdp_clover_off(int k)
+{
+  int b = k / 36, j = k % 36;
+  return j < 6 ? b * 6 + j : 12 + b * 30 + (j - 6);
+}
 
 __device__ __forceinline__ double host_read(const void *p, long long off, int ft)
 {
@@ -44,7 +59,7 @@ __device__ __forceinline__ void host_write(void *p, long long off, int ft, doubl
 __device__ __forceinline__ long long host_spinor_off(const HostLayout &L, const Geom &g, int rhs, int s,
                                                      int k)
 {
-  if (L.kind == HOST_CANONICAL) return ((long long)rhs * g.vh + s) * 24 + k;
+  if (L.kind != HOST_QPHIX) return ((long long)rhs * g.vh + s) * 24 + k;  // canonical / compacted qdp
   int xh = s % g.nxh, r = s / g.nxh;
   int y = r % g.ny;
   r /= g.ny;
@@ -147,8 +162,9 @@ __global__ void gauge_in_kernel(Geom g, HostLayout L, const void *host, void *de
     dst_s = ((c[3] * g.nz + c[2]) * g.ny + c[1]) * g.nxh + c[0] / 2;
   }
   double u[3][3][2];
-  if (L.kind == HOST_CANONICAL) {
-    long long base = (((long long)cb * 4 + mu) * g.vh + s) * 18;
+  if (L.kind != HOST_QPHIX) {
+    long long base = L.kind == HOST_CANONICAL ? (((long long)cb * 4 + mu) * g.vh + s) * 18
+                                              : (((long long)mu * 2 + cb) * g.vh + s) * 18;
     for (int r = 0; r < 3; r++)
       for (int c = 0; c < 3; c++)
         for (int ri = 0; ri < 2; ri++) u[r][c][ri] = host_read(host, base + (r * 3 + c) * 2 + ri, L.ft);
@@ -193,6 +209,9 @@ __global__ void clover_in_kernel(Geom g, HostLayout L, const void *host, void *d
   if (s >= g.vh) return;
   if (L.kind == HOST_CANONICAL) {
     for (int k = 0; k < nr; k++) dev_store_real<P>(dev, stride, vpc, s, k, host_read(host, (long long)s * nr + k, L.ft));
+  } else if (L.kind == HOST_QDP) {
+    for (int k = 0; k < nr; k++)
+      dev_store_real<P>(dev, stride, vpc, s, k, host_read(host, (long long)s * nr + qdp_clover_off(k), L.ft));
   } else {
     long long blk;
     int lane;
@@ -202,13 +221,17 @@ __global__ void clover_in_kernel(Geom g, HostLayout L, const void *host, void *d
   }
 }
 
+// canonical FP64 [Vh][NR], or (qdp) the compacted checkerboard half in
+// Chroma's triangle order, FP64 or FP32
 template <typename P>
-__global__ void clover_out_kernel(Geom g, void *host, const void *dev, long long stride, int vpc, int nr)
+__global__ void clover_out_kernel(Geom g, HostLayout L, void *host, const void *dev, long long stride, int vpc,
+                                  int nr)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= g.vh) return;
+  const bool qdp = L.kind == HOST_QDP;
   for (int k = 0; k < nr; k++)
-    reinterpret_cast<double *>(host)[(long long)s * nr + k] = dev_load_real<P>(dev, stride, vpc, s, k);
+    host_write(host, (long long)s * nr + (qdp ? qdp_clover_off(k) : k), L.ft, dev_load_real<P>(dev, stride, vpc, s, k));
 }
 
 }  // namespace qpx

@@ -442,6 +442,39 @@ def full_clover_to_real(fc):
     return np.ascontiguousarray(np.stack([fc.real, fc.imag], axis=-1)).reshape(-1)
 
 
+# ----------------------------------------------------------------------------
+# QDP++ / Chroma CB2 full-lattice arrays (site = cb * Vh + cb index, the order
+# include/qphix/qdp_packer_parscalar.h:94-110 reads)
+# ----------------------------------------------------------------------------
+
+
+def qdp_spinor(even, odd):
+    """full-lattice LatticeFermion [(nrhs,) V, 4, 3] from the two checkerboards"""
+    return np.ascontiguousarray(np.concatenate([even, odd], axis=-3))
+
+
+def qdp_spinor_cb(full, cb):
+    """checkerboard cb of a full-lattice spinor (a view)"""
+    vhalf = full.shape[-3] // 2
+    return full[..., cb * vhalf:(cb + 1) * vhalf, :, :]
+
+
+def qdp_gauge(gauge):
+    """multi1d<LatticeColorMatrix> [4, V, 3, 3] from the canonical [2, 4, Vh, 3, 3]"""
+    return np.ascontiguousarray(np.transpose(gauge, (1, 0, 2, 3, 4)).reshape(4, -1, 3, 3))
+
+
+def qdp_clover(packed):
+    """Chroma's clover triangles [V, 72] (diag[2][6], offd[2][15][2] per site)
+    from the packed canonical [2 cb, Vh, 2, 36]"""
+    p = packed.reshape(-1, 2, 36)
+    out = np.empty((p.shape[0], 72))
+    for b in range(2):
+        out[:, b * 6:(b + 1) * 6] = p[:, b, :6]
+        out[:, 12 + b * 30:12 + (b + 1) * 30] = p[:, b, 6:]
+    return out
+
+
 def kappa_to_mass(kappa):
     """M = (4 + m) - D/2 normalisation: kappa = 1/(2(4+m))."""
     return 1.0 / (2.0 * kappa) - 4.0
