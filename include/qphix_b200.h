@@ -54,9 +54,14 @@ enum { QPHIX_GPU_SPINOR = 0, QPHIX_GPU_GAUGE = 1, QPHIX_GPU_CLOVER = 2, QPHIX_GP
  * twisted_mass = mu and epsilon).  Its fields hold flavour pairs: right-hand
  * side 2k is the up, 2k + 1 the down flavour.  As a Dslash kind it is the
  * Wilson hop followed by mu_inv [(alpha - i isign mu g5 tau3) + eps tau1];
- * solved with CG (flavour-coupled: the pair is one system). */
+ * solved with CG (flavour-coupled: the pair is one system).
+ * QPHIX_GPU_NDTMCLOVER: the two-flavour twisted-mass clover operator
+ * (include/qphix/ndtm_reuse_operator_clover.h:23-165; twisted_mass = mu,
+ * epsilon), flavour pairs as for NDTM; its operator takes clov = A,
+ * invclov = the packed flavour-off-diagonal inverse and finv0 / finv1 = the
+ * full flavour-diagonal inverses (qphix_gpu_clover_invert_ndtm builds them). */
 enum { QPHIX_GPU_WILSON = 0, QPHIX_GPU_CLOVER_OP = 1, QPHIX_GPU_TM = 2, QPHIX_GPU_TMCLOVER = 3,
-       QPHIX_GPU_NDTM = 4 };
+       QPHIX_GPU_NDTM = 4, QPHIX_GPU_NDTMCLOVER = 5 };
 enum { QPHIX_GPU_HOST_CANONICAL = 0, QPHIX_GPU_HOST_QPHIX = 1, QPHIX_GPU_HOST_QDP = 2 };
 enum { QPHIX_GPU_HOST_F64 = 0, QPHIX_GPU_HOST_F32 = 1, QPHIX_GPU_HOST_F16 = 2 };
 enum { QPHIX_GPU_SOLVER_CG = 0, QPHIX_GPU_SOLVER_BICGSTAB = 1, QPHIX_GPU_SOLVER_MR = 2 };
@@ -189,6 +194,17 @@ int qphix_gpu_dslash_achimbdpsi(const qphix_gpu_op_params *p, qphix_gpu_field re
                                 double beta, int isign, int cb, double musign);
 int qphix_gpu_dslash_dir(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
                          qphix_gpu_field gauge, int cb, int dir);
+/* Two-flavour twisted-mass clover hop: the Wilson hop of both flavours of
+ * each (up, down) pair followed by the two-flavour inverse clover term --
+ * Dslash::dslash then TMClovDslash::two_flav_inverse_clover_term
+ * (tm_clov_dslash_def.h:96-110, ndtm_reuse_operator_clover.h:121-126), one
+ * kernel.  finv_up / finv_dn are used as given for isign = +1 and swapped for
+ * isign = -1.  The second half of that operator is
+ * qphix_gpu_dslash_achimbdpsi with kind QPHIX_GPU_NDTMCLOVER, aux = A and
+ * rho = twisted_mass (two_flav_AChiMinusBDPsi, tm_clov_dslash_def.h:84-92). */
+int qphix_gpu_dslash_two_flav_clover(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                                     qphix_gpu_field gauge, qphix_gpu_field finv_up, qphix_gpu_field finv_dn,
+                                     qphix_gpu_field clov_odiag, int isign, int cb);
 int qphix_gpu_clover_apply(qphix_gpu_field res, qphix_gpu_field chi, qphix_gpu_field clov);
 
 /* ---- clover term on the device ----------------------------------------------
@@ -206,6 +222,13 @@ int qphix_gpu_clover_build(qphix_gpu_field clov, qphix_gpu_field gauge, int cb, 
 int qphix_gpu_clover_invert(qphix_gpu_field dst, qphix_gpu_field src);
 int qphix_gpu_clover_invert_twisted(qphix_gpu_field dst_plus, qphix_gpu_field dst_minus, qphix_gpu_field src,
                                     double mu);
+/* The inverse of the two-flavour diagonal block [[A + i mu g5, -eps],
+ * [-eps, A - i mu g5]] of checkerboard A: finv_up = Q (A - i mu g5), finv_dn =
+ * Q (A + i mu g5) (full clover fields) and clov_odiag = eps Q (clover field),
+ * Q = (A^2 + mu^2 - eps^2)^-1 -- the invclov[2] and invclov_odiag arguments of
+ * EvenOddNDTMCloverReuseOperator (ndtm_reuse_operator_clover.h:38-50). */
+int qphix_gpu_clover_invert_ndtm(qphix_gpu_field finv_up, qphix_gpu_field finv_dn, qphix_gpu_field clov_odiag,
+                                 qphix_gpu_field src, double mu, double eps);
 int qphix_gpu_clover_convert(qphix_gpu_field dst, qphix_gpu_field src);
 
 /* ---- even-odd operators ----------------------------------------------------

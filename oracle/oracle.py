@@ -118,7 +118,7 @@ def make_lattice(dims, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0, tbc=None):
 class OracleOp:
     """Keeps the numpy buffers alive for an or_operator."""
 
-    KINDS = {"wilson": 0, "clover": 1, "tm": 2, "tmclover": 3, "ndtm": 4}
+    KINDS = {"wilson": 0, "clover": 1, "tm": 2, "tmclover": 3, "ndtm": 4, "ndtmclover": 5}
 
     def __init__(self, kind, L, gauge, clov=None, invclov=None, finv=None,
                  mass=0.0, twisted_mass=0.0, rho=0.0, epsilon=0.0):
@@ -149,7 +149,7 @@ class OracleOp:
         self.op = op
         self.vh = int(np.prod(L.dims[:])) // 2
         # two-flavour operators act on [flavour][Vh][4][3]
-        self.shape = (2, self.vh, 4, 3) if kind == "ndtm" else (self.vh, 4, 3)
+        self.shape = (2, self.vh, 4, 3) if kind in ("ndtm", "ndtmclover") else (self.vh, 4, 3)
 
     def apply(self, x, isign=1, target_cb=1):
         xi = _r(x)

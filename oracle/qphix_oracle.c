@@ -371,7 +371,7 @@ static const double *gauge_cb(const or_operator *op, int cb)
 
 long or_op_len(const or_operator *op)
 {
-  return 24 * or_vh(&op->L) * (op->kind == OR_OP_NDTM ? 2 : 1);
+  return 24 * or_vh(&op->L) * ((op->kind == OR_OP_NDTM || op->kind == OR_OP_NDTMCLOVER) ? 2 : 1);
 }
 
 /* include/qphix/ndtm_reuse_operator.h:68-110 (EvenOddNDTMWilsonReuseOperator):
@@ -416,11 +416,50 @@ static void ndtm_apply(const or_operator *op, double *res, const double *in, int
   free(tp);
 }
 
+/* include/qphix/ndtm_reuse_operator_clover.h:117-128 (EvenOddNDTMCloverReuseOperator):
+   t_f = D_{other,target} in_f (Wilson hop, both flavours);
+   two_flav_inverse_clover_term (tm_clov_dslash_body.h:1184-1204; per site
+   codegen/dslash_common.cc:1198-1341):
+     u_up = F_a t_up + C t_dn, u_dn = F_b t_dn + C t_up,
+     (F_a, F_b) = (finv[0], finv[1]) for isign = +1, swapped for isign = -1;
+   two_flav_AChiMinusBDPsi (tm_clov_dslash_body.h:1345-1365, flavour sign of
+   rho :983): res_f = A in_f + i s_f rho isign g5 in_f - 0.25 D u_f - eps in_{1-f},
+   rho = twisted_mass, s_up = +1, s_dn = -1 */
+static void ndtmclov_apply(const or_operator *op, double *res, const double *in, int isign, int target_cb)
+{
+  const or_lattice *L = &op->L;
+  long vh = or_vh(L), n1 = 24 * vh;
+  int other = 1 - target_cb;
+  double *t = (double *)malloc(sizeof(double) * 2 * n1);
+  double *u = (double *)malloc(sizeof(double) * 2 * n1);
+  double *c = (double *)malloc(sizeof(double) * n1);
+  for (int f = 0; f < 2; f++) or_dslash(L, t + f * n1, in + f * n1, gauge_cb(op, other), isign, other);
+  const double *fa = isign == 1 ? op->finv[0] : op->finv[1];
+  const double *fb = isign == 1 ? op->finv[1] : op->finv[0];
+  for (int f = 0; f < 2; f++) {
+    or_fullclover_apply(vh, u + f * n1, t + f * n1, f == 0 ? fa : fb);
+    or_clover_apply(vh, c, t + (1 - f) * n1, op->invclov);
+    for (long i = 0; i < n1; i++) u[f * n1 + i] += c[i];
+  }
+  for (int f = 0; f < 2; f++) {
+    or_clov_achimbdpsi(L, res + f * n1, u + f * n1, in + f * n1, op->gauge, op->clov, 0.25,
+                       (f == 0 ? 1.0 : -1.0) * op->twisted_mass, isign, target_cb);
+    for (long i = 0; i < n1; i++) res[f * n1 + i] -= op->epsilon * in[(1 - f) * n1 + i];
+  }
+  free(t);
+  free(u);
+  free(c);
+}
+
 void or_eo_apply(const or_operator *op, double *res, const double *in,
                  int isign, int target_cb)
 {
   if (op->kind == OR_OP_NDTM) {
     ndtm_apply(op, res, in, isign, target_cb);
+    return;
+  }
+  if (op->kind == OR_OP_NDTMCLOVER) {
+    ndtmclov_apply(op, res, in, isign, target_cb);
     return;
   }
   const or_lattice *L = &op->L;

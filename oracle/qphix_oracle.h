@@ -83,8 +83,13 @@ void or_tmclov_dslash(const or_lattice *L, double *res, const double *psi,
 
 /* ---- even-odd operators ------------------------------------------------- */
 /* OR_OP_NDTM: two-flavour (non-degenerate) twisted-mass Wilson, vectors
-   [flavour up, down][Vh][24] (include/qphix/ndtm_reuse_operator.h) */
-enum { OR_OP_WILSON = 0, OR_OP_CLOVER = 1, OR_OP_TM = 2, OR_OP_TMCLOVER = 3, OR_OP_NDTM = 4 };
+   [flavour up, down][Vh][24] (include/qphix/ndtm_reuse_operator.h)
+   OR_OP_NDTMCLOVER: two-flavour twisted-mass clover
+   (include/qphix/ndtm_reuse_operator_clover.h): clov = A (target cb),
+   invclov = packed flavour-off-diagonal inverse, finv = full up / down
+   flavour-diagonal inverses (other cb), twisted_mass = mu, epsilon */
+enum { OR_OP_WILSON = 0, OR_OP_CLOVER = 1, OR_OP_TM = 2, OR_OP_TMCLOVER = 3, OR_OP_NDTM = 4,
+       OR_OP_NDTMCLOVER = 5 };
 typedef struct {
   int kind;
   or_lattice L;

@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libqphix_b200.so")
 OK, EINVAL, ENOMEM, ECUDA, ENOTCONV, EBREAKDOWN, EUNSUPPORTED = 0, -1, -2, -3, -4, -5, -6
 F64, F32, F16, BF16, Q16, Q16F32 = 0, 1, 2, 3, 4, 5
 SPINOR, GAUGE, CLOVER, FULLCLOVER = 0, 1, 2, 3
-WILSON, CLOVER_OP, TM, TMCLOVER, NDTM = 0, 1, 2, 3, 4
+WILSON, CLOVER_OP, TM, TMCLOVER, NDTM, NDTMCLOVER = 0, 1, 2, 3, 4, 5
 HOST_CANONICAL, HOST_QPHIX, HOST_QDP = 0, 1, 2
 HOST_F64, HOST_F32, HOST_F16 = 0, 1, 2
 SOLVER_CG, SOLVER_BICGSTAB, SOLVER_MR = 0, 1, 2
@@ -89,10 +89,12 @@ _SIGS = {
     "qphix_gpu_dslash": ([C.POINTER(OpParams), P, P, P, P, P, I_, I_], I_),
     "qphix_gpu_dslash_achimbdpsi": ([C.POINTER(OpParams), P, P, P, P, P, D, D, I_, I_, D], I_),
     "qphix_gpu_dslash_dir": ([C.POINTER(OpParams), P, P, P, I_, I_], I_),
+    "qphix_gpu_dslash_two_flav_clover": ([C.POINTER(OpParams), P, P, P, P, P, P, I_, I_], I_),
     "qphix_gpu_clover_apply": ([P, P, P], I_),
     "qphix_gpu_clover_build": ([P, P, I_, D, D, D], I_),
     "qphix_gpu_clover_invert": ([P, P], I_),
     "qphix_gpu_clover_invert_twisted": ([P, P, P, D], I_),
+    "qphix_gpu_clover_invert_ndtm": ([P, P, P, P, D, D], I_),
     "qphix_gpu_clover_convert": ([P, P], I_),
     "qphix_gpu_eo_op_create": ([C.POINTER(OpParams), P, P, P, P, P, PP], I_),
     "qphix_gpu_eo_op_destroy": ([P], I_),

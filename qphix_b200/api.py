@@ -326,6 +326,14 @@ def clover_invert_twisted(dst_plus, dst_minus, src, mu):
     return dst_plus, dst_minus
 
 
+def clover_invert_ndtm(finv_up, finv_dn, clov_odiag, src, mu, eps):
+    """the two-flavour inverses of EvenOddNDTMCloverReuseOperator
+    (ndtm_reuse_operator_clover.h:38-50): Q (A -/+ i mu g5) and eps Q,
+    Q = (A^2 + mu^2 - eps^2)^-1"""
+    check(L._lib.qphix_gpu_clover_invert_ndtm(finv_up.h, finv_dn.h, clov_odiag.h, src.h, mu, eps))
+    return finv_up, finv_dn, clov_odiag
+
+
 def clover_convert(dst, src):
     check(L._lib.qphix_gpu_clover_convert(dst.h, src.h))
     return dst
@@ -438,6 +446,40 @@ class EvenOddNDTMWilsonOperator(EvenOddLinearOperator):
     def __init__(self, mass, twisted_mass, epsilon, u, t_boundary=-1.0, aniso_s=1.0, aniso_t=1.0):
         super().__init__(op_params(L.NDTM, t_boundary, aniso_s, aniso_t, None, None, mass=mass,
                                    twisted_mass=twisted_mass, epsilon=epsilon), u)
+
+
+class EvenOddNDTMCloverOperator(EvenOddLinearOperator):
+    """include/qphix/ndtm_reuse_operator_clover.h:23-165
+    (EvenOddNDTMCloverReuseOperator): the two-flavour twisted-mass clover
+    operator; clov = A of the target checkerboard, invclov_odiag and
+    invclov = (up, down) the inverses of the other checkerboard's two-flavour
+    block (clover_invert_ndtm).  Fields hold (up, down) pairs as for
+    EvenOddNDTMWilsonOperator."""
+
+    def __init__(self, twisted_mass, epsilon, u, clov, invclov_odiag, invclov, t_boundary=-1.0,
+                 aniso_s=1.0, aniso_t=1.0):
+        super().__init__(op_params(L.NDTMCLOVER, t_boundary, aniso_s, aniso_t, None, None,
+                                   twisted_mass=twisted_mass, epsilon=epsilon), u, clov, invclov_odiag,
+                         tuple(invclov))
+
+
+class TMClovDslashTwoFlav:
+    """The two-flavour members of TMClovDslash (tm_clov_dslash_def.h:76-110):
+    the Wilson hop followed by the two-flavour inverse clover term, and
+    two_flav_AChiMinusBDPsi."""
+
+    def __init__(self, lat, t_boundary, aniso_s, aniso_t, twisted_mass, epsilon):
+        self.lat = lat
+        self.p = op_params(L.NDTMCLOVER, t_boundary, aniso_s, aniso_t, twisted_mass=twisted_mass,
+                           epsilon=epsilon)
+
+    def dslash_inverse_clover(self, res, psi, u, invclov, invclov_odiag, isign, cb):
+        check(L._lib.qphix_gpu_dslash_two_flav_clover(C.byref(self.p), res.h, psi.h, u.h, invclov[0].h,
+                                                      invclov[1].h, invclov_odiag.h, isign, cb))
+
+    def two_flav_AChiMinusBDPsi(self, res, psi, chi, u, clov, beta, isign, cb):
+        check(L._lib.qphix_gpu_dslash_achimbdpsi(C.byref(self.p), res.h, psi.h, chi.h, u.h, clov.h, 0.0,
+                                                 beta, isign, cb, 1.0))
 
 
 class EvenOddTMCloverOperator(EvenOddLinearOperator):

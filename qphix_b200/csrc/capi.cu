@@ -647,7 +647,7 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
                                 const DslashArgs &a)
 {
   const bool gen = a.dir_mask != 0xFFu || a.tbc_mask != 0;
-  if (epi == EPI_NDTM || achi == ACHI_NDTM) {  // both flavours of a site in one thread
+  if (is_two_flavour(epi, achi)) {  // both flavours of a site in one thread
     QPX_REQUIRE(!gen, "two-flavour twisted mass takes all hops without twisted boundary phases");
     DslashShape sh;
     sh.R = 2;
@@ -814,7 +814,7 @@ static void tm_derived(const qphix_gpu_op_params &p, double &dmu, double &dmu_in
 // res = EPI(D psi) on checkerboard cb
 static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphix_gpu_field_s *psi,
                         qphix_gpu_field_s *gauge, qphix_gpu_field_s *aux, qphix_gpu_field_s *aux2, int isign,
-                        int cb, unsigned dir_mask = 0xFFu)
+                        int cb, unsigned dir_mask = 0xFFu, qphix_gpu_field_s *aux3 = nullptr)
 {
   require_spinor(res, "res");
   require_spinor(psi, "psi");
@@ -861,6 +861,21 @@ static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qp
     a.mu = -isign * mu * mu_inv;
     a.eps = eps * mu_inv;
     epi = EPI_NDTM;
+    break;
+  }
+  case QPHIX_GPU_NDTMCLOVER: {  // include/qphix/ndtm_reuse_operator_clover.h:121-126
+    QPX_REQUIRE(res->nrhs % 2 == 0, "two-flavour fields hold an even number of right-hand sides (up, down pairs)");
+    QPX_REQUIRE(aux && aux2 && aux->kind == QPHIX_GPU_FULLCLOVER && aux2->kind == QPHIX_GPU_FULLCLOVER,
+                "two-flavour clover dslash needs the two full flavour-diagonal inverses");
+    QPX_REQUIRE(aux3 && aux3->kind == QPHIX_GPU_CLOVER, "two-flavour clover dslash needs the off-diagonal inverse");
+    require_same(res, aux);
+    require_same(res, aux2);
+    require_same(res, aux3);
+    // isign swaps the flavour-diagonal inverses (tm_clov_dslash_body.h:1193-1200)
+    a.clov = (isign == 1 ? aux : aux2)->carg();
+    a.clov2 = (isign == 1 ? aux2 : aux)->carg();
+    a.clov3 = aux3->carg();
+    epi = EPI_NDFCLOV;
     break;
   }
   default:
@@ -926,6 +941,15 @@ static void achi_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphi
     a.eps = p.epsilon;
     achi = ACHI_NDTM;
     break;
+  case QPHIX_GPU_NDTMCLOVER:  // include/qphix/tm_clov_dslash_body.h:1345-1365
+    QPX_REQUIRE(res->nrhs % 2 == 0, "two-flavour fields hold an even number of right-hand sides (up, down pairs)");
+    QPX_REQUIRE(aux && aux->kind == QPHIX_GPU_CLOVER, "two-flavour clover achimbdpsi needs the clover term A");
+    require_same(res, aux);
+    a.clov = aux->carg();
+    a.rho = p.twisted_mass;  // the up flavour's; the down flavour's is -rho (:983)
+    a.eps = p.epsilon;
+    achi = ACHI_NDCLOV;
+    break;
   default:
     throw Error(QPHIX_GPU_EINVAL, "bad operator kind");
   }
@@ -951,7 +975,21 @@ extern "C" int qphix_gpu_dslash(const qphix_gpu_op_params *p, qphix_gpu_field re
 {
   return guard([&] {
     QPX_REQUIRE(p, "null params");
+    QPX_REQUIRE(p->kind != QPHIX_GPU_NDTMCLOVER, "the two-flavour clover hop is qphix_gpu_dslash_two_flav_clover");
     dslash_core(*p, res, psi, gauge, aux, aux2, isign, cb);
+  });
+}
+
+extern "C" int qphix_gpu_dslash_two_flav_clover(const qphix_gpu_op_params *p, qphix_gpu_field res,
+                                                qphix_gpu_field psi, qphix_gpu_field gauge,
+                                                qphix_gpu_field finv_up, qphix_gpu_field finv_dn,
+                                                qphix_gpu_field clov_odiag, int isign, int cb)
+{
+  return guard([&] {
+    QPX_REQUIRE(p, "null params");
+    qphix_gpu_op_params q = *p;
+    q.kind = QPHIX_GPU_NDTMCLOVER;
+    dslash_core(q, res, psi, gauge, finv_up, finv_dn, isign, cb, 0xFFu, clov_odiag);
   });
 }
 
@@ -1041,6 +1079,30 @@ extern "C" int qphix_gpu_clover_invert(qphix_gpu_field dst, qphix_gpu_field src)
   });
 }
 
+extern "C" int qphix_gpu_clover_invert_ndtm(qphix_gpu_field finv_up, qphix_gpu_field finv_dn,
+                                            qphix_gpu_field clov_odiag, qphix_gpu_field src, double mu, double eps)
+{
+  return guard([&] {
+    QPX_REQUIRE(finv_up && finv_dn && clov_odiag && src, "null argument");
+    QPX_REQUIRE(finv_up->kind == QPHIX_GPU_FULLCLOVER && finv_dn->kind == QPHIX_GPU_FULLCLOVER,
+                "flavour-diagonal inverses must be full clover fields");
+    QPX_REQUIRE(clov_odiag->kind == QPHIX_GPU_CLOVER && src->kind == QPHIX_GPU_CLOVER,
+                "src and the off-diagonal inverse must be clover fields");
+    QPX_REQUIRE(finv_up->prec == finv_dn->prec && finv_up->prec == clov_odiag->prec,
+                "destinations must share a precision");
+    QPX_REQUIRE(same_shape(finv_up->lat, src->lat) && same_shape(finv_dn->lat, src->lat) &&
+                    same_shape(clov_odiag->lat, src->lat),
+                "fields belong to lattices of different shape");
+    QPX_REQUIRE(clov_odiag != src, "distinct fields required");
+    auto *lat = src->lat;
+    launch_clover_invert(src->prec, finv_up->prec, lat->geom(), src->data, lat->stride, src->spec.vpc,
+                         finv_up->data, finv_dn->data, finv_up->spec.vpc, 2, mu,
+                         dim3((unsigned)((lat->vh + 63) / 64)), lat->stream, clov_odiag->data, clov_odiag->spec.vpc,
+                         eps);
+    check_launch();
+  });
+}
+
 extern "C" int qphix_gpu_clover_invert_twisted(qphix_gpu_field dst_plus, qphix_gpu_field dst_minus,
                                                qphix_gpu_field src, double mu)
 {
@@ -1087,6 +1149,9 @@ extern "C" int qphix_gpu_eo_op_create(const qphix_gpu_op_params *p, qphix_gpu_fi
     QPX_REQUIRE(gauge && gauge->kind == QPHIX_GPU_GAUGE, "gauge must be a gauge field");
     if (p->kind == QPHIX_GPU_CLOVER_OP) QPX_REQUIRE(clov && invclov, "clover operator needs clov and invclov");
     if (p->kind == QPHIX_GPU_TMCLOVER) QPX_REQUIRE(clov && finv0 && finv1, "tm clover operator needs clov, finv0/1");
+    if (p->kind == QPHIX_GPU_NDTMCLOVER)
+      QPX_REQUIRE(clov && invclov && finv0 && finv1,
+                  "two-flavour clover operator needs clov, invclov (off-diagonal inverse) and finv0/1");
     auto *op = new qphix_gpu_eo_op_s();
     op->serial = g_serial++;
     op->p = *p;
@@ -1152,6 +1217,10 @@ static void eo_apply(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *res, qphix_gpu_fi
     break;
   case QPHIX_GPU_TMCLOVER:  // include/qphix/twisted_mass_clover.h:92-102
     dslash_core(p, tmp, in, op->gauge, op->finv0, op->finv1, isign, other);
+    achi_core(p, res, tmp, in, op->gauge, op->clov, 0.0, 0.25, isign, target_cb, 1.0, o);
+    break;
+  case QPHIX_GPU_NDTMCLOVER:  // include/qphix/ndtm_reuse_operator_clover.h:117-128
+    dslash_core(p, tmp, in, op->gauge, op->finv0, op->finv1, isign, other, 0xFFu, op->invclov);
     achi_core(p, res, tmp, in, op->gauge, op->clov, 0.0, 0.25, isign, target_cb, 1.0, o);
     break;
   default:
@@ -1488,11 +1557,13 @@ void sync_op_fields(const qphix_gpu_eo_op_s *op, const qphix_gpu_lattice_s *lat)
   }
 }
 
+static bool two_flavour_kind(int kind) { return kind == QPHIX_GPU_NDTM || kind == QPHIX_GPU_NDTMCLOVER; }
+
 void check_solver_fields(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs,
                          bool two_flavour_ok = false)
 {
   QPX_REQUIRE(op, "null operator");
-  QPX_REQUIRE(two_flavour_ok || op->p.kind != QPHIX_GPU_NDTM,
+  QPX_REQUIRE(two_flavour_ok || !two_flavour_kind(op->p.kind),
               "two-flavour operators are solved with CG (the flavour pair as one system)");
   require_spinor(x, "x");
   require_spinor(rhs, "rhs");
@@ -1542,7 +1613,7 @@ void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
   const int nr = x->nrhs, prec = x->prec;
   // two-flavour operator: each (up, down) pair is one system whose inner
   // products sum over both flavours (include/qphix/invcg.h with num_flav = 2)
-  const bool coupled = op->p.kind == QPHIX_GPU_NDTM;
+  const bool coupled = two_flavour_kind(op->p.kind);
   QPX_REQUIRE(!coupled || nr % 2 == 0, "two-flavour fields hold (up, down) pairs");
   Timer timer(lat);
   Tmp mp(lat, prec, nr), mmp(lat, prec, nr), r(lat, prec, nr), p(lat, prec, nr);

@@ -12,6 +12,13 @@
 //   clover_invert  packed A^-1 (exact 6x6 inverse per block)
 //   clover_invert_twisted  full (A + i mu g5)^-1 and (A - i mu g5)^-1 for
 //                  the twisted-mass clover operator (g5 = +1 on block 0)
+//   clover_invert_ndtm  the inverse of the two-flavour diagonal block
+//                  [[A + i mu g5, -eps], [-eps, A - i mu g5]]: with
+//                  Q = (A^2 + mu^2 - eps^2)^-1 (A commutes with g5) it is
+//                  [[Q (A - i mu g5), eps Q], [eps Q, Q (A + i mu g5)]]; the
+//                  flavour-diagonal blocks as full clover fields, eps Q packed
+//                  (the fields include/qphix/ndtm_reuse_operator_clover.h:38-50
+//                   takes, tm_clov_dslash_def.h:96-104)
 // All arithmetic in FP64; results are stored in the destination field's
 // precision.
 #include "qpx_finalize.cuh"
@@ -189,10 +196,11 @@ __device__ void invert6(zd a[6][6], zd inv[6][6])
   }
 }
 
-// mode 0: packed Hermitian inverse of A; mode 1: full inverses of A +/- i mu g5
+// mode 0: packed Hermitian inverse of A; mode 1: full inverses of A +/- i mu g5;
+// mode 2: the two-flavour inverses (full out0 = up, out1 = down, packed out2)
 template <typename Pin, typename Q>
 __global__ void clover_invert_kernel(Geom geo, const void *in, long long stride, int vpc_in, void *out0, void *out1,
-                                     int vpc_out, int mode, double mu)
+                                     int vpc_out, int mode, double mu, void *out2, int vpc_out2, double eps)
 {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= geo.vh) return;
@@ -207,7 +215,38 @@ __global__ void clover_invert_kernel(Geom geo, const void *in, long long stride,
         a[i][j] = v;
         a[j][i] = conj(v);
       }
-    if (mode == 0) {
+    if (mode == 2) {
+      const double g5 = (b == 0) ? 1.0 : -1.0;
+      zd m[6][6], q[6][6];
+      for (int i = 0; i < 6; i++)
+        for (int j = 0; j < 6; j++) {
+          zd v = {0.0, 0.0};
+          for (int k = 0; k < 6; k++) v = v + a[i][k] * a[k][j];
+          m[i][j] = v;
+        }
+      for (int i = 0; i < 6; i++) m[i][i].re += mu * mu - eps * eps;
+      invert6(m, q);
+      for (int f = 0; f < 2; f++) {  // up: Q (A - i mu g5), down: Q (A + i mu g5)
+        const double tw = (f == 0 ? -1.0 : 1.0) * mu * g5;
+        void *o = f == 0 ? out0 : out1;
+        for (int i = 0; i < 6; i++)
+          for (int j = 0; j < 6; j++) {
+            zd v = {0.0, 0.0};
+            for (int k = 0; k < 6; k++) v = v + q[i][k] * a[k][j];
+            v.re -= tw * q[i][j].im;  // + i tw Q_ij
+            v.im += tw * q[i][j].re;
+            dev_store_real<Q>(o, stride, vpc_out, s, 72 * b + (i * 6 + j) * 2, v.re);
+            dev_store_real<Q>(o, stride, vpc_out, s, 72 * b + (i * 6 + j) * 2 + 1, v.im);
+          }
+      }
+      for (int i = 0; i < 6; i++) dev_store_real<Q>(out2, stride, vpc_out2, s, 36 * b + i, eps * q[i][i].re);
+      for (int i = 1; i < 6; i++)
+        for (int j = 0; j < i; j++) {
+          int od = i * (i - 1) / 2 + j;
+          dev_store_real<Q>(out2, stride, vpc_out2, s, 36 * b + 6 + 2 * od, eps * q[i][j].re);
+          dev_store_real<Q>(out2, stride, vpc_out2, s, 36 * b + 7 + 2 * od, eps * q[i][j].im);
+        }
+    } else if (mode == 0) {
       zd inv[6][6];
       invert6(a, inv);
       for (int i = 0; i < 6; i++) dev_store_real<Q>(out0, stride, vpc_out, s, 36 * b + i, inv[i][i].re);
@@ -281,10 +320,12 @@ void launch_clover_build(int recon, int prec_out, Geom geo, GaugeArg g, void *ou
 }
 
 void launch_clover_invert(int prec_in, int prec_out, Geom geo, const void *in, long long stride, int vpc_in, void *o0,
-                          void *o1, int vpc_out, int mode, double mu, dim3 grid, cudaStream_t st)
+                          void *o1, int vpc_out, int mode, double mu, dim3 grid, cudaStream_t st, void *o2,
+                          int vpc_out2, double eps)
 {
   QPX_IN_SWITCH(prec_in, QPX_OUT_SWITCH(prec_out, (clover_invert_kernel<Pin, Q><<<grid, 64, 0, st>>>(
-                                                       geo, in, stride, vpc_in, o0, o1, vpc_out, mode, mu))));
+                                                       geo, in, stride, vpc_in, o0, o1, vpc_out, mode, mu, o2,
+                                                       vpc_out2, eps))));
 }
 
 void launch_clover_convert(int prec_in, int prec_out, Geom geo, const void *in, int vpc_in, void *out, int vpc_out,

@@ -39,6 +39,10 @@ void launch_dslash_nd(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStr
     dslash_kernel<P, RECON, EPI_NDTM, ACHI_NONE, 2, S, 1, false><<<grid, block, 0, st>>>(a);
   else if (epi == EPI_NONE && achi == ACHI_NDTM)
     dslash_kernel<P, RECON, EPI_NONE, ACHI_NDTM, 2, S, 1, false><<<grid, block, 0, st>>>(a);
+  else if (achi == ACHI_NONE && epi == EPI_NDFCLOV)
+    dslash_kernel<P, RECON, EPI_NDFCLOV, ACHI_NONE, 2, S, 1, false><<<grid, block, 0, st>>>(a);
+  else if (epi == EPI_NONE && achi == ACHI_NDCLOV)
+    dslash_kernel<P, RECON, EPI_NONE, ACHI_NDCLOV, 2, S, 1, false><<<grid, block, 0, st>>>(a);
   else
     throw Error(QPHIX_GPU_EINVAL, "unsupported two-flavour dslash combination");
 }
@@ -65,7 +69,7 @@ bool launch_dslash_p(int recon, int epi, int achi, const DslashShape &sh, const 
 {
   constexpr bool fp32 = std::is_same<typename P::real, float>::value;
   if (recon != 12 && recon != 18) return false;
-  if (epi == EPI_NDTM || achi == ACHI_NDTM) {  // two-flavour twisted mass: R = 2 only
+  if (is_two_flavour(epi, achi)) {  // two-flavour twisted mass (clover): R = 2 only
     if (sh.R != 2 || sh.SP != 1 || sh.gen) return false;
     if (!a) return true;
     const bool plus = a->isign == 1;

@@ -50,8 +50,22 @@ namespace qpx {
 //   ACHI_NDTM: out_f = alpha (1 + i s_f isign mu g5) chi_f - beta acc_f
 //              - eps chi_{1-f}, s_up = +1, s_dn = -1
 //              (include/qphix/tm_dslash_body.h:1174-1207)
-enum Epi : int { EPI_NONE = 0, EPI_CLOV = 1, EPI_TMINV = 2, EPI_FCLOV = 3, EPI_NDTM = 4 };
-enum Achi : int { ACHI_NONE = 0, ACHI_ALPHA = 1, ACHI_CLOV = 2, ACHI_TM = 3, ACHI_NDTM = 4 };
+// and the two-flavour twisted-mass clover operator
+// (include/qphix/ndtm_reuse_operator_clover.h:117-128):
+//   EPI_NDFCLOV: out_up = F_a acc_up + C acc_dn, out_dn = F_b acc_dn + C acc_up
+//              with F_a, F_b the full flavour-diagonal inverses (clov, clov2;
+//              the host swaps them for isign = -1) and C the packed
+//              flavour-off-diagonal inverse (clov3)
+//              (tm_clov_dslash_body.h:1184-1204, codegen/dslash_common.cc:
+//               1198-1341)
+//   ACHI_NDCLOV: out_f = A chi_f + i s_f isign rho g5 chi_f - beta acc_f
+//              - eps chi_{1-f} (tm_clov_dslash_body.h:983,1345-1365)
+enum Epi : int { EPI_NONE = 0, EPI_CLOV = 1, EPI_TMINV = 2, EPI_FCLOV = 3, EPI_NDTM = 4, EPI_NDFCLOV = 5 };
+enum Achi : int { ACHI_NONE = 0, ACHI_ALPHA = 1, ACHI_CLOV = 2, ACHI_TM = 3, ACHI_NDTM = 4, ACHI_NDCLOV = 5 };
+__host__ __device__ inline bool is_two_flavour(int epi, int achi)
+{
+  return epi == EPI_NDTM || epi == EPI_NDFCLOV || achi == ACHI_NDTM || achi == ACHI_NDCLOV;
+}
 enum Post : int {
   POST_STORE = 0,  // store out
   POST_CG = 1,     // r -= a out ; x += a p ; |r|^2   (a = state S_A[rhs]); out not stored
@@ -86,6 +100,7 @@ struct DslashArgs {
   SpinorArg out, in, chi;
   GaugeArg gauge;
   CloverArg clov;
+  CloverArg clov2, clov3;  // EPI_NDFCLOV: down-flavour full inverse, off-diagonal packed inverse
   double coeff_s;       // spatial hops (aniso_s, times the caller's beta)
   double coeff_t;       // temporal hops away from the t edges (aniso_t)
   double coeff_t_edge;  // temporal hops across the global t edge (aniso_t * t_boundary)
@@ -265,6 +280,34 @@ __device__ __forceinline__ void herm6_apply(const T *blk, const T *in, T *out, i
   for (int i = 0; i < 6; i++) x[i] = {in[((2 * b + i / 3) * 3 + i % 3) * 2], in[((2 * b + i / 3) * 3 + i % 3) * 2 + 1]};
 #pragma unroll
   for (int i = 0; i < 6; i++) y[i] = rmul(blk[i], x[i]);
+#pragma unroll
+  for (int i = 1; i < 6; i++) {
+#pragma unroll
+    for (int j = 0; j < i; j++) {
+      int od = i * (i - 1) / 2 + j;
+      cx<T> a = {blk[6 + 2 * od], blk[6 + 2 * od + 1]};
+      y[i] = cmad(a, x[j], y[i]);
+      y[j] = cmadc(a, x[i], y[j]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    out[((2 * b + i / 3) * 3 + i % 3) * 2] = y[i].re;
+    out[((2 * b + i / 3) * 3 + i % 3) * 2 + 1] = y[i].im;
+  }
+}
+
+// out_block += A_b in_block (packed Hermitian block as in herm6_apply)
+template <typename T>
+__device__ __forceinline__ void herm6_acc(const T *blk, const T *in, T *out, int b)
+{
+  cx<T> x[6], y[6];
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    const int k = ((2 * b + i / 3) * 3 + i % 3) * 2;
+    x[i] = {in[k], in[k + 1]};
+    y[i] = {mad(blk[i], x[i].re, out[k]), mad(blk[i], x[i].im, out[k + 1])};
+  }
 #pragma unroll
   for (int i = 1; i < 6; i++) {
 #pragma unroll
@@ -512,6 +555,24 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
             }
           }
         }
+      } else if (EPI == EPI_NDFCLOV) {
+        if constexpr (R == 2) {
+#pragma unroll
+          for (int b = 0; b < 2; b++) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+              T rows[24];
+              L::template load_clover<144>(a.clov, s, 72 * b + 24 * j, 24, rows);
+              full6_rows(rows, acc[0], res[0], b, j);
+              L::template load_clover<144>(a.clov2, s, 72 * b + 24 * j, 24, rows);
+              full6_rows(rows, acc[1], res[1], b, j);
+            }
+            T blk[36];
+            L::template load_clover<72>(a.clov3, s, 36 * b, 36, blk);
+            herm6_acc(blk, acc[1], res[0], b);  // up += C down
+            herm6_acc(blk, acc[0], res[1], b);  // down += C up
+          }
+        }
       } else {  // EPI_TMINV: mu_inv (1 - i mu isign g5) acc
         const T m = splat<T>(a.mu * ISIGN), mi = splat<T>(a.mu_inv);
 #pragma unroll
@@ -578,6 +639,30 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
               }
             }
           }
+        }
+      } else if (ACHI == ACHI_NDCLOV) {
+        if constexpr (R == 2) {
+#pragma unroll
+          for (int b = 0; b < 2; b++) {
+            T blk[36];
+            L::template load_clover<72>(a.clov, s, 36 * b, 36, blk);
+#pragma unroll
+            for (int r = 0; r < 2; r++) herm6_apply(blk, chi[r], res[r], b);
+          }
+          const T rh = splat<T>(a.rho * ISIGN), ne = splat<T>(-a.eps);
+#pragma unroll
+          for (int f = 0; f < 2; f++)
+#pragma unroll
+            for (int sp = 0; sp < 4; sp++) {
+              const T rr = ((sp < 2) == (f == 0)) ? rh : -rh;  // s_f g5 isign rho
+#pragma unroll
+              for (int c = 0; c < 3; c++) {
+                const int k = (sp * 3 + c) * 2;
+                res[f][k] = mad(ne, chi[1 - f][k], mad(nbeta, acc[f][k], mad(-rr, chi[f][k + 1], res[f][k])));
+                res[f][k + 1] =
+                    mad(ne, chi[1 - f][k + 1], mad(nbeta, acc[f][k + 1], mad(rr, chi[f][k], res[f][k + 1])));
+              }
+            }
         }
       } else {  // ACHI_TM: alpha (1 + i mu isign g5) chi - beta acc
         const T al = splat<T>(a.alpha), m = splat<T>(a.mu * ISIGN);

@@ -177,7 +177,8 @@ void launch_mshift(int prec, const MShiftArgs &a, dim3 grid, cudaStream_t st);
 void launch_clover_build(int recon, int prec_out, Geom geo, GaugeArg g, void *out, long long stride, int vpc, int cb,
                          double diag_mass, double cr, double ct, dim3 grid, cudaStream_t st);
 void launch_clover_invert(int prec_in, int prec_out, Geom geo, const void *in, long long stride, int vpc_in, void *o0,
-                          void *o1, int vpc_out, int mode, double mu, dim3 grid, cudaStream_t st);
+                          void *o1, int vpc_out, int mode, double mu, dim3 grid, cudaStream_t st, void *o2 = nullptr,
+                          int vpc_out2 = 0, double eps = 0.0);
 void launch_clover_convert(int prec_in, int prec_out, Geom geo, const void *in, int vpc_in, void *out, int vpc_out,
                            long long stride, int nr, dim3 grid, cudaStream_t st);
 

@@ -319,6 +319,18 @@ def twisted_full_inverse(packed, mu):
     return res
 
 
+def ndtm_clover_inverses(packed, mu, eps):
+    """Inverse of the two-flavour block [[A + i mu g5, -eps], [-eps, A - i mu g5]]:
+    (Q (A - i mu g5), Q (A + i mu g5)) as full 6x6 blocks and eps Q packed,
+    Q = (A^2 + mu^2 - eps^2)^-1 (g5 = +1 on block 0, -1 on block 1)."""
+    a = packed_to_blocks(packed)
+    eye = np.eye(6)
+    q = np.linalg.inv(a @ a + (mu * mu - eps * eps) * eye)
+    g5 = np.array([1.0, -1.0])[:, None, None]
+    qa = q @ a
+    return qa - 1j * mu * g5 * q, qa + 1j * mu * g5 * q, blocks_to_packed(eps * q)
+
+
 def full_from_packed(packed):
     return packed_to_blocks(packed)
 

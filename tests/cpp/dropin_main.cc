@@ -17,6 +17,7 @@
 #include "qphix/invcg.h"
 #include "qphix/minvcg.h"
 #include "qphix/ndtm_reuse_operator.h"
+#include "qphix/ndtm_reuse_operator_clover.h"
 #include "qphix/unprec_solver_wrapper.h"
 #include "qphix/wilson.h"
 
@@ -154,6 +155,30 @@ int main(int argc, char **argv)
     ncg(nres, nin, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
     write_from("out_ndcg_up", nres[0], sbytes);
     write_from("out_ndcg_dn", nres[1], sbytes);
+
+    // 7b. two-flavour twisted-mass clover: clov = A_odd, the caller's
+    // two-flavour inverses of the even block, operator and InvCG on the pair
+    {
+      size_t cbytes = F.cbytes;
+      size_t fbytes = (size_t)(geom.getPxyz() * geom.Nt() * 2 / 4) * sizeof(Geometry<double, 4, 2, true>::FullCloverBlock);
+      auto *odiag = geom.allocCBClov();
+      Geometry<double, 4, 2, true>::FullCloverBlock *finv[2] = {geom.allocCBFullClov(), geom.allocCBFullClov()};
+      read_into("d_ndc_odiag", odiag, cbytes);
+      read_into("d_ndc_fup", finv[0], fbytes);
+      read_into("d_ndc_fdn", finv[1], fbytes);
+      EvenOddNDTMCloverReuseOperator<double, 4, 2, true> NC(nd[1], nd[2], F.u, F.A_odd, odiag, finv, &geom, -1.0,
+                                                            1.0, 1.0);
+      NC(nres, nin, 1, 1);
+      write_from("out_ndc_up", nres[0], sbytes);
+      write_from("out_ndc_dn", nres[1], sbytes);
+      InvCG<double, 4, 2, true, EvenOddNDTMCloverReuseOperator<double, 4, 2, true>> nccg(NC, 2000);
+      nccg(nres, nin, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
+      write_from("out_ndccg_up", nres[0], sbytes);
+      write_from("out_ndccg_dn", nres[1], sbytes);
+      geom.free(odiag);
+      geom.free(finv[0]);
+      geom.free(finv[1]);
+    }
     geom.free(nres[0]);
     geom.free(nres[1]);
     geom.free(chi);

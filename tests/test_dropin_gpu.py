@@ -4,7 +4,8 @@ the library, fed QPhiX-layout host arrays (Geometry<double,4,2,true> with
 padding, and Geometry<float,8,2,true> for the inner solver of
 InvRichardsonMultiPrec) packed from seeded fields, and its outputs -- a
 Dslash, the clover operator, BiCGStab, CG, Richardson and multishift-CG
-solves, the two-flavour twisted-mass operator and its CG solve -- are
+solves, the two-flavour twisted-mass Wilson and clover operators and their
+CG solves -- are
 checked against the CPU oracle.  An UnprecSolverWrapper solve of the full
 (unpreconditioned) clover system is checked through its full residual."""
 import os
@@ -43,8 +44,12 @@ def test_cpp_dropin(tmp_path, oracle):
     lay.pack_spinor(psi)[1:].tofile(d / "d_psi")  # block 0 = what allocCBFourSpinor returns
     chi = F.gaussian_spinor(dims, 33)
     lay.pack_spinor(chi)[1:].tofile(d / "d_chi")
-    nd = (s["mass"], 0.3, 0.2)  # mass, mu, epsilon of the two-flavour operator
+    nd = (s["mass"], 0.3, 0.2)  # mass, mu, epsilon of the two-flavour operators
     np.array(nd, dtype=np.float64).tofile(d / "ndtm")
+    ndc_fu, ndc_fd, ndc_c = F.ndtm_clover_inverses(s["clov"][0], nd[1], nd[2])
+    lay.pack_clover(ndc_c).tofile(d / "d_ndc_odiag")
+    lay.pack_full_clover(ndc_fu).tofile(d / "d_ndc_fup")
+    lay.pack_full_clover(ndc_fd).tofile(d / "d_ndc_fdn")
     out = subprocess.run([str(exe), str(d)], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr + out.stdout
 
@@ -78,6 +83,13 @@ def test_cpp_dropin(tmp_path, oracle):
     assert rel_l2(got, N.apply(pair, 1, 1)) < 1e-13
     xn = np.stack([load("out_ndcg_up"), load("out_ndcg_dn")])
     r = pair - N.apply(N.apply(xn, 1), -1)
+    assert np.linalg.norm(r) / np.linalg.norm(pair) < 2e-10
+    NC = oracle.OracleOp("ndtmclover", L, s["gauge"], clov=s["clov"][1], invclov=ndc_c, finv=(ndc_fu, ndc_fd),
+                         twisted_mass=nd[1], epsilon=nd[2])
+    got = np.stack([load("out_ndc_up"), load("out_ndc_dn")])
+    assert rel_l2(got, NC.apply(pair, 1, 1)) < 1e-13
+    xn = np.stack([load("out_ndccg_up"), load("out_ndccg_dn")])
+    r = pair - NC.apply(NC.apply(xn, 1), -1)
     assert np.linalg.norm(r) / np.linalg.norm(pair) < 2e-10
     # unpreconditioned clover system: [[A_ee, -D_eo/2], [-D_oe/2, A_oo]] x = (chi, psi)
     xe, xo = load("out_unprec_e"), load("out_unprec_o")

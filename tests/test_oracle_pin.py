@@ -194,3 +194,57 @@ def test_ndtm_oracle_structure(oracle):
     a = np.vdot(y, op.apply(x, 1))
     b = np.vdot(op.apply(y, -1), x)
     assert abs(a - b) / abs(a) < 1e-13
+
+
+def test_ndtm_clover_inverses_invert_the_block():
+    """The two-flavour inverse clover fields (ndtm_reuse_operator_clover.h:38-50,
+    tm_clov_dslash_def.h:96-104) invert [[A + i mu g5, -eps], [-eps, A - i mu g5]]
+    on every site and chirality block."""
+    from qphix_b200 import fields as F
+    dims = (4, 4, 4, 8)
+    g = F.make_gauge(dims, 5, kind="weak")
+    A = F.make_clover(dims, g, 0.1, 1.2)[0]
+    mu, eps = 0.3, 0.2
+    fu, fd, c = F.ndtm_clover_inverses(A, mu, eps)
+    a = F.packed_to_blocks(A)
+    q = F.packed_to_blocks(c)
+    eye = np.eye(6)
+    for b, g5 in ((0, 1.0), (1, -1.0)):
+        B = np.block([[a[:, b] + 1j * mu * g5 * eye, -eps * np.broadcast_to(eye, a[:, b].shape)],
+                      [-eps * np.broadcast_to(eye, a[:, b].shape), a[:, b] - 1j * mu * g5 * eye]])
+        Binv = np.block([[fu[:, b], q[:, b]], [q[:, b], fd[:, b]]])
+        assert np.abs(B @ Binv - np.eye(12)).max() < 1e-12
+
+
+def test_ndtm_clover_oracle_structure(oracle):
+    """The two-flavour twisted-mass clover operator of the oracle
+    (ndtm_reuse_operator_clover.h:117-128): with epsilon = 0 it is the
+    twisted-mass clover operator with rho = +mu, (A +/- i mu g5)^-1 on the up
+    and rho = -mu with the inverses swapped on the down flavour (the check of
+    the reference's tests/testNDTMvsTMCloverFull.cc), and its isign = -1
+    application is its adjoint."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(__file__)))
+    from helpers import make_setup, rel_l2
+    from qphix_b200 import fields as F
+    dims = (4, 4, 4, 8)
+    s = make_setup(dims, seed=23, gauge_kind="weak", mass=0.1, mu=0.1)
+    L = oracle.make_lattice(dims, -1.0)
+    A = s["clov"]
+    mu = 0.3
+    x = np.stack([F.gaussian_spinor(dims, 1), F.gaussian_spinor(dims, 2)])
+    y = np.stack([F.gaussian_spinor(dims, 3), F.gaussian_spinor(dims, 4)])
+    fu, fd, c = F.ndtm_clover_inverses(A[0], mu, 0.0)
+    op0 = oracle.OracleOp("ndtmclover", L, s["gauge"], clov=A[1], invclov=c, finv=(fu, fd), twisted_mass=mu)
+    up = oracle.OracleOp("tmclover", L, s["gauge"], clov=A[1], finv=F.twisted_full_inverse(A[0], mu), rho=mu)
+    dn = oracle.OracleOp("tmclover", L, s["gauge"], clov=A[1], finv=F.twisted_full_inverse(A[0], -mu), rho=-mu)
+    for isign in (1, -1):
+        r = op0.apply(x, isign)
+        assert rel_l2(r[0], up.apply(x[0], isign)) < 1e-13
+        assert rel_l2(r[1], dn.apply(x[1], isign)) < 1e-13
+    fu, fd, c = F.ndtm_clover_inverses(A[0], mu, 0.2)
+    op = oracle.OracleOp("ndtmclover", L, s["gauge"], clov=A[1], invclov=c, finv=(fu, fd), twisted_mass=mu,
+                         epsilon=0.2)
+    a = np.vdot(y, op.apply(x, 1))
+    b = np.vdot(op.apply(y, -1), x)
+    assert abs(a - b) / abs(a) < 1e-13
