@@ -3,8 +3,10 @@
 //
 // Every reducing kernel computes up to QPX_MAX_RED doubles per right-hand
 // side per thread, reduces them over the block (warp shuffles, then a fixed
-// order over warps), writes one partial per (block, rhs, value), and the last
-// block to finish (atomic ticket) sums the partials in block order and runs a
+// order over warps, one barrier for all values), writes one partial per
+// (block, rhs, value), and the last block to finish (atomic ticket) folds the
+// partials -- warp w takes values w, w + 4, ...; lane l adds site blocks
+// l, l + 32, ... in order, then the warp's shuffle tree -- and runs a
 // finalize step on thread 0.  The order of every addition is fixed by the
 // launch shape, so results are bitwise reproducible run to run.
 //
@@ -106,23 +108,37 @@ __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, SolverState
                                                 int slots, const double val[R][QPX_MAX_RED], int sblock = -1,
                                                 int nsblocks = -1)
 {
-  __shared__ double smem[32];
+  constexpr int NW = QPX_BLOCK / 32;  // launches of these kernels use QPX_BLOCK threads
+  __shared__ double wpart[NW][R * QPX_MAX_RED];
   __shared__ bool am_last;
   if (sblock < 0) {
     sblock = blockIdx.x;
     nsblocks = gridDim.x;
   }
   const long long nblocks = (long long)gridDim.x * gridDim.y;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  // every live value's warp sum, then one barrier and a fixed-order sum over warps
 #pragma unroll
-  for (int r = 0; r < R; r++) {
-    int o = 0;
+  for (int r = 0; r < R; r++)
 #pragma unroll
-    for (int k = 0; k < QPX_MAX_RED; k++) {
+    for (int k = 0; k < QPX_MAX_RED; k++)
       if (slots & (1 << k)) {
-        double s = block_sum(val[r][k], smem);
-        if (threadIdx.x == 0 && rhs0 + r < nrhs)
-          ra.partials[((long long)sblock * nrhs + rhs0 + r) * ra.nval + o] = s;
-        o++;
+        const double s = warp_sum(val[r][k]);
+        if (lane == 0) wpart[wid][r * QPX_MAX_RED + k] = s;
+      }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+      int o = 0;
+#pragma unroll
+      for (int k = 0; k < QPX_MAX_RED; k++) {
+        if (slots & (1 << k)) {
+          double s = 0.0;
+          for (int w = 0; w < NW; w++) s += wpart[w][r * QPX_MAX_RED + k];
+          if (rhs0 + r < nrhs) ra.partials[((long long)sblock * nrhs + rhs0 + r) * ra.nval + o] = s;
+          o++;
+        }
       }
     }
   }
@@ -135,15 +151,18 @@ __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, SolverState
   __syncthreads();
   if (!am_last) return;
   __threadfence();
-  // last block: fold the partials of every site block, in block order
+  // last block: fold the partials of every site block, the values spread
+  // over the warps so that their loads are in flight together
   const int gx = nsblocks;
-  for (int idx = 0; idx < nrhs * ra.nval; idx++) {
+  const long long row = (long long)nrhs * ra.nval;
+  for (int idx = wid; idx < nrhs * ra.nval; idx += NW) {
     double acc = 0;
-    for (int b = threadIdx.x; b < gx; b += blockDim.x)
-      acc += __ldcg(ra.partials + (long long)b * nrhs * ra.nval + idx);
-    double s = block_sum(acc, smem);
-    if (threadIdx.x == 0) ra.result[idx] = s;
+#pragma unroll 4
+    for (int b = lane; b < gx; b += 32) acc += __ldcg(ra.partials + b * row + idx);
+    acc = warp_sum(acc);
+    if (lane == 0) ra.result[idx] = acc;
   }
+  __syncthreads();
   if (threadIdx.x == 0) {
     *ra.ticket = 0u;
     __threadfence();
