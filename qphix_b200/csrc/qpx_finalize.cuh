@@ -137,18 +137,25 @@ __device__ inline void finalize(int fin, SolverState *st, const double *res, int
     end_iteration(st, nrhs);
     break;
   // ---- BiCGStab with reliable updates ---------------------------------------
-  // As FIN_BICG_RX, but a right-hand side whose iterated residual fell below
-  // its update threshold (S_AUX1, delta^2 |r_true|^2 at the last update) or
-  // its target asks the host for a reliable update instead of stopping:
+  // As FIN_BICG_RX, but instead of stopping, right-hand sides whose iterated
+  // residual fell below their update threshold (S_AUX1, delta^2 |r_true|^2 at
+  // the last update) or their target ask the host for a reliable update:
   // st->status = 3 and the iteration graph stops (done) until the host has
-  // replaced r by the recomputed true residual.
+  // replaced r by the recomputed true residual.  One update serves every
+  // right-hand side of the batch, so it is asked for once half of the active
+  // ones have crossed, or as soon as one has fallen ten times below its
+  // threshold (before the low-precision recurrence drifts from the true
+  // residual); with one or two right-hand sides that is any crossing.
   case FIN_BICG_RU: {
     bool request = false;
+    int active = 0, crossed = 0;
     for (int r = 0; r < nrhs; r++) {
       if (st->rhs_done[r]) continue;
+      active++;
       double rn = res[r * nval];
       v[S_RNORM][r] = rn;
-      if (rn < v[S_AUX1][r] || rn < v[S_RSD][r]) request = true;
+      if (rn < v[S_AUX1][r] || rn < v[S_RSD][r]) crossed++;
+      if (rn < 0.1 * v[S_AUX1][r]) request = true;
       double rr = res[r * nval + 1], ri = res[r * nval + 2];
       if (rr == 0.0 && ri == 0.0) {
         request = true;  // let the true residual decide
@@ -163,6 +170,7 @@ __device__ inline void finalize(int fin, SolverState *st, const double *res, int
       v[S_BETA_IM][r] = t1r * t2i + t1i * t2r;
     }
     end_iteration(st, nrhs);
+    if (2 * crossed >= active && crossed > 0) request = true;
     if (request) {
       st->done = 1;
       st->status = 3;
