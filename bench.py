@@ -5,11 +5,14 @@ Workload (one step = one batched solve): even-odd preconditioned Wilson-clover
 operator on a 16^3x32 lattice, kappa = 0.1360 (bare mass 1/(2 kappa) - 4),
 c_sw = 1.0, links exp(i 0.3 H) with H drawn from the Gaussian unitary
 ensemble (stored 12-real), antiperiodic in t.  `--batch` right-hand sides are
-solved together to a 1e-10 relative true (FP64) residual by BiCGStab with
-reliable updates (iterations on FP16-storage / FP32-arithmetic fields, FP64
-solution and true residual; `--solver richardson` selects QPhiX's
-InvRichardsonMultiPrec instead, and the other one is timed beside it).  The
-plain FP64 BiCGStab solve of the same system is timed as well.
+solved together to a 1e-10 relative true (FP64) residual by QPhiX's
+mixed-precision scheme, InvRichardsonMultiPrec: FP64 outer defect correction
+(solution and true residual in FP64), inner BiCGStab on FP16-storage /
+FP32-arithmetic fields reducing each correction's residual by delta = 0.005.
+`--solver ru` selects BiCGStab with reliable updates (delta 0.03) instead;
+the other solver, and the default solver with a Q16 inner operator, are timed
+beside it.  The plain FP64 BiCGStab solve of the same system is timed as
+well.
 
 value  = solves/s with the right-hand sides resident in HBM
 e2e    = solves/s through the C ABI with host buffers: pinned host -> device
@@ -42,7 +45,10 @@ CSW = 1.0
 EPS = 0.3
 DIMS = (16, 16, 16, 32)
 RSD = 1e-10
-DELTA = 0.1
+# measured on this workload (8 rhs, FP16 inner): Richardson 0.003-0.01 all
+# reach 1e-10 in 6 corrections, 0.005 with the fewest inner iterations;
+# reliable-update BiCGStab is fastest at 0.03
+DEFAULT_DELTA = {"richardson": 0.005, "ru": 0.03}
 
 
 def parse():
@@ -56,10 +62,15 @@ def parse():
     ap.add_argument("--inner-recon", type=int, default=12, choices=[12, 18],
                     help="link storage of the inner operator (12- or 18-real)")
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--solver", default="ru", choices=["ru", "richardson"],
+    ap.add_argument("--solver", default="richardson", choices=["ru", "richardson"],
                     help="ru: BiCGStab with reliable updates; richardson: InvRichardsonMultiPrec")
-    ap.add_argument("--delta", type=float, default=0.03)
-    return ap.parse_args()
+    ap.add_argument("--delta", type=float, default=None,
+                    help="residual reduction per correction / reliable update (default: richardson "
+                         f"{DEFAULT_DELTA['richardson']}, ru {DEFAULT_DELTA['ru']})")
+    args = ap.parse_args()
+    if args.delta is None:
+        args.delta = DEFAULT_DELTA[args.solver]
+    return args
 
 
 # ---------------------------------------------------------------------------
@@ -168,7 +179,11 @@ def run_reference(args, rank, world):
     v = statistics.median([x["value"] for x in vals])
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "data": "synthetic", "config": config_dict(1, "f64"),
+            "data": "synthetic", "config": config_dict(args.batch, args.inner, args.solver, args.inner_recon,
+                                                        args.delta),
+            "reference_path": "the same system solved by FP64 clover BiCGStab on the CPU (oracle port of "
+                              "include/qphix/invbicgstab.h), one rhs at a time; a bounded sample of "
+                              "iterations scaled to a full solve",
             "cpu_baseline": {"value": v, "unit": "solves/s", "cores": vals[-1]["cores"], "kind": "port",
                              "sample": vals[-1]["sample"]},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -178,10 +193,11 @@ def run_reference(args, rank, world):
 METRIC = "Clover solves/s @1e-10 mixed vs FP64 plain, 1 B200; Dslash HBM GB/s; p99 ms"
 
 
-def config_dict(batch, inner, solver="ru", inner_recon=12):
+def config_dict(batch, inner, solver="richardson", inner_recon=12, delta=None):
     how = ("BiCGStab with reliable updates (FP64 true residual / solution, iterations in "
-           f"{inner} storage ({inner_recon}-real links) + FP32 arithmetic)" if solver == "ru" else
-           f"InvRichardsonMultiPrec (FP64 outer, BiCGStab inner in {inner} storage + FP32 arithmetic)")
+           f"{inner} storage ({inner_recon}-real links) + FP32 arithmetic, delta {delta})" if solver == "ru" else
+           f"InvRichardsonMultiPrec (FP64 outer defect correction, BiCGStab inner in {inner} storage "
+           f"({inner_recon}-real links) + FP32 arithmetic, delta {delta})")
     return {"workload": ("clover even-odd 16^3x32, kappa=0.1360, csw=1.0, links exp(i 0.3 H) "
                          f"(H GUE) 12-real, antiperiodic t; {how} to 1e-10 true residual"),
             "rhs_per_step": batch, "lattice": list(DIMS), "kappa": KAPPA, "csw": CSW,
@@ -224,9 +240,10 @@ def main():
     Ai = lat.clover(args.inner).upload(inputs["clov_odd"])
     Aii = lat.clover(args.inner).upload(inputs["invclov_even"])
     Mi = api.EvenOddCloverOperator(ui, Ai, Aii)
-    rich = api.InvRichardsonMultiPrec(M64, Mi, "bicgstab", delta=args.delta, max_iters=100,
-                                      inner_max_iters=5000)
-    ru = api.InvBiCGStabMixed(M64, Mi, delta=args.delta, max_iters=20000)
+    d_rich = args.delta if args.solver == "richardson" else DEFAULT_DELTA["richardson"]
+    d_ru = args.delta if args.solver == "ru" else DEFAULT_DELTA["ru"]
+    rich = api.InvRichardsonMultiPrec(M64, Mi, "bicgstab", delta=d_rich, max_iters=100, inner_max_iters=5000)
+    ru = api.InvBiCGStabMixed(M64, Mi, delta=d_ru, max_iters=20000)
     solver = ru if args.solver == "ru" else rich
     b_res = lat.spinor("f64", B).upload(inputs["rhs"])    # resident sources
     b = lat.spinor("f64", B)
@@ -330,9 +347,36 @@ def main():
         torch.cuda.synchronize()
         ots.append(e0.elapsed_time(e1))
     other_line = {"solver": "richardson" if args.solver == "ru" else "ru",
+                  "delta": d_rich if args.solver == "ru" else d_ru,
                   "solves_per_s": round(B * 1e3 / min(ots), 3),
                   "worst_true_rel_resid": max(i["true_rel_resid"] for i in oinf),
                   "iters": oinf[0]["n_iters"], "mv_apps": oinf[0]["mv_apps"]}
+
+    # ---- the same solver with a Q16 inner operator (16-bit fixed-point spinors
+    # with per-site norms, FP16 links and clover) ---------------------------------
+    q16_line = None
+    if args.inner != "q16":
+        uq = lat.gauge("q16", args.inner_recon).upload(inputs["gauge"])
+        Aq = lat.clover("q16").upload(inputs["clov_odd"])
+        Aiq = lat.clover("q16").upload(inputs["invclov_even"])
+        Mq = api.EvenOddCloverOperator(uq, Aq, Aiq)
+        sq = (api.InvRichardsonMultiPrec(M64, Mq, "bicgstab", delta=d_rich, max_iters=100, inner_max_iters=5000)
+              if args.solver == "richardson" else api.InvBiCGStabMixed(M64, Mq, delta=d_ru, max_iters=20000))
+        qts = []
+        for _ in range(3):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            api.copy(b, b_res)
+            api.zero(x)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            qinf = sq(x, b, RSD)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            qts.append(e0.elapsed_time(e1))
+        q16_line = {"inner": "q16", "solver": args.solver, "solves_per_s": round(B * 1e3 / min(qts[1:]), 3),
+                    "worst_true_rel_resid": max(i["true_rel_resid"] for i in qinf),
+                    "iters": qinf[0]["n_iters"], "mv_apps": qinf[0]["mv_apps"]}
 
     # ---- plain FP64 BiCGStab beside it ------------------------------------------
     fp64 = None
@@ -430,7 +474,7 @@ def main():
             "ms_per_step": round(total_s * 1e3 / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": f"mixed: f64 outer, f32 arithmetic on {args.inner} storage inner",
-            "data": "synthetic (seeded)", "config": config_dict(B, args.inner, args.solver, args.inner_recon),
+            "data": "synthetic (seeded)", "config": config_dict(B, args.inner, args.solver, args.inner_recon, args.delta),
             "e2e": {"value": round(e2e_value, 3), "unit": "solves/s", "h2d_bytes_per_step": bytes_io,
                     "d2h_bytes_per_step": bytes_io},
             "roofline": roof, "roofline_large_lattice": roof_big,
@@ -443,6 +487,9 @@ def main():
                        "delta": args.delta, "iters": outer_iters, "mv_apps": mv_apps,
                        "worst_true_rel_resid": worst_resid, "all_converged": converged},
             "other_mixed_solver": other_line,
+            "q16_inner": q16_line,
+            "q16_inner_vs_fp64_solves_ratio": (round(q16_line["solves_per_s"] / fp64["solves_per_s"], 3)
+                                               if (fp64 and q16_line) else None),
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
