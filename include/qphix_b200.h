@@ -337,12 +337,15 @@ int qphix_gpu_blas_norm2_noalloc(qphix_gpu_field x, double *out_dev);
  * x must stay valid until qphix_gpu_server_wait returns. */
 typedef struct qphix_gpu_server_s *qphix_gpu_server;
 
+enum { QPHIX_GPU_SERVE_RELIABLE_UPDATE = 0, QPHIX_GPU_SERVE_RICHARDSON = 1 };
 typedef struct {
   size_t hbm_budget_bytes;
   int slots;       /* requests in flight at once, 1 .. 64 */
-  int low_prec;    /* QPHIX_GPU_F32 / _F16 / _BF16 */
+  int low_prec;    /* QPHIX_GPU_F32 / _F16 / _BF16 / _Q16 / _Q16F32 */
   int max_bypass;
-  double delta;    /* reliable-update threshold, (0, 1) */
+  double delta;    /* reliable-update threshold / residual reduction per correction, (0, 1) */
+  int solver;      /* QPHIX_GPU_SERVE_RELIABLE_UPDATE (BiCGStab with reliable updates) or
+                      QPHIX_GPU_SERVE_RICHARDSON (InvRichardsonMultiPrec, BiCGStab inner) */
 } qphix_gpu_server_config;
 
 typedef struct {

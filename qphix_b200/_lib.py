@@ -39,7 +39,7 @@ class SolveInfo(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("slots", C.c_int), ("low_prec", C.c_int),
-                ("max_bypass", C.c_int), ("delta", C.c_double)]
+                ("max_bypass", C.c_int), ("delta", C.c_double), ("solver", C.c_int)]
 
 
 class Request(C.Structure):

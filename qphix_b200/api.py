@@ -742,10 +742,14 @@ class Server:
     admitted against an HBM budget; results are the FP64 solutions of
     M x = b on the odd checkerboard."""
 
-    def __init__(self, hbm_budget_bytes, slots=4, low_prec="f16", max_bypass=4, delta=0.1, device=0):
+    SOLVERS = {"ru": 0, "richardson": 1}
+
+    def __init__(self, hbm_budget_bytes, slots=4, low_prec="f16", max_bypass=4, delta=0.1, device=0,
+                 solver="ru"):
         lib()
         check(L._lib.qphix_gpu_init(device))
-        cfg = L.ServerConfig(int(hbm_budget_bytes), int(slots), PREC[low_prec], int(max_bypass), float(delta))
+        cfg = L.ServerConfig(int(hbm_budget_bytes), int(slots), PREC[low_prec], int(max_bypass), float(delta),
+                             self.SOLVERS[solver])
         h = C.c_void_p()
         check(L._lib.qphix_gpu_server_create(C.byref(cfg), C.byref(h)))
         self.h = h

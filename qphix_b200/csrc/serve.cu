@@ -101,9 +101,13 @@ size_t request_bytes(const qphix_gpu_server_s *S, const Ensemble &e, const qphix
   const long long vh = (long long)e.dims[0] / 2 * e.dims[1] * e.dims[2] * e.dims[3];
   const long long stride = (vh + 63) / 64 * 64;
   const int lp = S->cfg.low_prec, nr = r.nrhs;
-  // x, b, two solver temporaries, the operator temporary (FP64); six solver
-  // temporaries and the operator temporary (low precision)
-  size_t b = 5 * spinor_bytes(PREC_F64, stride, nr) + 7 * spinor_bytes(lp, stride, nr);
+  // reliable updates: x, b, two solver temporaries, the operator temporary
+  // (FP64); six solver temporaries and the operator temporary (low precision).
+  // Richardson: x, b, three outer temporaries, the operator temporary (FP64);
+  // two correction fields, five BiCGStab temporaries and the operator
+  // temporary (low precision)
+  const bool rich = S->cfg.solver == QPHIX_GPU_SERVE_RICHARDSON;
+  size_t b = (rich ? 6 : 5) * spinor_bytes(PREC_F64, stride, nr) + (rich ? 8 : 7) * spinor_bytes(lp, stride, nr);
   b += (size_t)nr * vh * 24 * sizeof(double);  // host-layout staging
   if (r.op_kind == QPHIX_GPU_CLOVER_OP)
     b += 3 * clover_bytes(PREC_F64, stride, 72) + 2 * clover_bytes(lp, stride, 72);
@@ -216,8 +220,12 @@ struct Worker {
       F.ops.push_back(op64);
       ok(qphix_gpu_eo_op_create(&p, e.glow, cl, il, f0l, f1l, &opl));
       F.ops.push_back(opl);
-      ok(qphix_gpu_solve_bicgstab_mixed(op64, opl, x, b, r.rsd_target, S->cfg.delta, r.max_iters, 1, 1,
-                                        info.data()));
+      if (S->cfg.solver == QPHIX_GPU_SERVE_RICHARDSON)
+        ok(qphix_gpu_solve_richardson(op64, opl, QPHIX_GPU_SOLVER_BICGSTAB, x, b, r.rsd_target, S->cfg.delta, 100,
+                                      r.max_iters, 1, 1, info.data()));
+      else
+        ok(qphix_gpu_solve_bicgstab_mixed(op64, opl, x, b, r.rsd_target, S->cfg.delta, r.max_iters, 1, 1,
+                                          info.data()));
       ok(qphix_gpu_field_download(x, r.x, &hl, -1));
     } catch (...) {
       lattice_trim(L);
@@ -341,6 +349,8 @@ extern "C" int qphix_gpu_server_create(const qphix_gpu_server_config *cfg, qphix
         cfg->low_prec != PREC_Q16 && cfg->low_prec != PREC_Q16F32)
       throw Error(QPHIX_GPU_EINVAL, "low_prec must be F32, F16, BF16, Q16 or Q16F32");
     if (!(cfg->delta > 0.0 && cfg->delta < 1.0)) throw Error(QPHIX_GPU_EINVAL, "delta must be in (0, 1)");
+    if (cfg->solver != QPHIX_GPU_SERVE_RELIABLE_UPDATE && cfg->solver != QPHIX_GPU_SERVE_RICHARDSON)
+      throw Error(QPHIX_GPU_EINVAL, "solver must be QPHIX_GPU_SERVE_RELIABLE_UPDATE or _RICHARDSON");
     S = new qphix_gpu_server_s();
     S->cfg = *cfg;
     if (S->cfg.max_bypass < 0) S->cfg.max_bypass = 0;

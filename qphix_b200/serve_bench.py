@@ -52,6 +52,9 @@ def main(argv=None):
     ap.add_argument("--calibrate", type=int, default=48)
     ap.add_argument("--seed", type=int, default=2025)
     ap.add_argument("--volumes", type=int, default=4, help="use the first N volumes of the list (quick runs)")
+    ap.add_argument("--solver", default="ru", choices=["ru", "richardson"],
+                    help="ru: BiCGStab with reliable updates (delta 0.1); richardson: InvRichardsonMultiPrec "
+                         "(delta 0.005)")
     args = ap.parse_args(argv)
     vols = VOLUMES[:args.volumes]
 
@@ -59,7 +62,8 @@ def main(argv=None):
     from . import fields as F
 
     t0 = time.perf_counter()
-    srv = api.Server(int(args.budget_gb * (1 << 30)), slots=args.slots, low_prec="f16")
+    srv = api.Server(int(args.budget_gb * (1 << 30)), slots=args.slots, low_prec="f16", solver=args.solver,
+                     delta=0.005 if args.solver == "richardson" else 0.1)
     ens = {}
     sources = {}
     for v, dims in enumerate(vols):
@@ -159,6 +163,7 @@ def main(argv=None):
         "worst_true_rel_resid": max(r["true_rel_resid"] for r in results),
         "server": st, "setup_s": setup_s,
         "data": "synthetic (seeded)",
+        "solver": args.solver,
     }
     print(json.dumps(line), flush=True)
 

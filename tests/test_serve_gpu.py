@@ -58,8 +58,8 @@ def _oracle_op(oracle, dims, gauge, kind, mass):
                            rho=MU)
 
 
-def _serve(api, gauges, reqs, slots, budget=8 << 30):
-    srv = api.Server(budget, slots=slots, low_prec="f16")
+def _serve(api, gauges, reqs, slots, budget=8 << 30, **kw):
+    srv = api.Server(budget, slots=slots, low_prec="f16", **kw)
     ens = {d: srv.add_ensemble(d, g) for d, g in gauges.items()}
     results = []
     if slots == 1:
@@ -87,6 +87,21 @@ def test_serve_results_match_oracle(api, oracle, gauges):
             r = b[k] - op.apply(x[k], 1, 1)
             assert np.linalg.norm(r) / np.linalg.norm(b[k]) < 1e-9, (kind, k)
         assert info["latency_s"] >= info["solve_s"] > 0
+
+
+def test_serve_richardson_matches_oracle(api, oracle, gauges):
+    """The server with the InvRichardsonMultiPrec solver (FP64 defect
+    correction, BiCGStab inner on the low-precision operator)."""
+    reqs = _requests()
+    results, stats = _serve(api, gauges, reqs, slots=3, solver="richardson", delta=0.005)
+    assert stats["completed"] == len(reqs) and stats["failed"] == 0
+    for (d, kind, kappa, nrhs, seed), (x, info) in zip(reqs, results):
+        assert info["status"] == 0 and info["true_rel_resid"] < 1e-10, (kind, info)
+        op = _oracle_op(oracle, d, gauges[d], kind, F.kappa_to_mass(kappa))
+        b = _rhs(d, nrhs, seed)
+        for k in range(nrhs):
+            r = b[k] - op.apply(x[k], 1, 1)
+            assert np.linalg.norm(r) / np.linalg.norm(b[k]) < 1e-9, (kind, k)
 
 
 def test_serve_same_alone_and_in_mix(api, gauges):
