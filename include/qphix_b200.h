@@ -207,6 +207,38 @@ int qphix_gpu_dslash_two_flav_clover(const qphix_gpu_op_params *p, qphix_gpu_fie
                                      qphix_gpu_field clov_odiag, int isign, int cb);
 int qphix_gpu_clover_apply(qphix_gpu_field res, qphix_gpu_field chi, qphix_gpu_field clov);
 
+/* ---- multi-GPU halo mode: a lattice cut into slabs along t --------------------
+ * (replaces the face packing and exchange of include/qphix/comm.h / face.h for
+ * a t decomposition).  Each rank's lattice is one slab (global t offset even,
+ * so local and global checkerboards agree).  A Dslash on a slab needs, from
+ * its neighbours, the source field's first (next slab) and last (previous
+ * slab) time slices and, once per gauge field, U_t on the previous slab's last
+ * slice.  qphix_gpu_halo_pack_* copy those faces into caller-owned device
+ * buffers; the caller moves them between ranks (NCCL send / recv, or device
+ * copies when the slabs share a GPU) and passes the received buffers to the
+ * *_halo Dslash entry points, which take every other hop from the slab.  The
+ * t boundary condition applies on the slabs holding the global edges.
+ * side 0 = first slice (sent to the previous slab), 1 = last slice (sent to
+ * the next slab). */
+typedef struct {
+  const void *psi_fwd;    /* the next slab's side-0 pack of the hopped field   */
+  const void *psi_bwd;    /* the previous slab's side-1 pack of it             */
+  const void *links_bwd;  /* the previous slab's qphix_gpu_halo_pack_links      */
+  int global_first;       /* this slab holds global t = 0                       */
+  int global_last;        /* this slab holds global t = Nt - 1                  */
+} qphix_gpu_halo_faces;
+int qphix_gpu_halo_spinor_bytes(qphix_gpu_field psi, size_t *bytes);
+int qphix_gpu_halo_pack_spinor(qphix_gpu_field psi, int side, void *dst);
+int qphix_gpu_halo_link_bytes(qphix_gpu_field gauge, size_t *bytes);
+int qphix_gpu_halo_pack_links(qphix_gpu_field gauge, void *dst);
+int qphix_gpu_dslash_halo(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                          qphix_gpu_field gauge, qphix_gpu_field aux, qphix_gpu_field aux2, int isign, int cb,
+                          const qphix_gpu_halo_faces *faces);
+int qphix_gpu_dslash_achimbdpsi_halo(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                                     qphix_gpu_field chi, qphix_gpu_field gauge, qphix_gpu_field aux, double alpha,
+                                     double beta, int isign, int cb, double musign,
+                                     const qphix_gpu_halo_faces *faces);
+
 /* ---- clover term on the device ----------------------------------------------
  * QPhiX takes the clover term and its inverse from its caller (Chroma's
  * QDPCloverTerm); these build them on the GPU from a resident FP64 gauge field:

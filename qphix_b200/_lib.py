@@ -31,6 +31,11 @@ class OpParams(C.Structure):
                 ("twisted_mass", C.c_double), ("prec_mass_rho", C.c_double), ("epsilon", C.c_double)]
 
 
+class HaloFaces(C.Structure):
+    _fields_ = [("psi_fwd", C.c_void_p), ("psi_bwd", C.c_void_p), ("links_bwd", C.c_void_p),
+                ("global_first", C.c_int), ("global_last", C.c_int)]
+
+
 class SolveInfo(C.Structure):
     _fields_ = [("n_iters", C.c_int), ("rsd_sq_final", C.c_double), ("site_flops", C.c_ulong),
                 ("mv_apps", C.c_ulong), ("status", C.c_int), ("true_rel_resid", C.c_double),
@@ -89,6 +94,13 @@ _SIGS = {
     "qphix_gpu_dslash": ([C.POINTER(OpParams), P, P, P, P, P, I_, I_], I_),
     "qphix_gpu_dslash_achimbdpsi": ([C.POINTER(OpParams), P, P, P, P, P, D, D, I_, I_, D], I_),
     "qphix_gpu_dslash_dir": ([C.POINTER(OpParams), P, P, P, I_, I_], I_),
+    "qphix_gpu_halo_spinor_bytes": ([P, C.POINTER(C.c_size_t)], I_),
+    "qphix_gpu_halo_pack_spinor": ([P, I_, P], I_),
+    "qphix_gpu_halo_link_bytes": ([P, C.POINTER(C.c_size_t)], I_),
+    "qphix_gpu_halo_pack_links": ([P, P], I_),
+    "qphix_gpu_dslash_halo": ([C.POINTER(OpParams), P, P, P, P, P, I_, I_, C.POINTER(HaloFaces)], I_),
+    "qphix_gpu_dslash_achimbdpsi_halo": ([C.POINTER(OpParams), P, P, P, P, P, D, D, I_, I_, D,
+                                          C.POINTER(HaloFaces)], I_),
     "qphix_gpu_dslash_two_flav_clover": ([C.POINTER(OpParams), P, P, P, P, P, P, I_, I_], I_),
     "qphix_gpu_clover_apply": ([P, P, P], I_),
     "qphix_gpu_clover_build": ([P, P, I_, D, D, D], I_),

@@ -646,7 +646,7 @@ std::string tune_key(const qphix_gpu_lattice_s *lat, int prec, int recon, int ep
 static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, int epi, int achi,
                                 const DslashArgs &a)
 {
-  const bool gen = a.dir_mask != 0xFFu || a.tbc_mask != 0;
+  const bool gen = a.dir_mask != 0xFFu || a.tbc_mask != 0 || a.halo;
   if (is_two_flavour(epi, achi)) {  // both flavours of a site in one thread
     QPX_REQUIRE(!gen, "two-flavour twisted mass takes all hops without twisted boundary phases");
     DslashShape sh;
@@ -812,9 +812,110 @@ static void tm_derived(const qphix_gpu_op_params &p, double &dmu, double &dmu_in
 }
 
 // res = EPI(D psi) on checkerboard cb
+// ---- halo mode (t slabs) ----------------------------------------------------
+static size_t face_sites(const qphix_gpu_lattice_s *lat) { return (size_t)lat->nxh * lat->dims[1] * lat->dims[2]; }
+
+static size_t halo_spinor_bytes(const qphix_gpu_field_s *f)
+{
+  const size_t face = face_sites(f->lat);
+  return (size_t)f->nrhs * face * ((size_t)f->spec.nchunk * f->spec.chunk_bytes + (f->norm ? sizeof(float) : 0));
+}
+
+static size_t halo_link_bytes(const qphix_gpu_field_s *g)
+{
+  return 2 * face_sites(g->lat) * (size_t)g->spec.nchunk * g->spec.chunk_bytes;
+}
+
+// the ghost-face arguments of a halo-mode launch hopping field psi with links gauge
+static void set_halo(DslashArgs &a, const qphix_gpu_op_params &p, const qphix_gpu_field_s *psi,
+                     const qphix_gpu_field_s *gauge, int cb, const qphix_gpu_halo_faces *faces)
+{
+  QPX_REQUIRE(faces->psi_fwd && faces->psi_bwd && faces->links_bwd, "halo faces: null buffer");
+  QPX_REQUIRE(a.tbc_mask == 0, "halo mode takes no twisted boundary phases");
+  const auto *lat = psi->lat;
+  const long long face = (long long)face_sites(lat);
+  QPX_REQUIRE(face % 4 == 0, "halo mode needs (Nx/2) Ny Nz divisible by 4");
+  auto ghost = [&](const void *buf) {
+    SpinorArg g;
+    g.data = const_cast<void *>(buf);
+    g.stride = face;
+    g.rhs_stride_chunks = (long long)psi->spec.nchunk * face;
+    g.norm = psi->norm ? reinterpret_cast<float *>(static_cast<char *>(g.data) +
+                                                   (size_t)psi->nrhs * face * psi->spec.nchunk *
+                                                       psi->spec.chunk_bytes)
+                       : nullptr;
+    return g;
+  };
+  a.halo = 1;
+  a.ghost_fwd = ghost(faces->psi_fwd);
+  a.ghost_bwd = ghost(faces->psi_bwd);
+  // the backward hop onto checkerboard cb reads U_t of the other checkerboard
+  a.ghost_link.data = static_cast<const char *>(faces->links_bwd) +
+                      (size_t)(1 - cb) * face * gauge->spec.nchunk * gauge->spec.chunk_bytes;
+  a.ghost_link.stride = face;
+  a.ghost_link.mu_stride = (long long)gauge->spec.nchunk * face;
+  a.coeff_t_edge = p.aniso_t * (faces->global_last ? p.t_boundary : 1.0);
+  a.coeff_t_bwd_edge = p.aniso_t * (faces->global_first ? p.t_boundary : 1.0);
+}
+
+extern "C" int qphix_gpu_halo_spinor_bytes(qphix_gpu_field psi, size_t *bytes)
+{
+  return guard([&] {
+    QPX_REQUIRE(psi && bytes, "null argument");
+    require_spinor(psi, "psi");
+    *bytes = halo_spinor_bytes(psi);
+  });
+}
+
+extern "C" int qphix_gpu_halo_link_bytes(qphix_gpu_field gauge, size_t *bytes)
+{
+  return guard([&] {
+    QPX_REQUIRE(gauge && bytes && gauge->kind == QPHIX_GPU_GAUGE, "gauge must be a gauge field");
+    *bytes = halo_link_bytes(gauge);
+  });
+}
+
+// [rhs][chunk][face] rows, then [rhs][face] norms: one strided copy each
+extern "C" int qphix_gpu_halo_pack_spinor(qphix_gpu_field psi, int side, void *dst)
+{
+  return guard([&] {
+    QPX_REQUIRE(psi && dst, "null argument");
+    require_spinor(psi, "psi");
+    QPX_REQUIRE(side == 0 || side == 1, "side must be 0 (first slice) or 1 (last slice)");
+    auto *lat = psi->lat;
+    const size_t face = face_sites(lat), cbytes = psi->spec.chunk_bytes;
+    const size_t s0 = side ? (size_t)(lat->dims[3] - 1) * face : 0;
+    const size_t rows = (size_t)psi->nrhs * psi->spec.nchunk;
+    QPX_CUDA(cudaMemcpy2DAsync(dst, face * cbytes, static_cast<const char *>(psi->data) + s0 * cbytes,
+                               (size_t)lat->stride * cbytes, face * cbytes, rows, cudaMemcpyDeviceToDevice,
+                               lat->stream));
+    if (psi->norm)
+      QPX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(dst) + rows * face * cbytes, face * sizeof(float),
+                                 psi->norm + s0, (size_t)lat->stride * sizeof(float), face * sizeof(float),
+                                 (size_t)psi->nrhs, cudaMemcpyDeviceToDevice, lat->stream));
+  });
+}
+
+// U_t on the last slice, checkerboard 0 then 1, [chunk][face] rows each
+extern "C" int qphix_gpu_halo_pack_links(qphix_gpu_field gauge, void *dst)
+{
+  return guard([&] {
+    QPX_REQUIRE(gauge && dst && gauge->kind == QPHIX_GPU_GAUGE, "gauge must be a gauge field");
+    auto *lat = gauge->lat;
+    const size_t face = face_sites(lat), cbytes = gauge->spec.chunk_bytes, nch = gauge->spec.nchunk;
+    const size_t s0 = (size_t)(lat->dims[3] - 1) * face, mu_stride = nch * lat->stride;
+    for (int c = 0; c < 2; c++)
+      QPX_CUDA(cudaMemcpy2DAsync(static_cast<char *>(dst) + c * nch * face * cbytes, face * cbytes,
+                                 static_cast<const char *>(gauge->data) + ((c * 4 + 3) * mu_stride + s0) * cbytes,
+                                 (size_t)lat->stride * cbytes, face * cbytes, nch, cudaMemcpyDeviceToDevice,
+                                 lat->stream));
+  });
+}
+
 static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphix_gpu_field_s *psi,
                         qphix_gpu_field_s *gauge, qphix_gpu_field_s *aux, qphix_gpu_field_s *aux2, int isign,
-                        int cb, unsigned dir_mask = 0xFFu, qphix_gpu_field_s *aux3 = nullptr)
+                        int cb, unsigned dir_mask = 0xFFu, qphix_gpu_field_s *aux3 = nullptr,
+                        const qphix_gpu_halo_faces *faces = nullptr)
 {
   require_spinor(res, "res");
   require_spinor(psi, "psi");
@@ -881,6 +982,10 @@ static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qp
   default:
     throw Error(QPHIX_GPU_EINVAL, "bad operator kind");
   }
+  if (faces) {
+    QPX_REQUIRE(!is_two_flavour(epi, ACHI_NONE), "halo mode is not provided for the two-flavour operators");
+    set_halo(a, p, psi, gauge, cb, faces);
+  }
   dslash_launch(lat, res->prec, gauge->recon, epi, ACHI_NONE, a);
 }
 
@@ -895,7 +1000,8 @@ struct ApplyOpts {
 
 static void achi_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphix_gpu_field_s *psi,
                       qphix_gpu_field_s *chi, qphix_gpu_field_s *gauge, qphix_gpu_field_s *aux, double alpha,
-                      double beta, int isign, int cb, double musign, const ApplyOpts &o)
+                      double beta, int isign, int cb, double musign, const ApplyOpts &o,
+                      const qphix_gpu_halo_faces *faces = nullptr)
 {
   require_spinor(res, "res");
   require_spinor(psi, "psi");
@@ -953,6 +1059,11 @@ static void achi_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphi
   default:
     throw Error(QPHIX_GPU_EINVAL, "bad operator kind");
   }
+  if (faces) {
+    QPX_REQUIRE(!is_two_flavour(EPI_NONE, achi), "halo mode is not provided for the two-flavour operators");
+    QPX_REQUIRE(!o.red_mask && o.post == POST_STORE, "halo launches take no fused solver updates");
+    set_halo(a, p, psi, gauge, cb, faces);
+  }
   a.post = o.post;
   if (o.w) a.w = o.w->sarg();
   if (o.r) a.r = o.r->sarg();
@@ -1000,6 +1111,27 @@ extern "C" int qphix_gpu_dslash_achimbdpsi(const qphix_gpu_op_params *p, qphix_g
   return guard([&] {
     QPX_REQUIRE(p, "null params");
     achi_core(*p, res, psi, chi, gauge, aux, alpha, beta, isign, cb, musign, ApplyOpts());
+  });
+}
+
+extern "C" int qphix_gpu_dslash_halo(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                                     qphix_gpu_field gauge, qphix_gpu_field aux, qphix_gpu_field aux2, int isign,
+                                     int cb, const qphix_gpu_halo_faces *faces)
+{
+  return guard([&] {
+    QPX_REQUIRE(p && faces, "null argument");
+    dslash_core(*p, res, psi, gauge, aux, aux2, isign, cb, 0xFFu, nullptr, faces);
+  });
+}
+
+extern "C" int qphix_gpu_dslash_achimbdpsi_halo(const qphix_gpu_op_params *p, qphix_gpu_field res,
+                                                qphix_gpu_field psi, qphix_gpu_field chi, qphix_gpu_field gauge,
+                                                qphix_gpu_field aux, double alpha, double beta, int isign, int cb,
+                                                double musign, const qphix_gpu_halo_faces *faces)
+{
+  return guard([&] {
+    QPX_REQUIRE(p && faces, "null argument");
+    achi_core(*p, res, psi, chi, gauge, aux, alpha, beta, isign, cb, musign, ApplyOpts(), faces);
   });
 }
 

@@ -111,6 +111,17 @@ struct DslashArgs {
   double rho;           // i rho gamma_5 term
   double eps;           // flavour splitting of the two-flavour twisted mass
   int post;
+  // halo mode (general path only): the lattice is one slab of a lattice cut
+  // along t; hops across the slab's t edges read ghost faces instead of
+  // wrapping.  ghost_fwd = psi on the next slab's first time slice,
+  // ghost_bwd = psi on the previous slab's last slice, ghost_link = U_t on
+  // that slice (the backward hop's link), each indexed by the face site
+  // (z ny + y) nx/2 + x/2.  The forward edge takes coeff_t_edge, the backward
+  // edge coeff_t_bwd_edge (aniso_t, times t_boundary on the global edges).
+  int halo;
+  SpinorArg ghost_fwd, ghost_bwd;
+  GaugeArg ghost_link;
+  double coeff_t_bwd_edge;
   SpinorArg r, x, p, w; // extra vectors for POST_CG and RED_DOT_W_OUT
   ReduceArg red;
   SolverState *state;   // nullable; supplies the done flag and POST_CG's a
@@ -459,11 +470,16 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
             (MU < 3) ? a.coeff_s : (tlast[l] ? a.coeff_t_edge : a.coeff_t);               \
         lanes_set(cf, c);                                                                 \
       }                                                                                   \
+      /* halo: the next slab's first slice (general path, one site per thread) */         \
+      const bool ghf = GEN && MU == 3 && a.halo && tlast[0];                              \
+      int ixf[SP];                                                                        \
+      _Pragma("unroll") for (int l = 0; l < SP; l++) ixf[l] =                             \
+          ghf ? s[l] - (a.geom.nt - 1) * sxyzt : nb[MU][1][l];                            \
       const cx<T> ph = {splat<T>(a.tbc[MU][0]), splat<T>(a.tbc[MU][1])};                  \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
         T psi[24], nrm;                                                                   \
-        L::load_raw(a.in, rhs0 + r, nb[MU][1], psi, nrm);                                 \
+        L::load_raw(ghf ? a.ghost_fwd : a.in, rhs0 + r, ixf, psi, nrm);                   \
         cx<T> h[2][3], ch[2][3];                                                          \
         project<MU, -ISIGN>(psi, h);                                                      \
         if (tw || SP == 2) { /* SP = 2: the folded form costs registers (spills) */       \
@@ -478,20 +494,27 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
     }                                                                                     \
     /* backward hop: U_mu(x - mu)^+ (1 + isign g) psi(x - mu) */                          \
     if (!GEN || (a.dir_mask & (1u << (2 * MU)))) {                                        \
+      /* halo: the previous slab's last slice and its U_t (general path) */               \
+      const bool ghb = GEN && MU == 3 && a.halo && tfirst[0];                             \
+      int ixb[SP];                                                                        \
+      _Pragma("unroll") for (int l = 0; l < SP; l++) ixb[l] = ghb ? s[l] : nb[MU][0][l];  \
       cx<T> u[3][3];                                                                      \
-      L::template load_link<RECON>(a.gauge, 1 - a.cb, MU, nb[MU][0], u);                  \
+      L::template load_link<RECON>(ghb ? a.ghost_link : a.gauge, ghb ? 0 : 1 - a.cb,      \
+                                   ghb ? 0 : MU, ixb, u);                                 \
       T cf;                                                                               \
       {                                                                                   \
         double c[SP];                                                                     \
         _Pragma("unroll") for (int l = 0; l < SP; l++) c[l] =                             \
-            (MU < 3) ? a.coeff_s : (tfirst[l] ? a.coeff_t_edge : a.coeff_t);              \
+            (MU < 3) ? a.coeff_s                                                          \
+                     : (tfirst[l] ? ((GEN && a.halo) ? a.coeff_t_bwd_edge : a.coeff_t_edge) \
+                                  : a.coeff_t);                                           \
         lanes_set(cf, c);                                                                 \
       }                                                                                   \
       const cx<T> ph = {splat<T>(a.tbc[MU][0]), splat<T>(-a.tbc[MU][1])};                 \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
         T psi[24], nrm;                                                                   \
-        L::load_raw(a.in, rhs0 + r, nb[MU][0], psi, nrm);                                 \
+        L::load_raw(ghb ? a.ghost_bwd : a.in, rhs0 + r, ixb, psi, nrm);                   \
         cx<T> h[2][3], ch[2][3];                                                          \
         project<MU, ISIGN>(psi, h);                                                       \
         if (tw || SP == 2) { /* SP = 2: the folded form costs registers (spills) */       \
