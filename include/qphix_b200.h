@@ -332,6 +332,12 @@ int qphix_gpu_blas_caxpby(const double a[2], qphix_gpu_field x, const double b[2
                                                       /* y = a x + b y: axpy :214, axpby :247, aypx :139, caxpy :696 */
 int qphix_gpu_blas_copy(qphix_gpu_field dst, qphix_gpu_field src);               /* :18  */
 int qphix_gpu_blas_zero(qphix_gpu_field x);                                      /* :49  */
+int qphix_gpu_blas_caxpby_norm2(const double a[2], qphix_gpu_field x, const double b[2], qphix_gpu_field y,
+                                double *out);          /* y = a x + b y, |y|^2: axpyNorm2 :312 */
+int qphix_gpu_blas_xmy_norm2(qphix_gpu_field x, qphix_gpu_field y, qphix_gpu_field z, double *out);
+                                                      /* z = x - y, |z|^2: xmyNorm2Spinor :345, xmy2Norm2Spinor :360 */
+int qphix_gpu_blas_inner_product_norm(qphix_gpu_field x, qphix_gpu_field y, double *out);
+                                                      /* out[3 nrhs]: <x,y> re, im, |x|^2: innerProductNorm :573 */
 
 /* ---- squared norms without allocation ---------------------------------------
  * No counterpart in the reference.  Same result as qphix_gpu_blas_norm2, for

@@ -123,6 +123,9 @@ _SIGS = {
     "qphix_gpu_blas_norm2_noalloc": ([P, P], I_),
     "qphix_gpu_blas_inner_product": ([P, P, P], I_),
     "qphix_gpu_blas_caxpby": ([P, P, P, P], I_),
+    "qphix_gpu_blas_caxpby_norm2": ([P, P, P, P, P], I_),
+    "qphix_gpu_blas_xmy_norm2": ([P, P, P, P], I_),
+    "qphix_gpu_blas_inner_product_norm": ([P, P, P], I_),
     "qphix_gpu_blas_copy": ([P, P], I_),
     "qphix_gpu_blas_zero": ([P], I_),
     "qphix_gpu_server_create": ([C.POINTER(ServerConfig), PP], I_),

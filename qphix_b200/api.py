@@ -698,6 +698,29 @@ def caxpby(a, x, b, y):
     check(L._lib.qphix_gpu_blas_caxpby(av, x.h, bv, y.h))
 
 
+def caxpby_norm2(a, x, b, y):
+    """y = a x + b y; returns |y|^2 per rhs (axpyNorm2)"""
+    av = (C.c_double * 2)(complex(a).real, complex(a).imag)
+    bv = (C.c_double * 2)(complex(b).real, complex(b).imag)
+    out = np.zeros(x.nrhs)
+    check(L._lib.qphix_gpu_blas_caxpby_norm2(av, x.h, bv, y.h, out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+def xmy_norm2(x, y, z):
+    """z = x - y; returns |z|^2 per rhs (xmyNorm2Spinor; z = y: xmy2Norm2Spinor)"""
+    out = np.zeros(x.nrhs)
+    check(L._lib.qphix_gpu_blas_xmy_norm2(x.h, y.h, z.h, out.ctypes.data_as(C.c_void_p)))
+    return out
+
+
+def inner_product_norm(x, y):
+    """(<x, y>, |x|^2) per rhs (innerProductNorm)"""
+    out = np.zeros(3 * x.nrhs)
+    check(L._lib.qphix_gpu_blas_inner_product_norm(x.h, y.h, out.ctypes.data_as(C.c_void_p)))
+    return out[0::3] + 1j * out[1::3], out[2::3]
+
+
 def copy(dst, src):
     check(L._lib.qphix_gpu_blas_copy(dst.h, src.h))
 

@@ -1488,6 +1488,70 @@ extern "C" int qphix_gpu_blas_inner_product(qphix_gpu_field x, qphix_gpu_field y
   });
 }
 
+// y = a x + b y, out[r] = |y_r|^2 (axpyNorm2, include/qphix/blas_new_c.h:312-343)
+extern "C" int qphix_gpu_blas_caxpby_norm2(const double a[2], qphix_gpu_field x, const double b[2],
+                                           qphix_gpu_field y, double *out)
+{
+  return guard([&] {
+    require_spinor(x, "x");
+    require_spinor(y, "y");
+    require_same(x, y);
+    QPX_REQUIRE(a && b && out, "null argument");
+    BlasCall c;
+    c.op = B_CAXPBY_NORM;
+    c.x = x;
+    c.y = y;
+    c.a = cval(a[0], a[1]);
+    c.b = cval(b[0], b[1]);
+    c.slots = 0x1;
+    blas_launch(x->lat, x->prec, x->nrhs, c);
+    const double *r = fetch_result(x->lat, x->nrhs, 1);
+    for (int i = 0; i < x->nrhs; i++) out[i] = r[i];
+  });
+}
+
+// z = x - y, out[r] = |z_r|^2 (xmyNorm2Spinor, blas_new_c.h:345-358; z may be y:
+// xmy2Norm2Spinor, :360-395)
+extern "C" int qphix_gpu_blas_xmy_norm2(qphix_gpu_field x, qphix_gpu_field y, qphix_gpu_field z, double *out)
+{
+  return guard([&] {
+    require_spinor(x, "x");
+    require_spinor(y, "y");
+    require_spinor(z, "z");
+    require_same(x, y);
+    require_same(x, z);
+    QPX_REQUIRE(out, "null out");
+    BlasCall c;
+    c.op = B_XMY_NORM;
+    c.x = x;
+    c.y = y;
+    c.z = z;
+    c.slots = 0x1;
+    blas_launch(x->lat, x->prec, x->nrhs, c);
+    const double *r = fetch_result(x->lat, x->nrhs, 1);
+    for (int i = 0; i < x->nrhs; i++) out[i] = r[i];
+  });
+}
+
+// out[3 r .. 3 r + 2] = Re <x, y>, Im <x, y>, |x|^2 (innerProductNorm, blas_new_c.h:573-625)
+extern "C" int qphix_gpu_blas_inner_product_norm(qphix_gpu_field x, qphix_gpu_field y, double *out)
+{
+  return guard([&] {
+    require_spinor(x, "x");
+    require_spinor(y, "y");
+    require_same(x, y);
+    QPX_REQUIRE(out, "null out");
+    BlasCall c;
+    c.op = B_DOTNORM;
+    c.x = x;
+    c.y = y;
+    c.slots = 0x7;
+    blas_launch(x->lat, x->prec, x->nrhs, c);
+    const double *r = fetch_result(x->lat, x->nrhs, 3);
+    for (int i = 0; i < 3 * x->nrhs; i++) out[i] = r[i];
+  });
+}
+
 extern "C" int qphix_gpu_blas_caxpby(const double a[2], qphix_gpu_field x, const double b[2], qphix_gpu_field y)
 {
   return guard([&] {

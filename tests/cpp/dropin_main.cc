@@ -10,6 +10,7 @@
 #include <string>
 #include <vector>
 
+#include "qphix/blas_new_c.h"
 #include "qphix/clover.h"
 #include "qphix/geometry.h"
 #include "qphix/inv_richardson_multiprec.h"
@@ -193,6 +194,52 @@ int main(int argc, char **argv)
       unprec(&fx, &fb, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
       write_from("out_unprec_e", fx.getCBData(0), sbytes);
       write_from("out_unprec_o", fx.getCBData(1), sbytes);
+    }
+
+    // 9. BLAS (blas_new_c.h) on host arrays: psi, chi as read
+    {
+      auto *a = geom.allocCBFourSpinor();
+      auto *b = geom.allocCBFourSpinor();
+      auto *c = geom.allocCBFourSpinor();
+      auto *ch = geom.allocCBFourSpinor();
+      read_into("d_chi", ch, sbytes);
+      double out[16];
+      norm2Spinor(out[0], psi, geom, 1);
+      innerProduct(out + 1, psi, ch, geom, 1);
+      innerProductNorm(out + 3, psi, ch, geom, 1);
+      copySpinor(a, psi, geom, 1);
+      axpy(0.5, ch, a, geom, 1);                    // a = psi + 0.5 chi
+      write_from("out_blas_axpy", a, sbytes);
+      copySpinor(b, ch, geom, 1);
+      axpby(2.0, psi, -1.5, b, geom, 1);            // b = 2 psi - 1.5 chi
+      write_from("out_blas_axpby", b, sbytes);
+      xmyNorm2Spinor(c, psi, ch, out[6], geom, 1);  // c = psi - chi
+      write_from("out_blas_xmy", c, sbytes);
+      copySpinor(c, ch, geom, 1);
+      aypx(-0.25, psi, c, geom, 1);                 // c = psi - 0.25 chi
+      write_from("out_blas_aypx", c, sbytes);
+      double ca[2] = {0.3, -0.7};
+      copySpinor(c, ch, geom, 1);
+      caxpySpinor(ca, psi, c, geom, 1);             // c = (0.3 - 0.7i) psi + chi
+      write_from("out_blas_caxpy", c, sbytes);
+      axpyNorm2(1.0, psi, c, out[7], geom, 1);      // c += psi
+      copySpinor(c, psi, geom, 1);
+      ymeqx(ch, c, geom, 1);                        // c = psi - chi
+      ax(3.0, c, geom, 1);                          // c = 3 (psi - chi)
+      write_from("out_blas_ax", c, sbytes);
+      zeroSpinor(c, geom, 1);
+      norm2Spinor(out[8], c, geom, 1);
+      // FP64 -> float Geometry and back
+      auto *f = geomf.allocCBFourSpinor();
+      convert(f, 1.0, psi, geomf, geom, 1);
+      convert(c, 2.0, f, geom, geomf, 1);             // c = 2 psi (through FP32)
+      write_from("out_blas_convert", c, sbytes);
+      write_from("out_blas_scalars", out, sizeof(double) * 9);
+      geomf.free(f);
+      geom.free(a);
+      geom.free(b);
+      geom.free(c);
+      geom.free(ch);
     }
 
     for (int s = 0; s < ns; s++) geom.free(xs[s]);

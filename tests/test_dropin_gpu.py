@@ -91,6 +91,19 @@ def test_cpp_dropin(tmp_path, oracle):
     xn = np.stack([load("out_ndccg_up"), load("out_ndccg_dn")])
     r = pair - NC.apply(NC.apply(xn, 1), -1)
     assert np.linalg.norm(r) / np.linalg.norm(pair) < 2e-10
+    # BLAS of blas_new_c.h on host arrays
+    sc = np.fromfile(d / "out_blas_scalars")
+    assert abs(sc[0] - np.vdot(psi, psi).real) < 1e-12 * sc[0]
+    ip = np.vdot(psi, chi)
+    assert abs(sc[1] + 1j * sc[2] - ip) < 1e-12 * abs(ip) and abs(sc[3] + 1j * sc[4] - ip) < 1e-12 * abs(ip)
+    assert abs(sc[5] - np.vdot(psi, psi).real) < 1e-12 * sc[5]
+    assert abs(sc[6] - np.vdot(psi - chi, psi - chi).real) < 1e-12 * sc[6]
+    c2 = (0.3 - 0.7j) * psi + chi + psi
+    assert abs(sc[7] - np.vdot(c2, c2).real) < 1e-12 * sc[7] and sc[8] == 0.0
+    for name, ref in (("axpy", psi + 0.5 * chi), ("axpby", 2 * psi - 1.5 * chi), ("xmy", psi - chi),
+                      ("aypx", psi - 0.25 * chi), ("caxpy", (0.3 - 0.7j) * psi + chi), ("ax", 3 * (psi - chi))):
+        assert rel_l2(load("out_blas_" + name), ref) < 1e-15, name
+    assert rel_l2(load("out_blas_convert"), 2 * psi) < 1e-7  # through FP32
     # unpreconditioned clover system: [[A_ee, -D_eo/2], [-D_oe/2, A_oo]] x = (chi, psi)
     xe, xo = load("out_unprec_e"), load("out_unprec_o")
     re = oracle.clover_apply(xe, s["clov"][0]) - 0.5 * oracle.dslash(L, xo, s["gauge"], 1, 0) - chi

@@ -303,3 +303,28 @@ def test_multishift_fp32_with_fp64_refinement(api, oracle, setup):
         x = x64.download()
         r = b - (O.apply(O.apply(x, 1), -1) + sh * x)
         assert np.linalg.norm(r) / bn < tol, (sh, np.linalg.norm(r) / bn)
+
+
+def test_fused_blas_entry_points():
+    """qphix_gpu_blas_caxpby_norm2 / _xmy_norm2 / _inner_product_norm
+    (axpyNorm2, xmyNorm2Spinor, innerProductNorm of include/qphix/blas_new_c.h)
+    against numpy, FP64, two right-hand sides."""
+    from qphix_b200 import api
+    dims = (4, 4, 4, 8)
+    lat = api.Lattice(dims)
+    xs = np.stack([F.gaussian_spinor(dims, 300 + k) for k in range(2)])
+    ys = np.stack([F.gaussian_spinor(dims, 310 + k) for k in range(2)])
+    x = lat.spinor("f64", 2).upload(xs)
+    y = lat.spinor("f64", 2).upload(ys)
+    ip, nx = api.inner_product_norm(x, y)
+    for k in range(2):
+        assert abs(ip[k] - np.vdot(xs[k], ys[k])) < 1e-12 * abs(ip[k])
+        assert abs(nx[k] - np.vdot(xs[k], xs[k]).real) < 1e-12 * nx[k]
+    z = lat.spinor("f64", 2)
+    n = api.xmy_norm2(x, y, z)
+    assert np.allclose(z.download(), xs - ys, rtol=0, atol=1e-14)
+    assert np.allclose(n, [np.vdot(xs[k] - ys[k], xs[k] - ys[k]).real for k in range(2)], rtol=1e-12)
+    n = api.caxpby_norm2(0.5 - 0.25j, x, 2.0, y)
+    ref = (0.5 - 0.25j) * xs + 2.0 * ys
+    assert np.allclose(y.download(), ref, rtol=0, atol=1e-14)
+    assert np.allclose(n, [np.vdot(ref[k], ref[k]).real for k in range(2)], rtol=1e-12)
