@@ -77,21 +77,6 @@ __device__ __forceinline__ double warp_sum(double v)
   return v;
 }
 
-// Sum `val` over the block; result valid in thread 0.  All threads must call.
-__device__ __forceinline__ double block_sum(double val, double *smem)
-{
-  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  int nw = (blockDim.x + 31) >> 5;
-  val = warp_sum(val);
-  __syncthreads();
-  if (lane == 0) smem[wid] = val;
-  __syncthreads();
-  double r = 0;
-  if (threadIdx.x == 0)
-    for (int w = 0; w < nw; w++) r += smem[w];
-  return r;
-}
-
 __device__ inline void finalize(int fin, SolverState *st, const double *res, int nrhs, int nval);
 
 // Called by every thread of every block after the block's per-thread values

@@ -88,3 +88,18 @@ def test_oracle_hermiticity(oracle):
     a = np.vdot(y, oracle.dslash(L, x, s["gauge"], 1, 0))
     b = np.vdot(oracle.dslash(L, y, s["gauge"], -1, 1), x)
     assert abs(a - b) / abs(a) < 1e-13
+
+
+def test_bench_reference_arm_runs_on_cpu():
+    """`bench.py --impl reference` (the CPU path of the same system, timed on
+    host cores) prints the contract's line without a GPU."""
+    import json
+    import sys
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                          "--warmup", "0"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "solves/s"
+    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"] == {"value": line["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
