@@ -177,6 +177,26 @@ class TMDslash : public Dslash<FT, veclen, soalen, compress12>
                "tm dslashAChiMinusBDPsi");
     s.download_spinor(out, res);
   }
+
+  // res_f = alpha (1 + i s_f isign mu/(4+m) g5) chi_f - beta D psi_f - epsilon chi_{1-f},
+  // s_up = +1, s_dn = -1 (tm_dslash_body.h:1174-1207)
+  void two_flav_AChiMinusBDPsi(FourSpinorBlock *const res[2], const FourSpinorBlock *const psi[2],
+                               const FourSpinorBlock *const chi[2], const SU3MatrixBlock *u, double alpha,
+                               double beta, double epsilon, int isign, int cb)
+  {
+    Geom &s = *this->s;
+    auto g = gpu::upload_gauge_cb(s, u, cb);
+    auto in = s.upload_flavours(psi);
+    auto x = s.upload_flavours(chi);
+    gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0, 2);
+    qphix_gpu_op_params q = this->p;
+    q.kind = QPHIX_GPU_NDTM;
+    q.epsilon = epsilon;
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&q, out.get(), in.get(), x.get(), g.get(), nullptr, alpha, beta, isign,
+                                           cb, 1.0),
+               "tm two_flav_AChiMinusBDPsi");
+    s.download_flavours(out, res);
+  }
 };
 
 template <typename FT, int veclen, int soalen, bool compress12>
@@ -198,15 +218,16 @@ class TMClovDslash : public Dslash<FT, veclen, soalen, compress12>
     this->p.prec_mass_rho = prec_mass_rho;
   }
 
-  // res = invclov[isign == 1 ? 0 : 1] D psi (flavour 0; tm_clov_dslash_body.h:352)
+  // res = invclov[k] D psi, k = 0 for (isign = +1, up) and (isign = -1, down),
+  // else 1 (tm_clov_dslash_body.h:348-353)
   void dslash(FourSpinorBlock *res, const FourSpinorBlock *psi, const SU3MatrixBlock *u,
               const FullCloverBlock *const invclov[2], int isign, int cb, int fl = 0)
   {
-    if (fl != 0) throw std::invalid_argument("TMClovDslash: only flavour 0 (degenerate) is supported");
+    if (fl != 0 && fl != 1) throw std::invalid_argument("TMClovDslash: flavour must be 0 (up) or 1 (down)");
     Geom &s = *this->s;
     auto g = gpu::upload_gauge_cb(s, u, cb);
-    auto f0 = s.upload_full_clover(invclov[0]);
-    auto f1 = s.upload_full_clover(invclov[1]);
+    auto f0 = s.upload_full_clover(invclov[fl]);
+    auto f1 = s.upload_full_clover(invclov[1 - fl]);
     auto in = s.upload_spinor(psi);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
     gpu::check(qphix_gpu_dslash(&this->p, out.get(), in.get(), g.get(), f0.get(), f1.get(), isign, cb),
@@ -214,21 +235,65 @@ class TMClovDslash : public Dslash<FT, veclen, soalen, compress12>
     s.download_spinor(out, res);
   }
 
+  // res = (A + i rho_f g5) chi - beta D psi, rho_up = prec_mass_rho, rho_dn = -prec_mass_rho
+  // (tm_clov_dslash_body.h:983)
   void dslashAChiMinusBDPsi(FourSpinorBlock *res, const FourSpinorBlock *psi, const FourSpinorBlock *chi,
                             const SU3MatrixBlock *u, const CloverBlock *clov, const double beta, int isign, int cb,
                             int fl = 0)
   {
-    if (fl != 0) throw std::invalid_argument("TMClovDslash: only flavour 0 (degenerate) is supported");
+    if (fl != 0 && fl != 1) throw std::invalid_argument("TMClovDslash: flavour must be 0 (up) or 1 (down)");
     Geom &s = *this->s;
     auto g = gpu::upload_gauge_cb(s, u, cb);
     auto c = s.upload_clover(clov);
     auto in = s.upload_spinor(psi);
     auto x = s.upload_spinor(chi);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
-    gpu::check(qphix_gpu_dslash_achimbdpsi(&this->p, out.get(), in.get(), x.get(), g.get(), c.get(), 0.0, beta, isign,
-                                           cb, 1.0),
+    qphix_gpu_op_params q = this->p;
+    if (fl == 1) q.prec_mass_rho = -q.prec_mass_rho;
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&q, out.get(), in.get(), x.get(), g.get(), c.get(), 0.0, beta, isign, cb,
+                                           1.0),
                "tm clover dslashAChiMinusBDPsi");
     s.download_spinor(out, res);
+  }
+
+  // the two-flavour inverse clover term alone: res_up = fcl_a psi_up + C psi_dn,
+  // res_dn = fcl_b psi_dn + C psi_up, (fcl_a, fcl_b) = (fcl[0], fcl[1]) for
+  // isign = +1, swapped for -1 (tm_clov_dslash_body.h:1184-1343)
+  void two_flav_inverse_clover_term(FourSpinorBlock *const res[2], const FourSpinorBlock *const psi[2],
+                                    const FullCloverBlock *const fcl[2], const CloverBlock *const clOffDiag,
+                                    int isign)
+  {
+    Geom &s = *this->s;
+    auto in = s.upload_flavours(psi);
+    auto f0 = s.upload_full_clover(fcl[0]);
+    auto f1 = s.upload_full_clover(fcl[1]);
+    auto c = s.upload_clover(clOffDiag);
+    gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0, 2);
+    gpu::check(qphix_gpu_two_flav_clover_apply(out.get(), in.get(), f0.get(), f1.get(), c.get(), isign),
+               "two_flav_inverse_clover_term");
+    s.download_flavours(out, res);
+  }
+
+  // res_f = (A + i rho_f g5) chi_f - beta D psi_f - epsilon chi_{1-f}
+  // (tm_clov_dslash_body.h:1345-1365)
+  void two_flav_AChiMinusBDPsi(FourSpinorBlock *const res[2], const FourSpinorBlock *const psi[2],
+                               const FourSpinorBlock *const chi[2], const SU3MatrixBlock *u, const CloverBlock *clov,
+                               const double beta, const double epsilon, const int isign, const int cb)
+  {
+    Geom &s = *this->s;
+    auto g = gpu::upload_gauge_cb(s, u, cb);
+    auto c = s.upload_clover(clov);
+    auto in = s.upload_flavours(psi);
+    auto x = s.upload_flavours(chi);
+    gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0, 2);
+    qphix_gpu_op_params q = this->p;
+    q.kind = QPHIX_GPU_NDTMCLOVER;
+    q.twisted_mass = this->p.prec_mass_rho;
+    q.epsilon = epsilon;
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&q, out.get(), in.get(), x.get(), g.get(), c.get(), 0.0, beta, isign, cb,
+                                           1.0),
+               "tm clover two_flav_AChiMinusBDPsi");
+    s.download_flavours(out, res);
   }
 };
 

@@ -261,6 +261,12 @@ int qphix_gpu_clover_invert_twisted(qphix_gpu_field dst_plus, qphix_gpu_field ds
  * EvenOddNDTMCloverReuseOperator (ndtm_reuse_operator_clover.h:38-50). */
 int qphix_gpu_clover_invert_ndtm(qphix_gpu_field finv_up, qphix_gpu_field finv_dn, qphix_gpu_field clov_odiag,
                                  qphix_gpu_field src, double mu, double eps);
+/* The two-flavour inverse clover term alone (no hop) on (up, down) pairs:
+ * res_up = Fa psi_up + C psi_dn, res_dn = Fb psi_dn + C psi_up with
+ * (Fa, Fb) = (finv_up, finv_dn), swapped for isign = -1
+ * (TMClovDslash::two_flav_inverse_clover_term, tm_clov_dslash_def.h:96-110). */
+int qphix_gpu_two_flav_clover_apply(qphix_gpu_field res, qphix_gpu_field psi, qphix_gpu_field finv_up,
+                                    qphix_gpu_field finv_dn, qphix_gpu_field clov_odiag, int isign);
 int qphix_gpu_clover_convert(qphix_gpu_field dst, qphix_gpu_field src);
 
 /* ---- even-odd operators ----------------------------------------------------

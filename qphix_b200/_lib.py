@@ -107,6 +107,7 @@ _SIGS = {
     "qphix_gpu_clover_invert": ([P, P], I_),
     "qphix_gpu_clover_invert_twisted": ([P, P, P, D], I_),
     "qphix_gpu_clover_invert_ndtm": ([P, P, P, P, D, D], I_),
+    "qphix_gpu_two_flav_clover_apply": ([P, P, P, P, P, I_], I_),
     "qphix_gpu_clover_convert": ([P, P], I_),
     "qphix_gpu_eo_op_create": ([C.POINTER(OpParams), P, P, P, P, P, PP], I_),
     "qphix_gpu_eo_op_destroy": ([P], I_),

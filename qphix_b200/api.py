@@ -477,6 +477,11 @@ class TMClovDslashTwoFlav:
         check(L._lib.qphix_gpu_dslash_two_flav_clover(C.byref(self.p), res.h, psi.h, u.h, invclov[0].h,
                                                       invclov[1].h, invclov_odiag.h, isign, cb))
 
+    def two_flav_inverse_clover_term(self, res, psi, invclov, invclov_odiag, isign):
+        """the inverse clover term alone (tm_clov_dslash_def.h:96-110)"""
+        check(L._lib.qphix_gpu_two_flav_clover_apply(res.h, psi.h, invclov[0].h, invclov[1].h, invclov_odiag.h,
+                                                     isign))
+
     def two_flav_AChiMinusBDPsi(self, res, psi, chi, u, clov, beta, isign, cb):
         check(L._lib.qphix_gpu_dslash_achimbdpsi(C.byref(self.p), res.h, psi.h, chi.h, u.h, clov.h, 0.0,
                                                  beta, isign, cb, 1.0))

@@ -1211,6 +1211,31 @@ extern "C" int qphix_gpu_clover_invert(qphix_gpu_field dst, qphix_gpu_field src)
   });
 }
 
+extern "C" int qphix_gpu_two_flav_clover_apply(qphix_gpu_field res, qphix_gpu_field psi, qphix_gpu_field finv_up,
+                                               qphix_gpu_field finv_dn, qphix_gpu_field clov_odiag, int isign)
+{
+  return guard([&] {
+    require_spinor(res, "res");
+    require_spinor(psi, "psi");
+    require_same(res, psi);
+    QPX_REQUIRE(res != psi, "res and psi must be different fields");
+    QPX_REQUIRE(res->nrhs == psi->nrhs && psi->nrhs % 2 == 0, "two-flavour fields hold (up, down) pairs");
+    QPX_REQUIRE(finv_up && finv_dn && finv_up->kind == QPHIX_GPU_FULLCLOVER && finv_dn->kind == QPHIX_GPU_FULLCLOVER,
+                "the flavour-diagonal inverses must be full clover fields");
+    QPX_REQUIRE(clov_odiag && clov_odiag->kind == QPHIX_GPU_CLOVER, "the off-diagonal inverse must be a clover field");
+    require_same(res, finv_up);
+    require_same(res, finv_dn);
+    require_same(res, clov_odiag);
+    QPX_REQUIRE(isign == 1 || isign == -1, "isign must be +1 or -1");
+    auto *lat = res->lat;
+    // isign swaps the flavour-diagonal inverses (tm_clov_dslash_body.h:1193-1200)
+    const auto *fa = isign == 1 ? finv_up : finv_dn, *fb = isign == 1 ? finv_dn : finv_up;
+    launch_two_flav_clover(res->prec, (int)lat->vh, res->nrhs / 2, res->sarg(), psi->sarg(), fa->carg(), fb->carg(),
+                           clov_odiag->carg(), lat->stream);
+    check_launch();
+  });
+}
+
 extern "C" int qphix_gpu_clover_invert_ndtm(qphix_gpu_field finv_up, qphix_gpu_field finv_dn,
                                             qphix_gpu_field clov_odiag, qphix_gpu_field src, double mu, double eps)
 {

@@ -276,6 +276,74 @@ __global__ void clover_invert_kernel(Geom geo, const void *in, long long stride,
   }
 }
 
+// The two-flavour inverse clover term on its own (no hop), one (up, down)
+// pair per thread: out_up = Fa psi_up + C psi_dn, out_dn = Fb psi_dn + C psi_up
+// (TMClovDslash::two_flav_inverse_clover_term, tm_clov_dslash_body.h:1184-1343;
+// per-site form codegen/dslash_common.cc:1198-1341), FP64 arithmetic
+template <typename P>
+__global__ void two_flav_clover_kernel(int vh, int npairs, SpinorArg out, SpinorArg in, CloverArg fa, CloverArg fb,
+                                       CloverArg c)
+{
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (s >= vh || k >= npairs) return;
+  using T = typename P::real;
+  T up[24], dn[24], f[72], cl[36];
+  SpinorIO<P>::load(in, 2 * k, s, up);
+  SpinorIO<P>::load(in, 2 * k + 1, s, dn);
+  double ou[24], od[24];
+  for (int b = 0; b < 2; b++) {
+    // one 6-vector block: index i = 3 (spin - 2b) + colour
+    zd xu[6], xd[6];
+    for (int i = 0; i < 6; i++) {
+      const int e = ((2 * b + i / 3) * 3 + i % 3) * 2;
+      xu[i] = zd{(double)up[e], (double)up[e + 1]};
+      xd[i] = zd{(double)dn[e], (double)dn[e + 1]};
+    }
+    zd yu[6], yd[6];
+    CloverIO<P, 144>::load(fa, s, 72 * b, 72, f);
+    for (int i = 0; i < 6; i++) {
+      zd v = {0.0, 0.0};
+      for (int j = 0; j < 6; j++) v = v + zd{(double)f[(i * 6 + j) * 2], (double)f[(i * 6 + j) * 2 + 1]} * xu[j];
+      yu[i] = v;
+    }
+    CloverIO<P, 144>::load(fb, s, 72 * b, 72, f);
+    for (int i = 0; i < 6; i++) {
+      zd v = {0.0, 0.0};
+      for (int j = 0; j < 6; j++) v = v + zd{(double)f[(i * 6 + j) * 2], (double)f[(i * 6 + j) * 2 + 1]} * xd[j];
+      yd[i] = v;
+    }
+    // packed Hermitian C: up += C dn, dn += C up
+    CloverIO<P, 72>::load(c, s, 36 * b, 36, cl);
+    for (int i = 0; i < 6; i++) {
+      yu[i] = yu[i] + zd{(double)cl[i], 0.0} * xd[i];
+      yd[i] = yd[i] + zd{(double)cl[i], 0.0} * xu[i];
+    }
+    for (int i = 1; i < 6; i++)
+      for (int j = 0; j < i; j++) {
+        const int od = i * (i - 1) / 2 + j;
+        const zd a = {(double)cl[6 + 2 * od], (double)cl[7 + 2 * od]};
+        yu[i] = yu[i] + a * xd[j];
+        yu[j] = yu[j] + conj(a) * xd[i];
+        yd[i] = yd[i] + a * xu[j];
+        yd[j] = yd[j] + conj(a) * xu[i];
+      }
+    for (int i = 0; i < 6; i++) {
+      const int e = ((2 * b + i / 3) * 3 + i % 3) * 2;
+      ou[e] = yu[i].re;
+      ou[e + 1] = yu[i].im;
+      od[e] = yd[i].re;
+      od[e + 1] = yd[i].im;
+    }
+  }
+  for (int e = 0; e < 24; e++) {
+    up[e] = (T)ou[e];
+    dn[e] = (T)od[e];
+  }
+  SpinorIO<P>::store(out, 2 * k, s, up);
+  SpinorIO<P>::store(out, 2 * k + 1, s, dn);
+}
+
 template <typename Pin, typename Q>
 __global__ void clover_convert_kernel(Geom geo, const void *in, int vpc_in, void *out, int vpc_out, long long stride,
                                       int nr)
@@ -326,6 +394,21 @@ void launch_clover_invert(int prec_in, int prec_out, Geom geo, const void *in, l
   QPX_IN_SWITCH(prec_in, QPX_OUT_SWITCH(prec_out, (clover_invert_kernel<Pin, Q><<<grid, 64, 0, st>>>(
                                                        geo, in, stride, vpc_in, o0, o1, vpc_out, mode, mu, o2,
                                                        vpc_out2, eps))));
+}
+
+void launch_two_flav_clover(int prec, int vh, int npairs, SpinorArg out, SpinorArg in, CloverArg fa, CloverArg fb,
+                            CloverArg c, cudaStream_t st)
+{
+  dim3 grid((unsigned)((vh + 63) / 64), (unsigned)npairs);
+  switch (prec) {
+  case PREC_F64: two_flav_clover_kernel<F64><<<grid, 64, 0, st>>>(vh, npairs, out, in, fa, fb, c); break;
+  case PREC_F32: two_flav_clover_kernel<F32><<<grid, 64, 0, st>>>(vh, npairs, out, in, fa, fb, c); break;
+  case PREC_F16: two_flav_clover_kernel<F16><<<grid, 64, 0, st>>>(vh, npairs, out, in, fa, fb, c); break;
+  case PREC_BF16: two_flav_clover_kernel<BF16><<<grid, 64, 0, st>>>(vh, npairs, out, in, fa, fb, c); break;
+  case PREC_Q16: two_flav_clover_kernel<Q16><<<grid, 64, 0, st>>>(vh, npairs, out, in, fa, fb, c); break;
+  case PREC_Q16F32: two_flav_clover_kernel<Q16F32><<<grid, 64, 0, st>>>(vh, npairs, out, in, fa, fb, c); break;
+  default: throw Error(QPHIX_GPU_EINVAL, "bad precision");
+  }
 }
 
 void launch_clover_convert(int prec_in, int prec_out, Geom geo, const void *in, int vpc_in, void *out, int vpc_out,

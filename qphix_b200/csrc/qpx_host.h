@@ -179,6 +179,8 @@ void launch_clover_build(int recon, int prec_out, Geom geo, GaugeArg g, void *ou
 void launch_clover_invert(int prec_in, int prec_out, Geom geo, const void *in, long long stride, int vpc_in, void *o0,
                           void *o1, int vpc_out, int mode, double mu, dim3 grid, cudaStream_t st, void *o2 = nullptr,
                           int vpc_out2 = 0, double eps = 0.0);
+void launch_two_flav_clover(int prec, int vh, int npairs, SpinorArg out, SpinorArg in, CloverArg fa, CloverArg fb,
+                            CloverArg c, cudaStream_t st);
 void launch_clover_convert(int prec_in, int prec_out, Geom geo, const void *in, int vpc_in, void *out, int vpc_out,
                            long long stride, int nr, dim3 grid, cudaStream_t st);
 

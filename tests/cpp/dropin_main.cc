@@ -176,6 +176,19 @@ int main(int argc, char **argv)
       nccg(nres, nin, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
       write_from("out_ndccg_up", nres[0], sbytes);
       write_from("out_ndccg_dn", nres[1], sbytes);
+      // 7c. the Dslash-level two-flavour members on (psi, chi)
+      const Geometry<double, 4, 2, true>::FourSpinorBlock *swp[2] = {chi, psi};
+      TMClovDslash<double, 4, 2, true> TC(&geom, -1.0, 1.0, 1.0, nullptr, nullptr, nd[1]);
+      TC.two_flav_inverse_clover_term(nres, nin, finv, odiag, 1);
+      write_from("out_2f_inv_up", nres[0], sbytes);
+      write_from("out_2f_inv_dn", nres[1], sbytes);
+      TC.two_flav_AChiMinusBDPsi(nres, nin, swp, F.u[1], F.A_odd, 0.25, nd[2], 1, 1);
+      write_from("out_2f_clachi_up", nres[0], sbytes);
+      write_from("out_2f_clachi_dn", nres[1], sbytes);
+      TMDslash<double, 4, 2, true> TD(&geom, -1.0, 1.0, 1.0, nd[0], nd[1]);
+      TD.two_flav_AChiMinusBDPsi(nres, nin, swp, F.u[1], 4.0 + nd[0], 0.25, nd[2], -1, 1);
+      write_from("out_2f_tmachi_up", nres[0], sbytes);
+      write_from("out_2f_tmachi_dn", nres[1], sbytes);
       geom.free(odiag);
       geom.free(finv[0]);
       geom.free(finv[1]);

@@ -91,6 +91,20 @@ def test_cpp_dropin(tmp_path, oracle):
     xn = np.stack([load("out_ndccg_up"), load("out_ndccg_dn")])
     r = pair - NC.apply(NC.apply(xn, 1), -1)
     assert np.linalg.norm(r) / np.linalg.norm(pair) < 2e-10
+    # Dslash-level two-flavour members (tm_clov_dslash_def.h:76-110, tm_dslash_def.h)
+    got = np.stack([load("out_2f_inv_up"), load("out_2f_inv_dn")])
+    ref = np.stack([oracle.fullclover_apply(psi, ndc_fu) + oracle.clover_apply(chi, ndc_c),
+                    oracle.fullclover_apply(chi, ndc_fd) + oracle.clover_apply(psi, ndc_c)])
+    assert rel_l2(got, ref) < 1e-13
+    got = np.stack([load("out_2f_clachi_up"), load("out_2f_clachi_dn")])
+    ref = np.stack([oracle.clov_achimbdpsi(L, psi, chi, s["gauge"], s["clov"][1], 0.25, nd[1], 1, 1) - nd[2] * psi,
+                    oracle.clov_achimbdpsi(L, chi, psi, s["gauge"], s["clov"][1], 0.25, -nd[1], 1, 1) - nd[2] * chi])
+    assert rel_l2(got, ref) < 1e-13
+    got = np.stack([load("out_2f_tmachi_up"), load("out_2f_tmachi_dn")])
+    al = 4.0 + nd[0]
+    ref = np.stack([oracle.tm_achimbdpsi(L, psi, chi, s["gauge"], al, 0.25, nd[0], nd[1], -1, 1, 1.0) - nd[2] * psi,
+                    oracle.tm_achimbdpsi(L, chi, psi, s["gauge"], al, 0.25, nd[0], nd[1], -1, 1, -1.0) - nd[2] * chi])
+    assert rel_l2(got, ref) < 1e-13
     # BLAS of blas_new_c.h on host arrays
     sc = np.fromfile(d / "out_blas_scalars")
     assert abs(sc[0] - np.vdot(psi, psi).real) < 1e-12 * sc[0]
