@@ -5,9 +5,9 @@
 // side per thread, reduces them over the block (warp shuffles, then a fixed
 // order over warps, one barrier for all values), writes one partial per
 // (block, rhs, value), and the last block to finish (atomic ticket) folds the
-// partials -- warp w takes values w, w + 4, ...; lane l adds site blocks
-// l, l + 32, ... in order, then the warp's shuffle tree -- and runs a
-// finalize step on thread 0.  The order of every addition is fixed by the
+// partials -- four values at a time, thread t adds site blocks t, t + 128,
+// ... in order, then a shuffle tree per warp and the warps in order -- and
+// runs a finalize step on thread 0.  The order of every addition is fixed by the
 // launch shape, so results are bitwise reproducible run to run.
 //
 // The finalize step updates a SolverState in device memory (Krylov scalars
@@ -136,18 +136,34 @@ __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, SolverState
   __syncthreads();
   if (!am_last) return;
   __threadfence();
-  // last block: fold the partials of every site block, the values spread
-  // over the warps so that their loads are in flight together
-  const int gx = nsblocks;
-  const long long row = (long long)nrhs * ra.nval;
-  for (int idx = wid; idx < nrhs * ra.nval; idx += NW) {
-    double acc = 0;
+  // last block: fold the partials of every site block.  All threads split
+  // the site blocks, four values at a time, so that many loads are in flight
+  // even when a launch reduces only a few values over thousands of blocks.
+  __shared__ double wsum[NW][4];
+  const int gx = nsblocks, nres = nrhs * ra.nval;
+  const long long row = (long long)nres;
+  for (int v0 = 0; v0 < nres; v0 += 4) {
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 4
-    for (int b = lane; b < gx; b += 32) acc += __ldcg(ra.partials + b * row + idx);
-    acc = warp_sum(acc);
-    if (lane == 0) ra.result[idx] = acc;
+    for (int b = threadIdx.x; b < gx; b += QPX_BLOCK) {
+      const double *p = ra.partials + b * row + v0;
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        if (v0 + j < nres) acc[j] += __ldcg(p + j);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const double s = warp_sum(acc[j]);
+      if (lane == 0) wsum[wid][j] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4 && v0 + (int)threadIdx.x < nres) {
+      double s = 0.0;
+      for (int w = 0; w < NW; w++) s += wsum[w][threadIdx.x];
+      ra.result[v0 + threadIdx.x] = s;
+    }
+    __syncthreads();
   }
-  __syncthreads();
   if (threadIdx.x == 0) {
     *ra.ticket = 0u;
     __threadfence();
