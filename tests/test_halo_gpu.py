@@ -133,3 +133,23 @@ def test_halo_refuses_twisted_phases_and_two_flavours(api, setup):
     assert L._lib.qphix_gpu_dslash_halo(C.byref(p), y.h, x.h, u.h, None, None, 1, 0, C.byref(f)) != 0
     p = api.op_params(L.NDTM, mass=0.1, twisted_mass=0.2, epsilon=0.1)
     assert L._lib.qphix_gpu_dslash_halo(C.byref(p), y.h, x.h, u.h, None, None, 1, 0, C.byref(f)) != 0
+
+
+def test_slab_operator_with_exchange_faces_one_slab(api, setup):
+    """The per-rank path (SlabOperator with exchange_faces) on one slab: the
+    exchange returns the slab's own faces, so the operator must equal the
+    one-GPU clover operator."""
+    s = setup
+    slab = halo.TSlab(DIMS, 1, 0)
+    lat = api.Lattice(slab.dims)
+    u = lat.gauge("f64", 12).upload(s["gauge"])
+    A = lat.clover().upload(s["clov"][1])
+    Ai = lat.clover().upload(s["invclov"][0])
+    p = api.op_params(L.CLOVER_OP, -1.0, *ANISO)
+    M = halo.SlabOperator(slab, lat, p, u, lambda f, l: halo.exchange_faces(f, l, slab), clov=A, invclov=Ai)
+    x = lat.spinor().upload(F.gaussian_spinor(DIMS, 9))
+    y, z = lat.spinor(), lat.spinor()
+    for isign in (1, -1):
+        M(y, x, isign, 1)
+        api.EvenOddCloverOperator(u, A, Ai, -1.0, *ANISO)(z, x, isign, 1)
+        assert rel_l2(y.download(), z.download()) < 1e-14
