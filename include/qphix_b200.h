@@ -219,7 +219,9 @@ int qphix_gpu_clover_apply(qphix_gpu_field res, qphix_gpu_field chi, qphix_gpu_f
  * *_halo Dslash entry points, which take every other hop from the slab.  The
  * t boundary condition applies on the slabs holding the global edges.
  * side 0 = first slice (sent to the previous slab), 1 = last slice (sent to
- * the next slab). */
+ * the next slab).  The packs are asynchronous on the field's lattice stream
+ * (synchronise it before another stream or rank reads the buffer); dst must
+ * hold qphix_gpu_halo_spinor_bytes / _link_bytes. */
 typedef struct {
   const void *psi_fwd;    /* the next slab's side-0 pack of the hopped field   */
   const void *psi_bwd;    /* the previous slab's side-1 pack of it             */
