@@ -235,3 +235,53 @@ class LocalSlabs:
             self.achimbdpsi(ops, outs, tmps, ins, 4.0 + p.mass, 0.25, isign, target_cb)
         else:
             self.achimbdpsi(ops, outs, tmps, ins, 0.0, 0.25, isign, target_cb)
+
+
+
+def cg(apply, x, b, rsd_target, max_iters, allreduce=None):
+    """CG on M^+ M over the slabs of a t-cut lattice, with the recurrence of
+    include/qphix/invcg.h:160-340, one right-hand side per field.  x and b
+    are lists of this process's slab fields (one per slab it holds);
+    apply(outs, ins, isign) applies the even-odd operator on them (exchanging
+    faces); allreduce(v) sums a float over the ranks (None: one process holds
+    every slab, e.g. LocalSlabs).  Norms are summed over the slabs, so every
+    rank takes the same steps.  Returns (iterations, |r|^2 / |b|^2)."""
+    if any(f.nrhs != 1 for f in list(x) + list(b)):
+        raise ValueError("the slab CG takes one right-hand side per field")
+    red = allreduce or (lambda v: v)
+
+    def fresh():
+        return [api.Field(f.lat, L.SPINOR, f.prec, 0, 1) for f in x]
+
+    r, p, mp, mmp = fresh(), fresh(), fresh(), fresh()
+
+    def norm(fs):
+        return float(red(sum(float(api.norm2(f)[0]) for f in fs)))
+
+    bn = norm(b)
+    apply(mp, x, 1)
+    apply(mmp, mp, -1)
+    for rr, bb, mm, pp in zip(r, b, mmp, p):
+        api.copy(rr, bb)
+        api.caxpby(-1.0, mm, 1.0, rr)  # r = b - M^+ M x
+        api.copy(pp, rr)
+    c = norm(r)
+    target = rsd_target * rsd_target * bn
+    it = 0
+    while c > target and it < max_iters:
+        apply(mp, p, 1)
+        apply(mmp, mp, -1)
+        a = c / norm(mp)
+        for xx, rr, pp, mm in zip(x, r, p, mmp):
+            api.caxpby(a, pp, 1.0, xx)
+            api.caxpby(-a, mm, 1.0, rr)
+        cp = norm(r)
+        it += 1
+        if cp <= target:
+            c = cp
+            break
+        beta = cp / c
+        for pp, rr in zip(p, r):
+            api.caxpby(1.0, rr, beta, pp)  # p = r + beta p
+        c = cp
+    return it, c / bn if bn > 0 else 0.0

@@ -153,3 +153,25 @@ def test_slab_operator_with_exchange_faces_one_slab(api, setup):
         M(y, x, isign, 1)
         api.EvenOddCloverOperator(u, A, Ai, -1.0, *ANISO)(z, x, isign, 1)
         assert rel_l2(y.download(), z.download()) < 1e-14
+
+
+@pytest.mark.parametrize("nslabs", [2, 4])
+def test_slab_cg_matches_one_gpu_cg(api, oracle, setup, nslabs):
+    """CG on M^+ M with the clover operator over 2 / 4 slabs (faces exchanged
+    every application, norms summed over the slabs) converges like the one-GPU
+    solver: the same iteration count (within one), the true residual below the
+    target, and the solutions equal to 1e-8."""
+    s = setup
+    ls = halo.LocalSlabs(DIMS, nslabs)
+    ops = _ops(api, ls, s, "clover", "f64", 1)
+    b = F.gaussian_spinor(DIMS, 11)
+    bs = [lat.spinor().upload(sl.cut_spinor(b)) for sl, lat in zip(ls.slabs, ls.lats)]
+    xs = [lat.spinor() for lat in ls.lats]
+    it, rr = halo.cg(lambda outs, ins, isign: ls.eo_apply(ops, outs, ins, isign, 1), xs, bs, 1e-10, 2000)
+    x = np.concatenate([f.download() for f in xs])
+    O = _oracle_op(oracle, s, "clover", 1)
+    r = b - O.apply(O.apply(x, 1), -1)
+    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10 and rr < 1e-20
+    xo, io = oracle.cg(O, b, 1e-10, 2000)
+    assert abs(it - io.n_iters) <= 1, (it, io.n_iters)
+    assert rel_l2(x, xo) < 1e-8
