@@ -17,7 +17,9 @@ transport's job:
   are read where they lie), which checks the halo path against the whole
   lattice.
 
-Only the operators are distributed; the solvers run on one GPU.
+The even-odd operators and a CG on M^+ M (`cg`, norms summed over the slabs
+with a pluggable all-reduce) run distributed; the graph-captured solvers of
+the library run on one GPU.
 """
 from __future__ import annotations
 
