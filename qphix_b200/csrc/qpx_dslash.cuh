@@ -153,6 +153,62 @@ __device__ __forceinline__ void project(const T *psi, cx<T> h[2][3])
   }
 }
 
+// The same projection on FP16 storage, one site per thread: the raw half2
+// words (re, im of spin s, colour c in word 3 s + c) are combined in half
+// precision -- i p = (-p.im, p.re) is a half swap -- and only the 12 results
+// are widened to FP32, instead of the 24 inputs.  Each sum adds one FP16
+// rounding to inputs that already carry the FP16 storage error.
+template <int MU, int SG>
+__device__ __forceinline__ void project_h2(const __half2 w[12], cx<float> h[2][3])
+{
+  const __half2 isg = __floats2half2_rn(-(float)SG, (float)SG);  // SG i p = swap(p) (-SG, SG)
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const __half2 p0 = w[c], p1 = w[3 + c], p2 = w[6 + c], p3 = w[9 + c];
+    __half2 h0, h1;
+    if (MU == 0) {  // h0 = p0 + SG i p3, h1 = p1 + SG i p2
+      h0 = __hfma2(__lowhigh2highlow(p3), isg, p0);
+      h1 = __hfma2(__lowhigh2highlow(p2), isg, p1);
+    } else if (MU == 1) {  // h0 = p0 - SG p3, h1 = p1 + SG p2
+      h0 = SG > 0 ? __hsub2(p0, p3) : __hadd2(p0, p3);
+      h1 = SG > 0 ? __hadd2(p1, p2) : __hsub2(p1, p2);
+    } else if (MU == 2) {  // h0 = p0 + SG i p2, h1 = p1 - SG i p3
+      h0 = __hfma2(__lowhigh2highlow(p2), isg, p0);
+      h1 = __hfma2(__lowhigh2highlow(p3), __hneg2(isg), p1);
+    } else {  // h0 = p0 + SG p2, h1 = p1 + SG p3
+      h0 = SG > 0 ? __hadd2(p0, p2) : __hsub2(p0, p2);
+      h1 = SG > 0 ? __hadd2(p1, p3) : __hsub2(p1, p3);
+    }
+    const float2 f0 = __half22float2(h0), f1 = __half22float2(h1);
+    h[0][c] = {f0.x, f0.y};
+    h[1][c] = {f1.x, f1.y};
+  }
+}
+
+// the FP16 one-site path's loads for project_h2: the 12 raw words and the norm
+__device__ __forceinline__ void load_h2(const SpinorArg &f, int rhs, long long s, __half2 w[12], float &nrm)
+{
+  const uint4 *p = reinterpret_cast<const uint4 *>(f.data) + rhs * f.rhs_stride_chunks + s;
+  nrm = __ldg(f.norm + rhs * f.stride + s);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const uint4 d = __ldg(p + k * f.stride);
+    w[4 * k] = *reinterpret_cast<const __half2 *>(&d.x);
+    w[4 * k + 1] = *reinterpret_cast<const __half2 *>(&d.y);
+    w[4 * k + 2] = *reinterpret_cast<const __half2 *>(&d.z);
+    w[4 * k + 3] = *reinterpret_cast<const __half2 *>(&d.w);
+  }
+}
+
+template <typename Lane>
+struct HalfProjection {
+  static constexpr bool value = false;
+};
+template <>
+struct HalfProjection<Lanes<F16, 1>> {
+  static constexpr bool value = true;
+};
+
 // --- reconstruct-accumulate of (1 + SG gamma_mu) from chi = U h -------------
 // QPX_ADD(k, v): acc[k] += SG v ; QPX_SUB(k, v): acc[k] -= SG v (signs
 // resolved at compile time)
@@ -478,10 +534,17 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
       const cx<T> ph = {splat<T>(a.tbc[MU][0]), splat<T>(a.tbc[MU][1])};                  \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
-        T psi[24], nrm;                                                                   \
-        L::load_raw(ghf ? a.ghost_fwd : a.in, rhs0 + r, ixf, psi, nrm);                   \
+        T nrm;                                                                            \
         cx<T> h[2][3], ch[2][3];                                                          \
-        project<MU, -ISIGN>(psi, h);                                                      \
+        if constexpr (HalfProjection<L>::value) {                                         \
+          __half2 w[12];                                                                  \
+          load_h2(ghf ? a.ghost_fwd : a.in, rhs0 + r, ixf[0], w, nrm);                    \
+          project_h2<MU, -ISIGN>(w, h);                                                   \
+        } else {                                                                          \
+          T psi[24];                                                                      \
+          L::load_raw(ghf ? a.ghost_fwd : a.in, rhs0 + r, ixf, psi, nrm);                 \
+          project<MU, -ISIGN>(psi, h);                                                    \
+        }                                                                                 \
         if (tw || SP == 2) { /* SP = 2: the folded form costs registers (spills) */       \
           scale_h(h, cf * nrm, tw, ph);                                                   \
           link_mult<false>(u, h, ch);                                                     \
@@ -513,10 +576,17 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
       const cx<T> ph = {splat<T>(a.tbc[MU][0]), splat<T>(-a.tbc[MU][1])};                 \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
-        T psi[24], nrm;                                                                   \
-        L::load_raw(ghb ? a.ghost_bwd : a.in, rhs0 + r, ixb, psi, nrm);                   \
+        T nrm;                                                                            \
         cx<T> h[2][3], ch[2][3];                                                          \
-        project<MU, ISIGN>(psi, h);                                                       \
+        if constexpr (HalfProjection<L>::value) {                                         \
+          __half2 w[12];                                                                  \
+          load_h2(ghb ? a.ghost_bwd : a.in, rhs0 + r, ixb[0], w, nrm);                    \
+          project_h2<MU, ISIGN>(w, h);                                                    \
+        } else {                                                                          \
+          T psi[24];                                                                      \
+          L::load_raw(ghb ? a.ghost_bwd : a.in, rhs0 + r, ixb, psi, nrm);                 \
+          project<MU, ISIGN>(psi, h);                                                     \
+        }                                                                                 \
         if (tw || SP == 2) { /* SP = 2: the folded form costs registers (spills) */       \
           scale_h(h, cf * nrm, tw, ph);                                                   \
           link_mult<true>(u, h, ch);                                                      \
