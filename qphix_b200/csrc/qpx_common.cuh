@@ -605,20 +605,44 @@ struct CloverIO<Q16F32, NR> : CloverIO<F32, NR> {};
 // ---------------------------------------------------------------------------
 // lattice geometry as seen by a kernel
 // ---------------------------------------------------------------------------
+// Division by a divisor fixed at launch, as a multiply-high, an add and a
+// shift (Granlund and Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, section 4): for 1 <= d < 2^31 and
+// 0 <= n < 2^31, with l = ceil(log2 d) and m = floor(2^32 (2^l - d) / d) + 1
+// (m < 2^32), n / d = (umulhi(m, n) + n) >> l, and the sum stays below 2^32.
+// A run-time integer division costs a few tens of instructions instead.
+struct DivU {
+  uint32_t m;
+  int l;
+};
+inline DivU make_divu(int d)
+{
+  int l = 0;
+  while ((1ull << l) < (unsigned long long)d) l++;
+  const unsigned long long m =
+      ((1ull << 32) * ((1ull << l) - (unsigned long long)d)) / (unsigned long long)d + 1;
+  return DivU{(uint32_t)m, l};
+}
+__device__ __forceinline__ int div_by(int n, DivU d)
+{
+  return (int)((__umulhi(d.m, (uint32_t)n) + (uint32_t)n) >> d.l);
+}
+
 struct Geom {
   int nx, ny, nz, nt, nxh;
   int vh;
+  DivU div_nxh, div_ny, div_nz;  // make_divu of nxh, ny, nz
 };
 
 __device__ __forceinline__ void site_coords(const Geom &g, int s, int cb, int &xh, int &y, int &z,
                                             int &t, int &par)
 {
-  xh = s % g.nxh;
-  int r = s / g.nxh;
-  y = r % g.ny;
-  r /= g.ny;
-  z = r % g.nz;
-  t = r / g.nz;
+  const int r = div_by(s, g.div_nxh);
+  xh = s - r * g.nxh;
+  const int r2 = div_by(r, g.div_ny);
+  y = r - r2 * g.ny;
+  t = div_by(r2, g.div_nz);
+  z = r2 - t * g.nz;
   par = (y + z + t + cb) & 1;  // x = 2 xh + par
 }
 

@@ -86,6 +86,9 @@ struct qphix_gpu_lattice_s {
     g.nt = dims[3];
     g.nxh = nxh;
     g.vh = (int)vh;
+    g.div_nxh = qpx::make_divu(nxh);
+    g.div_ny = qpx::make_divu(dims[1]);
+    g.div_nz = qpx::make_divu(dims[2]);
     return g;
   }
 };
