@@ -17,8 +17,9 @@ well.
 value  = solves/s with the right-hand sides resident in HBM
 e2e    = solves/s through the C ABI with host buffers: pinned host -> device
          upload of the sources, solve, device -> host download of x per step
-roofline: the dominant kernel (the FP16 clover Dslash of the inner solve),
-         timed alone on the same lattice with L2 flushed before every launch.
+roofline: the dominant kernel (the FP16 clover Dslash A chi - b D psi of the
+         inner solve), timed alone on the same lattice with L2 flushed before
+         every launch; the operator's first kernel (A^-1 D psi) beside it.
 cpu_baseline: the CPU oracle (FP64 clover BiCGStab iterations) on the host
          cores, scaled to a full solve by the FP64 iteration count.
 
@@ -402,12 +403,15 @@ def main():
                 "status": inf["status"]}
 
     # ---- roofline: the FP16 clover Dslash kernel (inner solve), L2 flushed ------
-    def dslash_roofline(dims, prec, nrhs, n=20):
-        """The FP16 clover Dslash A^-1 D psi (the first kernel of every inner
-        operator application) in the solve's own launch configuration, timed
-        alone with CUDA events on the lattice's stream, L2 flushed before
-        every launch.  Algorithmic bytes per site: nrhs x (input + output
-        spinor) + 8 links (12 reals) + the packed clover inverse (72 reals)."""
+    def dslash_roofline(dims, prec, nrhs, n=20, achi=False):
+        """One FP16 clover Dslash of the inner operator in the solve's launch
+        configuration, timed alone with CUDA events on the lattice's stream,
+        L2 flushed before every launch: A^-1 D psi (the operator's first
+        kernel) or, with achi, A chi - b D psi on the odd checkerboard (its
+        second kernel, the larger share of the solve; in the solve it also
+        carries the fused reductions, which this timing leaves out).
+        Algorithmic bytes per site: nrhs x (input + output spinor, + chi) +
+        8 links (12 reals) + the packed clover term (72 reals)."""
         from qphix_b200 import fields as F
         lat2 = lat if dims == DIMS else api.Lattice(dims, device=local)
         if dims != DIMS:
@@ -415,20 +419,29 @@ def main():
         # a larger lattice: the C2 links tiled (link values do not change timing)
         g = inputs["gauge"] if dims == DIMS else np.tile(inputs["gauge"], (1, 1, F.vh(dims) // F.vh(DIMS), 1, 1))
         u = lat2.gauge(prec, 12).upload(g)
-        cl = lat2.clover(prec).upload(inputs["invclov_even"] if dims == DIMS else
-                                      np.tile(inputs["invclov_even"][:1], (F.vh(dims), 1, 1)))
+        ckey = "clov_odd" if achi else "invclov_even"
+        cl = lat2.clover(prec).upload(inputs[ckey] if dims == DIMS else
+                                      np.tile(inputs[ckey][:1], (F.vh(dims), 1, 1)))
         psi = lat2.spinor(prec, nrhs).upload(np.stack([F.gaussian_spinor(dims, 3 + i) for i in range(nrhs)]))
         out = lat2.spinor(prec, nrhs)
+        chi = (lat2.spinor(prec, nrhs).upload(np.stack([F.gaussian_spinor(dims, 40 + i) for i in range(nrhs)]))
+               if achi else None)
         D = api.ClovDslash(lat2, -1.0, 1.0, 1.0)
+
+        def launch():
+            if achi:
+                D.dslashAChiMinusBDPsi(out, psi, chi, u, cl, 0.25, 1, 1)
+            else:
+                D.dslash(out, psi, u, cl, 1, 0)
         for _ in range(3):
-            D.dslash(out, psi, u, cl, 1, 0)
+            launch()
         durs = []
         for _ in range(n):
             with torch.cuda.stream(stream):
                 flush.fill_(1)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            D.dslash(out, psi, u, cl, 1, 0)
+            launch()
             e1.record(stream)
             torch.cuda.synchronize()
             durs.append(e0.elapsed_time(e1) / 1e3)
@@ -436,21 +449,28 @@ def main():
         esize = {"f16": 2, "bf16": 2, "q16": 2, "q16f32": 2, "f32": 4, "f64": 8}[prec]
         lsize = 4 if prec == "q16f32" else esize  # links and clover
         norm = 4 if prec in ("f16", "bf16", "q16", "q16f32") else 0
-        per_site = nrhs * 2 * (24 * esize + norm) + 8 * 12 * lsize + 72 * lsize
+        per_site = nrhs * (3 if achi else 2) * (24 * esize + norm) + 8 * 12 * lsize + 72 * lsize
         t = statistics.mean(durs)
         return per_site, vh, t
 
     peak, peak_kind = peaks()
-    per_site, vh, t = dslash_roofline(DIMS, args.inner, B)
+    per_site, vh, t = dslash_roofline(DIMS, args.inner, B, achi=True)
     achieved = per_site * vh / t / 1e9
-    traffic = profile_traffic().get(f"clover_dslash_{args.inner}_12_{'x'.join(map(str, DIMS))}_n{B}")
+    traffic = profile_traffic().get(f"clover_achi_{args.inner}_12_{'x'.join(map(str, DIMS))}_n{B}")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
             "traffic": (round(traffic * vh) if traffic else None),
-            "kernel": f"clover Dslash A^-1 D psi, {args.inner} storage, 12-real links, {B} rhs per launch "
-                      f"(the inner operator's first kernel, as launched in the solve)",
+            "kernel": f"clover Dslash A chi - b D psi, {args.inner} storage, 12-real links, {B} rhs per launch "
+                      f"(the inner operator's second kernel and the solve's largest share, timed without "
+                      f"its fused reductions; traffic from the in-solve launch)",
             "bytes_per_site": per_site, "sites": vh, "nrhs": B, "launch_us": round(t * 1e6, 2),
             "note": "the 16^3x32 working set fits in L2 within a solve; L2 is flushed before each timed launch"}
+    ps1, _, t1 = dslash_roofline(DIMS, args.inner, B)
+    traffic1 = profile_traffic().get(f"clover_dslash_{args.inner}_12_{'x'.join(map(str, DIMS))}_n{B}")
+    roof_first = {"kernel": f"clover Dslash A^-1 D psi, {args.inner} storage, {B} rhs (the operator's first kernel)",
+                  "bytes_per_site": ps1, "achieved": round(ps1 * vh / t1 / 1e9, 1),
+                  "frac": round(ps1 * vh / t1 / 1e9 / peak, 4), "launch_us": round(t1 * 1e6, 2),
+                  "traffic": (round(traffic1 * vh) if traffic1 else None)}
     big = (32, 32, 32, 64)
     ps2, vh2, t2 = dslash_roofline(big, args.inner, 1, n=10)
     traffic2 = profile_traffic().get(f"clover_dslash_{args.inner}_12_32x32x32x64_n1")
@@ -477,7 +497,7 @@ def main():
             "data": "synthetic (seeded)", "config": config_dict(B, args.inner, args.solver, args.inner_recon, args.delta),
             "e2e": {"value": round(e2e_value, 3), "unit": "solves/s", "h2d_bytes_per_step": bytes_io,
                     "d2h_bytes_per_step": bytes_io},
-            "roofline": roof, "roofline_large_lattice": roof_big,
+            "roofline": roof, "roofline_first_kernel": roof_first, "roofline_large_lattice": roof_big,
             "cpu_baseline": cpu, "gpu_launches": int(n_launch),
             "clocks": clk,
             "p50_ms_per_step": round(p[len(p) // 2], 3), "p99_ms_per_step": round(p[min(len(p) - 1, int(0.99 * len(p)))], 3),
