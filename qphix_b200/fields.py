@@ -408,6 +408,39 @@ class QPhiXLayout:
                 out[self.g_block, slot, :, :, 1, self.g_lane] = mt.imag
         return out
 
+    def unpack_gauge(self, blocks):
+        """Forward links U_mu(x) [4, Vh, 3, 3] of a checkerboard from its
+        blocked array (slots 2mu + 1); with 12-real storage the third row of
+        U^T (the third column stored) is rebuilt as conj(row0 x row1) of the
+        transposed matrix, as the kernels do (codegen/dslash_common.cc:1895-1913)."""
+        a = np.asarray(blocks, dtype=np.float64)
+        nc = 2 if self.c12 else 3
+        out = np.empty((4, vh(self.dims), 3, 3), dtype=np.complex128)
+        for mu in range(4):
+            mt = a[self.g_block, 2 * mu + 1, :, :, 0, self.g_lane] + 1j * a[self.g_block, 2 * mu + 1, :, :, 1,
+                                                                             self.g_lane]
+            full = np.empty((mt.shape[0], 3, 3), dtype=np.complex128)
+            full[:, :nc] = mt
+            if nc == 2:
+                full[:, 2] = np.conj(np.cross(mt[:, 0], mt[:, 1]))
+            out[mu] = np.swapaxes(full, -1, -2)
+        return out
+
+    def unpack_back_gauge(self, blocks):
+        """Backward links [4, Vh, 3, 3] stored with a checkerboard (slots 2mu):
+        entry mu of site x is U_mu(x - mu), a link of the other checkerboard."""
+        a = np.asarray(blocks, dtype=np.float64)
+        nc = 2 if self.c12 else 3
+        out = np.empty((4, vh(self.dims), 3, 3), dtype=np.complex128)
+        for mu in range(4):
+            mt = a[self.g_block, 2 * mu, :, :, 0, self.g_lane] + 1j * a[self.g_block, 2 * mu, :, :, 1, self.g_lane]
+            full = np.empty((mt.shape[0], 3, 3), dtype=np.complex128)
+            full[:, :nc] = mt
+            if nc == 2:
+                full[:, 2] = np.conj(np.cross(mt[:, 0], mt[:, 1]))
+            out[mu] = np.swapaxes(full, -1, -2)
+        return out
+
     # clover: struct {diag1[6][V], off_diag1[15][2][V], diag2[6][V], off_diag2[15][2][V]}
     def pack_clover(self, packed, dtype=np.float64):
         out = np.zeros((self.n_gauge_blocks, 72, self.V), dtype=dtype)

@@ -1,4 +1,5 @@
-"""Generates tests/golden/reference_pin.npz from the reference's own code.
+"""Generates tests/golden/reference_pin.npz and reference_dslash_pin.npz from
+the reference's own code.
 
 Run in a checkout that has the reference sources (oracle/ref/Makefile builds
 oracle/_ref/libqphix_ref.so from them).  The fixture records, on seeded
@@ -6,6 +7,12 @@ inputs: the reference clover products (packed and full 6x6), BLAS results,
 and the reference CG / BiCGStab / MR / Richardson / multishift-CG solves
 driven with the oracle's even-odd clover operator.  tests/test_oracle_pin.py
 checks the oracle against this file wherever the reference is absent.
+
+reference_dslash_pin.npz holds fingerprints (norm and three seeded
+projections) of the outputs of QPhiX's code-generated Dslash family and
+even-odd operators (scalar build of oracle/ref/codegen.mk, 18-real links,
+antiperiodic t) for every kind, call, isign and checkerboard of
+tests/test_reference_dslash_pin.py.
 """
 import os
 import subprocess
@@ -63,7 +70,28 @@ def main():
     out["minv_x"], out["minv_iters"], out["minv_rsd"], out["minv_mv"] = np.stack(xs), it, fin, mv
     np.savez_compressed(os.path.join(HERE, "reference_pin.npz"), **out)
     print("wrote", os.path.join(HERE, "reference_pin.npz"))
+    dslash_fingerprints()
+
+
+def dslash_fingerprints():
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle", "ref"), "-f", "codegen.mk",
+                           "ISA=scalar", "-j8"])
+    import oracle as O
+    import ref_dslash as R
+    import test_reference_dslash_pin as T
+    s, psi, chi, probes = T._golden_inputs()
+    RL = R.RefLattice(T.DIMS, "double", "scalar", compress12=False, nthreads=4)
+    gp = RL.gauge(s["gauge"])
+    out = {}
+    for name, kind, op, isign, cb in T.golden_cases():
+        ref, _ = T.case(R, RL, O, s, kind, op, isign, cb, -1.0, (1.0, 1.0), psi, chi, gp)
+        out[name] = T.project(ref, probes)
+    np.savez_compressed(os.path.join(HERE, "reference_dslash_pin.npz"), **out)
+    print("wrote", os.path.join(HERE, "reference_dslash_pin.npz"))
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["--dslash"]:
+        dslash_fingerprints()
+    else:
+        main()
