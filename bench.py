@@ -11,8 +11,8 @@ mixed-precision scheme, InvRichardsonMultiPrec: FP64 outer defect correction
 FP32-arithmetic fields reducing each correction's residual by delta = 0.005.
 `--solver ru` selects BiCGStab with reliable updates (delta 0.03) instead;
 the other solver, and the default solver with a Q16 inner operator, are timed
-beside it.  The plain FP64 BiCGStab solve of the same system is timed as
-well.
+beside it.  Plain FP64 BiCGStab is timed on the same 8-rhs block (the ratio's
+denominator) and on one rhs at a time.
 
 value  = solves/s with the right-hand sides resident in HBM
 e2e    = solves/s through the C ABI with host buffers: pinned host -> device
@@ -20,8 +20,10 @@ e2e    = solves/s through the C ABI with host buffers: pinned host -> device
 roofline: the dominant kernel (the FP16 clover Dslash A chi - b D psi of the
          inner solve), timed alone on the same lattice with L2 flushed before
          every launch; the operator's first kernel (A^-1 D psi) beside it.
-cpu_baseline: the CPU oracle (FP64 clover BiCGStab iterations) on the host
-         cores, scaled to a full solve by the FP64 iteration count.
+cpu_baseline: QPhiX's own CPU path (its code-generated AVX-512 kernels and
+         InvRichardsonMultiPrec / InvBiCGStab, built from the reference
+         sources) solving one right-hand side of the same system to 1e-10 on
+         all host cores; --impl reference times the same solves per step.
 
 N > 1 GPUs: independent replicas (the path does not shard across GPUs here);
 value = all ranks' solves / max-over-ranks time.
@@ -146,48 +148,135 @@ def profile_traffic():
 
 
 # ---------------------------------------------------------------------------
-def cpu_oracle_sample(inputs, dims, n_iter_fp64, max_sample_iters=3):
-    """FP64 clover BiCGStab on the host cores (the CPU oracle), a bounded
-    number of iterations, scaled to a full solve by the FP64 iteration count."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-    L = O.make_lattice(dims, -1.0)
-    op = O.OracleOp("clover", L, inputs["gauge"], clov=inputs["clov_odd"],
-                    invclov=inputs["invclov_even"])
-    b = inputs["rhs"][0]
-    t0 = time.perf_counter()
-    _, info = O.bicgstab(op, b, 1e-30, max_sample_iters)
-    dt = time.perf_counter() - t0
-    per_iter = dt / max(1, max_sample_iters)
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    solve_s = per_iter * max(1, n_iter_fp64)
-    return {"value": 1.0 / solve_s, "unit": "solves/s", "cores": cores, "kind": "port",
-            "sample": f"{max_sample_iters} FP64 clover BiCGStab iterations on {'x'.join(map(str, dims))} "
-                      f"({dt:.1f} s), scaled to a {n_iter_fp64}-iteration solve"}
+REF_DELTA = 0.01  # the reference's fastest Richardson delta on this workload
+
+
+class ReferenceCPU:
+    """QPhiX's own CPU implementation of the path on the host cores: its
+    code-generated AVX-512 (else scalar) Dslash kernels behind its
+    EvenOddCloverOperator, InvBiCGStab and InvRichardsonMultiPrec templates,
+    compiled from the reference sources (oracle/_ref, oracle/ref/codegen.mk).
+    Without that build, the CPU oracle's port of the same solver stands in
+    (kind "port")."""
+
+    def __init__(self, inputs, dims):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        self.inputs, self.dims = inputs, dims
+        self.cores = os.cpu_count() or 1
+        self.model = _cpu_model()
+        import ref_dslash as R
+        self.isa = "avx512" if R.available("avx512") else ("scalar" if R.available("scalar") else None)
+        if self.isa is None:
+            self.kind = "port"
+            return
+        self.kind = "reference"
+        self.R = R
+        vo, so, vi, si = (8, 8, 16, 8) if self.isa == "avx512" else (1, 1, 1, 1)
+        self.layouts = f"double V={vo} S={so}, float V={vi} S={si}, 12-real links"
+        self.outer = R.RefLattice(dims, "double", self.isa, vo, so, True, self.cores)
+        self.inner = R.RefLattice(dims, "float", self.isa, vi, si, True, self.cores)
+        self.fo = self._fields(self.outer)
+        self.fi = self._fields(self.inner)
+        self.p = R.params(t_boundary=-1.0)
+
+    def _fields(self, RL):
+        g = RL.gauge(self.inputs["gauge"])
+        return [g[0], g[1], RL.clover(self.inputs["clov_odd"]), RL.clover(self.inputs["invclov_even"]), None]
+
+    def mixed(self, rhs):
+        """one full InvRichardsonMultiPrec<double, float> solve to 1e-10:
+        (seconds, outer iterations, relative residual, operator applications)"""
+        if self.kind == "port":
+            return self.fp64(rhs)
+        x, it, fin, mv, sec = self.outer.solve_richardson(self.inner, "clover", rhs, self.fo, self.fi, p=self.p,
+                                                          rsd=RSD, delta=REF_DELTA, max_iters=100,
+                                                          inner_max=5000)
+        return sec, it, float(np.sqrt(max(fin, 0.0))), mv
+
+    def fp64(self, rhs):
+        """one full FP64 InvBiCGStab solve to 1e-10 (same tuple)"""
+        if self.kind == "port":
+            import oracle as O
+            L = O.make_lattice(self.dims, -1.0)
+            op = O.OracleOp("clover", L, self.inputs["gauge"], clov=self.inputs["clov_odd"],
+                            invclov=self.inputs["invclov_even"])
+            t0 = time.perf_counter()
+            _, info = O.bicgstab(op, rhs, RSD, 5000)
+            sec = time.perf_counter() - t0
+            return sec, info.n_iters, float(np.sqrt(max(info.rsd_sq_final, 0.0)) / np.linalg.norm(rhs)), \
+                info.mv_apps
+        c = self.fo
+        x, it, fin, mv, sec = self.outer.solve("clover", "bicgstab", rhs, c[:2], c=(c[2], c[3], None), p=self.p,
+                                               rsd=RSD, max_iters=5000)
+        return sec, it, float(np.sqrt(max(fin, 0.0)) / np.linalg.norm(rhs)), mv
+
+    def describe(self, what):
+        if self.kind == "port":
+            return (f"{what} by the CPU oracle's port of include/qphix/invbicgstab.h (the reference's own "
+                    f"build is absent), {self.cores} OpenMP threads, {self.model}")
+        return (f"{what}: QPhiX's own code-generated {self.isa} kernels and solver templates "
+                f"({self.layouts}), {self.cores} OpenMP threads, {self.model}")
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown CPU"
+
+
+def cpu_baseline_leg(inputs, dims, repeats=2):
+    """The bench line's cpu_baseline: full single-rhs solves of the headline
+    system by the reference on the host cores (mixed precision, its
+    InvRichardsonMultiPrec, is the value; FP64 InvBiCGStab beside it)."""
+    ref = ReferenceCPU(inputs, dims)
+    rhs = inputs["rhs"][0]
+    ref.mixed(rhs)  # first call: page-in and thread start-up
+    runs = [ref.mixed(rhs) for _ in range(repeats)]
+    sec = statistics.median(r[0] for r in runs)
+    f64 = ref.fp64(rhs)
+    what = (f"{repeats} full InvRichardsonMultiPrec<double, float> solves (inner BiCGStab, delta {REF_DELTA}) of "
+            f"one rhs of the headline system to 1e-10 (median)") if ref.kind == "reference" else \
+        f"{repeats} full FP64 BiCGStab solves of one rhs to 1e-10 (median)"
+    return {"value": 1.0 / sec, "unit": "solves/s", "cores": ref.cores, "kind": ref.kind,
+            "sample": ref.describe(what), "isa": ref.isa,
+            "mixed": {"seconds": sec, "outer_iters": runs[-1][1], "rel_resid": runs[-1][2], "mv_apps": runs[-1][3]},
+            "fp64_bicgstab": {"solves_per_s": 1.0 / f64[0], "iters": f64[1], "rel_resid": f64[2],
+                              "mv_apps": f64[3]}}
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the CPU implementation of the path on the host cores."""
+    """--impl reference: QPhiX's own CPU implementation of the path on the
+    host cores (rank 0 only).  One step = one full solve to 1e-10 of one of
+    the headline system's right-hand sides (the reference has no multi-rhs
+    solver) with its mixed-precision InvRichardsonMultiPrec<double, float>;
+    value = solves / summed solver time."""
     if rank != 0:
         return
-    inputs = make_inputs(DIMS, 1)
-    n_fp64 = int(os.environ.get("QPHIX_BENCH_FP64_ITERS", "110"))
-    vals = []
-    for _ in range(args.warmup):
-        cpu_oracle_sample(inputs, DIMS, n_fp64, 1)
-    for _ in range(args.steps):
-        vals.append(cpu_oracle_sample(inputs, DIMS, n_fp64, 2))
-    v = statistics.median([x["value"] for x in vals])
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "data": "synthetic", "config": config_dict(args.batch, args.inner, args.solver, args.inner_recon,
-                                                        args.delta),
-            "reference_path": "the same system solved by FP64 clover BiCGStab on the CPU (oracle port of "
-                              "include/qphix/invbicgstab.h), one rhs at a time; a bounded sample of "
-                              "iterations scaled to a full solve",
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": vals[-1]["cores"], "kind": "port",
-                             "sample": vals[-1]["sample"]},
-            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    inputs = make_inputs(DIMS, args.batch)
+    ref = ReferenceCPU(inputs, DIMS)
+    for i in range(args.warmup):
+        ref.mixed(inputs["rhs"][i % args.batch])
+    runs = [ref.mixed(inputs["rhs"][i % args.batch]) for i in range(args.steps)]
+    total = sum(r[0] for r in runs)
+    v = args.steps / total
+    f64 = ref.fp64(inputs["rhs"][0])
+    what = (f"each step one full InvRichardsonMultiPrec<double, float> solve (inner BiCGStab, delta {REF_DELTA}) "
+            f"of one rhs to 1e-10" if ref.kind == "reference" else "each step one full FP64 BiCGStab solve")
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total * 1e3 / args.steps, 3),
+            "higher_is_better": True, "data": "synthetic (seeded)",
+            "config": config_dict(args.batch, args.inner, args.solver, args.inner_recon, args.delta),
+            "reference_path": ref.describe(what),
+            "worst_rel_resid": max(r[2] for r in runs), "outer_iters": runs[-1][1], "mv_apps": runs[-1][3],
+            "fp64_bicgstab": {"solves_per_s": round(1.0 / f64[0], 4), "iters": f64[1], "rel_resid": f64[2]},
+            "cpu_baseline": {"value": round(v, 4), "unit": "solves/s", "cores": ref.cores, "kind": ref.kind,
+                             "sample": ref.describe(what)},
+            "e2e": {"value": round(v, 4), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -380,36 +469,45 @@ def main():
                     "iters": qinf[0]["n_iters"], "mv_apps": qinf[0]["mv_apps"]}
 
     # ---- plain FP64 BiCGStab beside it ------------------------------------------
-    fp64 = None
+    fp64 = fp64_1 = None
     if not args.no_fp64:
+        bic = api.InvBiCGStab(M64, 5000)
+
+        def time_fp64(bf, xf, reps):
+            api.zero(xf)
+            infs = bic(xf, bf, RSD)
+            ts = []
+            for _ in range(reps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(1)
+                api.zero(xf)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                infs = bic(xf, bf, RSD)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            ms = statistics.median(ts)
+            n = len(infs)
+            return {"rhs_per_solve": n, "solves_per_s": n * 1e3 / ms, "ms_per_block": ms,
+                    "iters": max(i["n_iters"] for i in infs),
+                    "true_rel_resid": max(i["true_rel_resid"] for i in infs),
+                    "status": max(i["status"] for i in infs)}
+        # like for like: the same 8-rhs block the mixed solver takes
+        fp64 = time_fp64(b_res, x, max(2, min(args.steps, 4)))
         b1 = lat.spinor("f64", 1).upload(inputs["rhs"][0])
         x1 = lat.spinor("f64", 1)
-        bic = api.InvBiCGStab(M64, 5000)
-        api.zero(x1)
-        inf = bic(x1, b1, RSD)[0]
-        ts = []
-        for _ in range(max(2, min(args.steps, 5))):
-            with torch.cuda.stream(stream):
-                flush.fill_(1)
-            api.zero(x1)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            inf = bic(x1, b1, RSD)[0]
-            e1.record(stream)
-            torch.cuda.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        fp64 = {"solves_per_s": 1e3 / statistics.median(ts), "ms_per_solve": statistics.median(ts),
-                "iters": inf["n_iters"], "true_rel_resid": inf["true_rel_resid"],
-                "status": inf["status"]}
+        fp64_1 = time_fp64(b1, x1, max(2, min(args.steps, 5)))
 
     # ---- roofline: the FP16 clover Dslash kernel (inner solve), L2 flushed ------
-    def dslash_roofline(dims, prec, nrhs, n=20, achi=False):
+    def dslash_roofline(dims, prec, nrhs, n=20, achi=False, reduce=False):
         """One FP16 clover Dslash of the inner operator in the solve's launch
         configuration, timed alone with CUDA events on the lattice's stream,
         L2 flushed before every launch: A^-1 D psi (the operator's first
         kernel) or, with achi, A chi - b D psi on the odd checkerboard (its
-        second kernel, the larger share of the solve; in the solve it also
-        carries the fused reductions, which this timing leaves out).
+        second kernel, the larger share of the solve); with reduce, carrying
+        the reductions BiCGStab fuses into its t = M s launch (|t|^2 and
+        <t, s>, folded on the device, no host round trip) as in the solve.
         Algorithmic bytes per site: nrhs x (input + output spinor, + chi) +
         8 links (12 reals) + the packed clover term (72 reals)."""
         from qphix_b200 import fields as F
@@ -429,7 +527,9 @@ def main():
         D = api.ClovDslash(lat2, -1.0, 1.0, 1.0)
 
         def launch():
-            if achi:
+            if achi and reduce:
+                D.dslashAChiMinusBDPsiNorms(out, psi, chi, u, cl, 0.25, 1, 1, fetch=False)
+            elif achi:
                 D.dslashAChiMinusBDPsi(out, psi, chi, u, cl, 0.25, 1, 1)
             else:
                 D.dslash(out, psi, u, cl, 1, 0)
@@ -454,16 +554,18 @@ def main():
         return per_site, vh, t
 
     peak, peak_kind = peaks()
-    per_site, vh, t = dslash_roofline(DIMS, args.inner, B, achi=True)
+    per_site, vh, t = dslash_roofline(DIMS, args.inner, B, achi=True, reduce=True)
+    _, _, t_nored = dslash_roofline(DIMS, args.inner, B, achi=True)
     achieved = per_site * vh / t / 1e9
     traffic = profile_traffic().get(f"clover_achi_{args.inner}_12_{'x'.join(map(str, DIMS))}_n{B}")
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
             "traffic": (round(traffic * vh) if traffic else None),
             "kernel": f"clover Dslash A chi - b D psi, {args.inner} storage, 12-real links, {B} rhs per launch "
-                      f"(the inner operator's second kernel and the solve's largest share, timed without "
-                      f"its fused reductions; traffic from the in-solve launch)",
+                      f"(the inner operator's second kernel and the solve's largest share), with the |t|^2 and "
+                      f"<t, s> reductions fused into it as in the solve; traffic from the in-solve launch",
             "bytes_per_site": per_site, "sites": vh, "nrhs": B, "launch_us": round(t * 1e6, 2),
+            "launch_us_without_reductions": round(t_nored * 1e6, 2),
             "note": "the 16^3x32 working set fits in L2 within a solve; L2 is flushed before each timed launch"}
     ps1, _, t1 = dslash_roofline(DIMS, args.inner, B)
     traffic1 = profile_traffic().get(f"clover_dslash_{args.inner}_12_{'x'.join(map(str, DIMS))}_n{B}")
@@ -480,9 +582,8 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1:
-        n_fp64 = fp64["iters"] if fp64 else 110
         try:
-            cpu = cpu_oracle_sample(inputs, DIMS, n_fp64)
+            cpu = cpu_baseline_leg(inputs, DIMS)
         except Exception as e:  # pragma: no cover
             cpu = {"value": None, "error": str(e)}
 
@@ -503,6 +604,8 @@ def main():
             "p50_ms_per_step": round(p[len(p) // 2], 3), "p99_ms_per_step": round(p[min(len(p) - 1, int(0.99 * len(p)))], 3),
             "fp64_plain": fp64,
             "mixed_vs_fp64_solves_ratio": (round(value / world / fp64["solves_per_s"], 3) if fp64 else None),
+            "fp64_plain_1rhs": fp64_1,
+            "mixed_vs_fp64_1rhs_solves_ratio": (round(value / world / fp64_1["solves_per_s"], 3) if fp64_1 else None),
             "solver": {"kind": "bicgstab_reliable_update" if args.solver == "ru" else "richardson_bicgstab",
                        "delta": args.delta, "iters": outer_iters, "mv_apps": mv_apps,
                        "worst_true_rel_resid": worst_resid, "all_converged": converged},

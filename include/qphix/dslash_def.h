@@ -1,10 +1,12 @@
 // Drop-in Dslash family: Dslash (reference: include/qphix/dslash_def.h:27-58),
 // ClovDslash (clover_dslash_def.h:24-53), TMDslash (tm_dslash_def.h:23-49)
 // and TMClovDslash (tm_clov_dslash_def.h:30-66), same constructors and
-// member functions.  Each call moves its host arrays (QPhiX layout) to the
-// device, runs one sm_100a kernel and moves the result back; `u` is the
-// gauge array of the target checkerboard, as in QPhiX (its eight links per
-// site carry both hop directions).
+// member functions.  Each call moves its spinor arrays (QPhiX layout) to the
+// device, runs one sm_100a kernel and moves the result back; the gauge and
+// clover arrays are uploaded on first use and kept on the device for later
+// calls with the same arrays (invalidateFieldCache()).  `u` is the gauge
+// array of the target checkerboard, as in QPhiX (its eight links per site
+// carry both hop directions).
 #pragma once
 
 #include "qphix/geometry.h"
@@ -43,21 +45,21 @@ class Dslash
 
   void dslash(FourSpinorBlock *res, const FourSpinorBlock *psi, const SU3MatrixBlock *u, int isign, int cb)
   {
-    auto g = gpu::upload_gauge_cb(*s, u, cb);
+    qphix_gpu_field g = gauge_dev(u, cb);
     auto in = s->upload_spinor(psi);
     gpu::Field out(s->lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
-    gpu::check(qphix_gpu_dslash(&p, out.get(), in.get(), g.get(), nullptr, nullptr, isign, cb), "dslash");
+    gpu::check(qphix_gpu_dslash(&p, out.get(), in.get(), g, nullptr, nullptr, isign, cb), "dslash");
     s->download_spinor(out, res);
   }
 
   void dslashAChiMinusBDPsi(FourSpinorBlock *res, const FourSpinorBlock *psi, const FourSpinorBlock *chi,
                             const SU3MatrixBlock *u, double alpha, double beta, int isign, int cb)
   {
-    auto g = gpu::upload_gauge_cb(*s, u, cb);
+    qphix_gpu_field g = gauge_dev(u, cb);
     auto in = s->upload_spinor(psi);
     auto x = s->upload_spinor(chi);
     gpu::Field out(s->lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
-    gpu::check(qphix_gpu_dslash_achimbdpsi(&p, out.get(), in.get(), x.get(), g.get(), nullptr, alpha, beta, isign,
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&p, out.get(), in.get(), x.get(), g, nullptr, alpha, beta, isign,
                                            cb, 1.0),
                "dslashAChiMinusBDPsi");
     s->download_spinor(out, res);
@@ -65,19 +67,42 @@ class Dslash
 
   void dslashDir(FourSpinorBlock *res, const FourSpinorBlock *psi, const SU3MatrixBlock *u, int cb, int dir)
   {
-    auto g = gpu::upload_gauge_cb(*s, u, cb);
+    qphix_gpu_field g = gauge_dev(u, cb);
     auto in = s->upload_spinor(psi);
     gpu::Field out(s->lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
-    gpu::check(qphix_gpu_dslash_dir(&p, out.get(), in.get(), g.get(), cb, dir), "dslashDir");
+    gpu::check(qphix_gpu_dslash_dir(&p, out.get(), in.get(), g, cb, dir), "dslashDir");
     s->download_spinor(out, res);
   }
 
   void free(void *) {}
   Geom &getGeometry() { return *s; }
 
+  // Device copies of the gauge and clover arrays passed to this object are
+  // kept between calls (keyed by the host array's address; an array released
+  // through Geometry::free is never matched again).  A caller that rewrites
+  // one of those arrays in place and calls again must call this first.  Not
+  // part of QPhiX's interface (its kernels read the host arrays directly).
+  void invalidateFieldCache() { cache_.clear(); }
+
  protected:
+  typedef typename Geom::CloverBlock CloverBlock_;
+  typedef typename Geom::FullCloverBlock FullCloverBlock_;
+  qphix_gpu_field gauge_dev(const SU3MatrixBlock *u, int cb)
+  {
+    return cache_.get(u, cb, [&] { return gpu::upload_gauge_cb(*s, u, cb); });
+  }
+  qphix_gpu_field clover_dev(const CloverBlock_ *c)
+  {
+    return cache_.get(c, 2, [&] { return s->upload_clover(c); });
+  }
+  qphix_gpu_field full_clover_dev(const FullCloverBlock_ *c)
+  {
+    return cache_.get(c, 3, [&] { return s->upload_full_clover(c); });
+  }
+
   Geom *s;
   qphix_gpu_op_params p;
+  gpu::FieldCache cache_;
 };
 
 template <typename FT, int veclen, int soalen, bool compress12>
@@ -103,11 +128,11 @@ class ClovDslash : public Dslash<FT, veclen, soalen, compress12>
               int isign, int cb)
   {
     Geom &s = *this->s;
-    auto g = gpu::upload_gauge_cb(s, u, cb);
-    auto c = s.upload_clover(invclov);
+    qphix_gpu_field g = this->gauge_dev(u, cb);
+    qphix_gpu_field c = this->clover_dev(invclov);
     auto in = s.upload_spinor(psi);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
-    gpu::check(qphix_gpu_dslash(&this->p, out.get(), in.get(), g.get(), c.get(), nullptr, isign, cb), "clover dslash");
+    gpu::check(qphix_gpu_dslash(&this->p, out.get(), in.get(), g, c, nullptr, isign, cb), "clover dslash");
     s.download_spinor(out, res);
   }
 
@@ -116,12 +141,12 @@ class ClovDslash : public Dslash<FT, veclen, soalen, compress12>
                             const SU3MatrixBlock *u, const CloverBlock *clov, const double beta, int isign, int cb)
   {
     Geom &s = *this->s;
-    auto g = gpu::upload_gauge_cb(s, u, cb);
-    auto c = s.upload_clover(clov);
+    qphix_gpu_field g = this->gauge_dev(u, cb);
+    qphix_gpu_field c = this->clover_dev(clov);
     auto in = s.upload_spinor(psi);
     auto x = s.upload_spinor(chi);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
-    gpu::check(qphix_gpu_dslash_achimbdpsi(&this->p, out.get(), in.get(), x.get(), g.get(), c.get(), 0.0, beta, isign,
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&this->p, out.get(), in.get(), x.get(), g, c, 0.0, beta, isign,
                                            cb, 1.0),
                "clover dslashAChiMinusBDPsi");
     s.download_spinor(out, res);
@@ -130,10 +155,10 @@ class ClovDslash : public Dslash<FT, veclen, soalen, compress12>
   void clovMult(FourSpinorBlock *res, const FourSpinorBlock *chi, const CloverBlock *clov)
   {
     Geom &s = *this->s;
-    auto c = s.upload_clover(clov);
+    qphix_gpu_field c = this->clover_dev(clov);
     auto x = s.upload_spinor(chi);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
-    gpu::check(qphix_gpu_clover_apply(out.get(), x.get(), c.get()), "clovMult");
+    gpu::check(qphix_gpu_clover_apply(out.get(), x.get(), c), "clovMult");
     s.download_spinor(out, res);
   }
 };
@@ -168,11 +193,11 @@ class TMDslash : public Dslash<FT, veclen, soalen, compress12>
                             const double musign = 1.0)
   {
     Geom &s = *this->s;
-    auto g = gpu::upload_gauge_cb(s, u, cb);
+    qphix_gpu_field g = this->gauge_dev(u, cb);
     auto in = s.upload_spinor(psi);
     auto x = s.upload_spinor(chi);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
-    gpu::check(qphix_gpu_dslash_achimbdpsi(&this->p, out.get(), in.get(), x.get(), g.get(), nullptr, alpha, beta,
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&this->p, out.get(), in.get(), x.get(), g, nullptr, alpha, beta,
                                            isign, cb, musign),
                "tm dslashAChiMinusBDPsi");
     s.download_spinor(out, res);
@@ -185,14 +210,14 @@ class TMDslash : public Dslash<FT, veclen, soalen, compress12>
                                double beta, double epsilon, int isign, int cb)
   {
     Geom &s = *this->s;
-    auto g = gpu::upload_gauge_cb(s, u, cb);
+    qphix_gpu_field g = this->gauge_dev(u, cb);
     auto in = s.upload_flavours(psi);
     auto x = s.upload_flavours(chi);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0, 2);
     qphix_gpu_op_params q = this->p;
     q.kind = QPHIX_GPU_NDTM;
     q.epsilon = epsilon;
-    gpu::check(qphix_gpu_dslash_achimbdpsi(&q, out.get(), in.get(), x.get(), g.get(), nullptr, alpha, beta, isign,
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&q, out.get(), in.get(), x.get(), g, nullptr, alpha, beta, isign,
                                            cb, 1.0),
                "tm two_flav_AChiMinusBDPsi");
     s.download_flavours(out, res);
@@ -225,12 +250,12 @@ class TMClovDslash : public Dslash<FT, veclen, soalen, compress12>
   {
     if (fl != 0 && fl != 1) throw std::invalid_argument("TMClovDslash: flavour must be 0 (up) or 1 (down)");
     Geom &s = *this->s;
-    auto g = gpu::upload_gauge_cb(s, u, cb);
-    auto f0 = s.upload_full_clover(invclov[fl]);
-    auto f1 = s.upload_full_clover(invclov[1 - fl]);
+    qphix_gpu_field g = this->gauge_dev(u, cb);
+    qphix_gpu_field f0 = this->full_clover_dev(invclov[fl]);
+    qphix_gpu_field f1 = this->full_clover_dev(invclov[1 - fl]);
     auto in = s.upload_spinor(psi);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
-    gpu::check(qphix_gpu_dslash(&this->p, out.get(), in.get(), g.get(), f0.get(), f1.get(), isign, cb),
+    gpu::check(qphix_gpu_dslash(&this->p, out.get(), in.get(), g, f0, f1, isign, cb),
                "tm clover dslash");
     s.download_spinor(out, res);
   }
@@ -243,14 +268,14 @@ class TMClovDslash : public Dslash<FT, veclen, soalen, compress12>
   {
     if (fl != 0 && fl != 1) throw std::invalid_argument("TMClovDslash: flavour must be 0 (up) or 1 (down)");
     Geom &s = *this->s;
-    auto g = gpu::upload_gauge_cb(s, u, cb);
-    auto c = s.upload_clover(clov);
+    qphix_gpu_field g = this->gauge_dev(u, cb);
+    qphix_gpu_field c = this->clover_dev(clov);
     auto in = s.upload_spinor(psi);
     auto x = s.upload_spinor(chi);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0);
     qphix_gpu_op_params q = this->p;
     if (fl == 1) q.prec_mass_rho = -q.prec_mass_rho;
-    gpu::check(qphix_gpu_dslash_achimbdpsi(&q, out.get(), in.get(), x.get(), g.get(), c.get(), 0.0, beta, isign, cb,
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&q, out.get(), in.get(), x.get(), g, c, 0.0, beta, isign, cb,
                                            1.0),
                "tm clover dslashAChiMinusBDPsi");
     s.download_spinor(out, res);
@@ -265,11 +290,11 @@ class TMClovDslash : public Dslash<FT, veclen, soalen, compress12>
   {
     Geom &s = *this->s;
     auto in = s.upload_flavours(psi);
-    auto f0 = s.upload_full_clover(fcl[0]);
-    auto f1 = s.upload_full_clover(fcl[1]);
-    auto c = s.upload_clover(clOffDiag);
+    qphix_gpu_field f0 = this->full_clover_dev(fcl[0]);
+    qphix_gpu_field f1 = this->full_clover_dev(fcl[1]);
+    qphix_gpu_field c = this->clover_dev(clOffDiag);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0, 2);
-    gpu::check(qphix_gpu_two_flav_clover_apply(out.get(), in.get(), f0.get(), f1.get(), c.get(), isign),
+    gpu::check(qphix_gpu_two_flav_clover_apply(out.get(), in.get(), f0, f1, c, isign),
                "two_flav_inverse_clover_term");
     s.download_flavours(out, res);
   }
@@ -281,8 +306,8 @@ class TMClovDslash : public Dslash<FT, veclen, soalen, compress12>
                                const double beta, const double epsilon, const int isign, const int cb)
   {
     Geom &s = *this->s;
-    auto g = gpu::upload_gauge_cb(s, u, cb);
-    auto c = s.upload_clover(clov);
+    qphix_gpu_field g = this->gauge_dev(u, cb);
+    qphix_gpu_field c = this->clover_dev(clov);
     auto in = s.upload_flavours(psi);
     auto x = s.upload_flavours(chi);
     gpu::Field out(s.lattice(), QPHIX_GPU_SPINOR, Geom::device_prec(), 0, 2);
@@ -290,7 +315,7 @@ class TMClovDslash : public Dslash<FT, veclen, soalen, compress12>
     q.kind = QPHIX_GPU_NDTMCLOVER;
     q.twisted_mass = this->p.prec_mass_rho;
     q.epsilon = epsilon;
-    gpu::check(qphix_gpu_dslash_achimbdpsi(&q, out.get(), in.get(), x.get(), g.get(), c.get(), 0.0, beta, isign, cb,
+    gpu::check(qphix_gpu_dslash_achimbdpsi(&q, out.get(), in.get(), x.get(), g, c, 0.0, beta, isign, cb,
                                            1.0),
                "tm clover two_flav_AChiMinusBDPsi");
     s.download_flavours(out, res);

@@ -117,9 +117,21 @@ class Geometry
   {
     if (p) std::free(p - 1);
   }
-  void free(SU3MatrixBlock *p) { std::free(p); }
-  void free(CloverBlock *p) { std::free(p); }
-  void free(FullCloverBlock *p) { std::free(p); }
+  void free(SU3MatrixBlock *p)
+  {
+    ++gpu::host_field_epoch();
+    std::free(p);
+  }
+  void free(CloverBlock *p)
+  {
+    ++gpu::host_field_epoch();
+    std::free(p);
+  }
+  void free(FullCloverBlock *p)
+  {
+    ++gpu::host_field_epoch();
+    std::free(p);
+  }
 
   // ---- device side (not part of QPhiX's interface) --------------------------
   qphix_gpu_lattice lattice() const { return lat_; }

@@ -5,10 +5,12 @@
 // operation on the GPU through the C ABI in qphix_b200.h.
 #pragma once
 
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <stdexcept>
 #include <string>
+#include <vector>
 
 #include "../qphix_b200.h"
 
@@ -74,6 +76,50 @@ class Field
 
  private:
   qphix_gpu_field h_ = nullptr;
+};
+
+// Host gauge / clover arrays released through Geometry::free bump this
+// counter, so a device copy cached under an array's address is never reused
+// for a later allocation that lands at the same address.
+inline std::atomic<unsigned long> &host_field_epoch()
+{
+  static std::atomic<unsigned long> epoch{0};
+  return epoch;
+}
+
+// Device copies of the operator fields (gauge checkerboards, clover terms) a
+// Dslash object was handed, kept across its calls while the host array's
+// address and host_field_epoch() are unchanged: a caller that applies the
+// Dslash in a loop uploads its links once.  A caller that rewrites such an
+// array in place calls clear() (Dslash::invalidateFieldCache()).
+class FieldCache
+{
+ public:
+  template <typename Make>
+  qphix_gpu_field get(const void *host, int tag, Make &&make)
+  {
+    const unsigned long ep = host_field_epoch().load();
+    for (auto &e : entries_)
+      if (e.host == host && e.tag == tag && e.epoch == ep) return e.f.get();
+    std::vector<Entry> keep;  // drop copies of an older epoch
+    for (auto &e : entries_)
+      if (e.epoch == ep) keep.push_back(std::move(e));
+    entries_ = std::move(keep);
+    if (entries_.size() >= kMax) entries_.erase(entries_.begin());
+    entries_.push_back(Entry{host, tag, ep, make()});
+    return entries_.back().f.get();
+  }
+  void clear() { entries_.clear(); }
+
+ private:
+  static constexpr size_t kMax = 8;
+  struct Entry {
+    const void *host;
+    int tag;
+    unsigned long epoch;
+    Field f;
+  };
+  std::vector<Entry> entries_;
 };
 
 class EoOp

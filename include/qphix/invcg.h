@@ -11,6 +11,10 @@ namespace QPhiX
 
 namespace gpu
 {
+// solver kind of InvMRSmoother (a fixed number of MR iterations), beside the
+// QPHIX_GPU_SOLVER_* kinds of the C ABI
+constexpr int MR_SMOOTHER = 100;
+
 // Op::num_flav = 2 (two-flavour operators): x and rhs are (up, down) pairs,
 // solved as one system on a device field of two right-hand sides
 template <typename FT, int V, int S, bool C, typename Op>
@@ -41,6 +45,8 @@ class DeviceSolver : public AbstractSolver<FT, V, S, C, Op::num_flav>
       rc = qphix_gpu_solve_cg(M.gpu_op(), dx.get(), db.get(), rsd, MaxIters, isign, cb, infos);
     else if (kind == QPHIX_GPU_SOLVER_BICGSTAB)
       rc = qphix_gpu_solve_bicgstab(M.gpu_op(), dx.get(), db.get(), rsd, MaxIters, isign, cb, infos);
+    else if (kind == MR_SMOOTHER)  // RsdTarget is not a stopping test here (invmr.h:330-335)
+      rc = qphix_gpu_solve_mr_smoother(M.gpu_op(), dx.get(), db.get(), MaxIters, omega, isign, cb, infos);
     else
       rc = qphix_gpu_solve_mr(M.gpu_op(), dx.get(), db.get(), rsd, MaxIters, omega, isign, cb, infos);
     check(rc, "solver");
@@ -55,7 +61,8 @@ class DeviceSolver : public AbstractSolver<FT, V, S, C, Op::num_flav>
   }
 
   Geometry<FT, V, S, C> &getGeometry() override { return M.getGeometry(); }
-  int gpu_solver_kind() const override { return kind; }
+  // the smoother is not offered as the inner solver of InvRichardsonMultiPrec
+  int gpu_solver_kind() const override { return kind == MR_SMOOTHER ? -1 : kind; }
   qphix_gpu_eo_op gpu_solver_op() const override { return M.gpu_op(); }
   int gpu_max_iters() const override { return MaxIters; }
 
@@ -101,6 +108,21 @@ class InvMR : public gpu::DeviceSolver<FT, V, S, compress12, EvenOddLinearOperat
   InvMR(EvenOddLinearOperatorBase &M_, int MaxIters_, double Omega)
       : gpu::DeviceSolver<FT, V, S, compress12, EvenOddLinearOperatorBase>(M_, MaxIters_, QPHIX_GPU_SOLVER_MR,
                                                                             Omega)
+  {
+  }
+};
+
+// InvMRSmoother (reference invmr.h:294-354): exactly MaxIters MR iterations
+// with over-relaxation Omega and no residual test; n_iters = MaxIters and
+// rsd_sq_final = -1, as the reference's InvMRBase reports with
+// terminateOnResiduum = false.
+template <typename FT, int V, int S, bool compress12,
+          typename EvenOddLinearOperatorBase = EvenOddLinearOperator<FT, V, S, compress12>>
+class InvMRSmoother : public gpu::DeviceSolver<FT, V, S, compress12, EvenOddLinearOperatorBase>
+{
+ public:
+  InvMRSmoother(EvenOddLinearOperatorBase &M_, int MaxIters_, double Omega)
+      : gpu::DeviceSolver<FT, V, S, compress12, EvenOddLinearOperatorBase>(M_, MaxIters_, gpu::MR_SMOOTHER, Omega)
   {
   }
 };

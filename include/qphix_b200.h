@@ -194,6 +194,17 @@ int qphix_gpu_dslash_achimbdpsi(const qphix_gpu_op_params *p, qphix_gpu_field re
                                 double beta, int isign, int cb, double musign);
 int qphix_gpu_dslash_dir(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
                          qphix_gpu_field gauge, int cb, int dir);
+/* qphix_gpu_dslash_achimbdpsi with the reductions the solvers fuse into its
+ * epilogue (no counterpart in the reference, which calls norm2Spinor /
+ * innerProduct of blas_new_c.h:278,520 on the result in separate passes):
+ * per rhs r, in this order, out[nval r + 0] = |res_r|^2, then, when w is
+ * given, <w_r, res_r> (re, im), then <res_r, chi_r> (re, im); nval = 3, or 5
+ * with w.  Inner products are sum conj(first) second.  out == NULL leaves
+ * the values in the lattice's device result buffer (no host round trip). */
+int qphix_gpu_dslash_achimbdpsi_norms(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                                      qphix_gpu_field chi, qphix_gpu_field gauge, qphix_gpu_field aux,
+                                      double alpha, double beta, int isign, int cb, double musign, qphix_gpu_field w,
+                                      double *out);
 /* Two-flavour twisted-mass clover hop: the Wilson hop of both flavours of
  * each (up, down) pair followed by the two-flavour inverse clover term --
  * Dslash::dslash then TMClovDslash::two_flav_inverse_clover_term
@@ -358,10 +369,15 @@ int qphix_gpu_blas_inner_product_norm(qphix_gpu_field x, qphix_gpu_field y, doub
  * the nrhs results are written to out_dev, a device buffer of nrhs doubles
  * owned by the caller, asynchronously on the lattice's stream (synchronise it
  * before reading).  Limit: ceil(volcb / 128) * nrhs <= 65536, else
- * QPHIX_GPU_EINVAL.  The field's device must be the current device.  The
- * first call on a device looks up the array's device address; make that
- * first call before any stream capture.  Every call shares the array, so
- * calls whose kernels overlap on the GPU race. */
+ * QPHIX_GPU_EINVAL.  The field's device must be the current device, and
+ * out_dev device (or managed) memory of it; a host pointer is rejected with
+ * QPHIX_GPU_EINVAL before anything is launched.  The first call on a device
+ * looks up the array's device address; make that first call before any
+ * stream capture.  Under CUDA's lazy module loading (the default since CUDA
+ * 12.2) that first call is also when the device reserves the 512 KiB, so make
+ * it before the caller's allocator takes the free HBM (or set
+ * CUDA_MODULE_LOADING=EAGER).  Every call shares the array, so calls whose
+ * kernels overlap on the GPU race. */
 int qphix_gpu_blas_norm2_noalloc(qphix_gpu_field x, double *out_dev);
 
 /* ---- serving layer (no reference counterpart: the reference is a library

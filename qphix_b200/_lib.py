@@ -93,6 +93,7 @@ _SIGS = {
     "qphix_gpu_field_convert": ([P, P, D], I_),
     "qphix_gpu_dslash": ([C.POINTER(OpParams), P, P, P, P, P, I_, I_], I_),
     "qphix_gpu_dslash_achimbdpsi": ([C.POINTER(OpParams), P, P, P, P, P, D, D, I_, I_, D], I_),
+    "qphix_gpu_dslash_achimbdpsi_norms": ([C.POINTER(OpParams), P, P, P, P, P, D, D, I_, I_, D, P, P], I_),
     "qphix_gpu_dslash_dir": ([C.POINTER(OpParams), P, P, P, I_, I_], I_),
     "qphix_gpu_halo_spinor_bytes": ([P, C.POINTER(C.c_size_t)], I_),
     "qphix_gpu_halo_pack_spinor": ([P, I_, P], I_),

@@ -270,6 +270,17 @@ class ClovDslash(Dslash):
     def clovMult(self, res, chi, clov):
         check(L._lib.qphix_gpu_clover_apply(res.h, chi.h, clov.h))
 
+    def dslashAChiMinusBDPsiNorms(self, res, psi, chi, u, clov, beta, isign, cb, w=None, fetch=True):
+        """dslashAChiMinusBDPsi with its fused reductions (the solvers'
+        launch): per rhs [|res|^2, (<w,res> re, im,) <res,chi> re, im], or
+        None with fetch=False (values stay on the device)."""
+        nval = 5 if w is not None else 3
+        out = np.zeros(res.nrhs * nval) if fetch else None
+        check(L._lib.qphix_gpu_dslash_achimbdpsi_norms(
+            C.byref(self.p), res.h, psi.h, chi.h, u.h, clov.h, 0.0, beta, isign, cb, 1.0,
+            w.h if w is not None else None, out.ctypes.data if fetch else None))
+        return out.reshape(res.nrhs, nval) if fetch else None
+
 
 class TMDslash(Dslash):
     """include/qphix/tm_dslash_def.h:23-49"""

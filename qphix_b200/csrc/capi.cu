@@ -990,6 +990,8 @@ static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qp
 }
 
 // options for the second (achimbdpsi) kernel of an operator application
+static const double *fetch_result(qphix_gpu_lattice_s *lat, int nrhs, int nval);
+
 struct ApplyOpts {
   int post = POST_STORE;
   int red_mask = 0;
@@ -1111,6 +1113,31 @@ extern "C" int qphix_gpu_dslash_achimbdpsi(const qphix_gpu_op_params *p, qphix_g
   return guard([&] {
     QPX_REQUIRE(p, "null params");
     achi_core(*p, res, psi, chi, gauge, aux, alpha, beta, isign, cb, musign, ApplyOpts());
+  });
+}
+
+extern "C" int qphix_gpu_dslash_achimbdpsi_norms(const qphix_gpu_op_params *p, qphix_gpu_field res,
+                                                 qphix_gpu_field psi, qphix_gpu_field chi, qphix_gpu_field gauge,
+                                                 qphix_gpu_field aux, double alpha, double beta, int isign, int cb,
+                                                 double musign, qphix_gpu_field w, double *out)
+{
+  return guard([&] {
+    QPX_REQUIRE(p, "null params");
+    if (w) {
+      require_spinor(w, "w");
+      require_same(res, w);
+      QPX_REQUIRE(w->nrhs == res->nrhs, "rhs count mismatch");
+    }
+    ApplyOpts o;
+    o.red_mask = RED_NORM_OUT | RED_DOT_OUT_CHI | (w ? RED_DOT_W_OUT : 0);
+    o.fin = FIN_NONE;
+    o.w = w;
+    achi_core(*p, res, psi, chi, gauge, aux, alpha, beta, isign, cb, musign, o);
+    if (out) {
+      const int nval = red_nval(o.red_mask);
+      const double *h = fetch_result(res->lat, res->nrhs, nval);
+      for (int i = 0; i < res->nrhs * nval; i++) out[i] = h[i];
+    }
   });
 }
 

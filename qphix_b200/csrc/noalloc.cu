@@ -14,7 +14,11 @@
 //
 // Scratch: g_noalloc_scratch, 256 bytes of ticket / padding followed by
 // QPX_NOALLOC_PARTIALS doubles (512 KiB in all), held by every GPU that loads
-// the library until the process exits.  A call needs
+// the library until the process exits.  Under CUDA's lazy module loading
+// (the default since CUDA 12.2) a device reserves the array at the first
+// call made on it (the symbol lookup loads this file's module), so that
+// first call belongs before the caller's allocator reserves the free HBM;
+// CUDA_MODULE_LOADING=EAGER reserves it when the library is loaded.  A call needs
 // ceil(volcb / 128) x nrhs partials; larger requests are rejected.
 // Every call shares the array: the ticket is cleared at the start of each
 // call, and calls whose kernels overlap on the GPU (different streams, or
@@ -59,6 +63,15 @@ extern "C" int qphix_gpu_blas_norm2_noalloc(qphix_gpu_field x, double *out_dev)
   if (attr.device != dev)
     return qpx_set_last_error("the field's device is not the current device", QPHIX_GPU_EINVAL);
   if (dev < 0 || dev >= QPX_MAX_DEVICES) return qpx_set_last_error("device ordinal too large", QPHIX_GPU_EINVAL);
+  // the result is written by a kernel: out_dev must be device (or managed)
+  // memory of this device, never a host buffer
+  cudaPointerAttributes oattr;
+  if (cudaPointerGetAttributes(&oattr, out_dev) != cudaSuccess) {
+    cudaGetLastError();
+    return qpx_set_last_error("out_dev is not a device pointer", QPHIX_GPU_EINVAL);
+  }
+  if ((oattr.type != cudaMemoryTypeDevice && oattr.type != cudaMemoryTypeManaged) || oattr.device != dev)
+    return qpx_set_last_error("out_dev must be device or managed memory of the current device", QPHIX_GPU_EINVAL);
   const long long nblocks = (lat->vh + QPX_BLOCK - 1) / QPX_BLOCK;
   if (nblocks * x->nrhs > QPX_NOALLOC_PARTIALS)
     return qpx_set_last_error("qphix_gpu_blas_norm2_noalloc: ceil(volcb/128) * nrhs exceeds 65536 "

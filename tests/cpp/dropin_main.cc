@@ -18,7 +18,10 @@
 #include "qphix/invcg.h"
 #include "qphix/minvcg.h"
 #include "qphix/ndtm_reuse_operator.h"
+#include "qphix/invmr.h"
 #include "qphix/ndtm_reuse_operator_clover.h"
+#include "qphix/twisted_mass.h"
+#include "qphix/twisted_mass_clover.h"
 #include "qphix/unprec_solver_wrapper.h"
 #include "qphix/wilson.h"
 
@@ -253,6 +256,82 @@ int main(int argc, char **argv)
       geom.free(b);
       geom.free(c);
       geom.free(ch);
+    }
+
+    // 10. ClovDslash members, InvMR / InvMRSmoother with over-relaxation,
+    // the twisted-mass Wilson and twisted-mass clover even-odd operators
+    {
+      auto *chi = geom.allocCBFourSpinor();
+      auto *w = geom.allocCBFourSpinor();
+      read_into("d_chi", chi, sbytes);
+      ClovDslash<double, 4, 2, true> CD(&geom, -1.0, 1.0, 1.0, nullptr, nullptr, 0.05);
+      CD.dslash(w, psi, F.u[0], F.Ainv_even, 1, 0);
+      write_from("out_clov_dslash", w, sbytes);
+      CD.dslashAChiMinusBDPsi(w, psi, chi, F.u[1], F.A_odd, 0.25, -1, 1);
+      write_from("out_clov_achi", w, sbytes);
+      CD.clovMult(w, psi, F.A_odd);
+      write_from("out_clovmult", w, sbytes);
+
+      InvMR<double, 4, 2, true> mr(M, 2000, 1.1);
+      zeroSpinor(w, geom, 1);
+      mr(w, psi, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
+      write_from("out_mr_x", w, sbytes);
+      double minfo[3] = {(double)n_iters, rsd_sq, (double)mv};
+      write_from("out_mr_info", minfo, sizeof(minfo));
+      InvMRSmoother<double, 4, 2, true> sm(M, 5, 1.2);
+      zeroSpinor(w, geom, 1);
+      sm(w, psi, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
+      write_from("out_mrs_x", w, sbytes);
+      double sinfo[3] = {(double)n_iters, rsd_sq, (double)mv};
+      write_from("out_mrs_info", sinfo, sizeof(sinfo));
+
+      double tm[1];
+      read_into("tm_mu", tm, sizeof(tm));
+      EvenOddTMWilsonOperator<double, 4, 2, true> TW(mass, tm[0], F.u, &geom, -1.0, 1.0, 1.0);
+      TW(w, psi, 1, 1);
+      write_from("out_tmw_op", w, sbytes);
+      InvBiCGStab<double, 4, 2, true, EvenOddTMWilsonOperator<double, 4, 2, true>> tbicg(TW, 2000);
+      zeroSpinor(w, geom, 1);
+      tbicg(w, psi, 1e-10, n_iters, rsd_sq, flops, mv, 1, false, 1);
+      write_from("out_tmw_bicg_x", w, sbytes);
+
+      size_t fbytes = (size_t)(geom.getPxyz() * geom.Nt() * 2 / 4) * sizeof(Geometry<double, 4, 2, true>::FullCloverBlock);
+      Geometry<double, 4, 2, true>::FullCloverBlock *tinv[2] = {geom.allocCBFullClov(), geom.allocCBFullClov()};
+      read_into("d_tm_finv0", tinv[0], fbytes);
+      read_into("d_tm_finv1", tinv[1], fbytes);
+      EvenOddTMCloverOperator<double, 4, 2, true> TMC(F.u, F.A_odd, tinv, &geom, -1.0, 1.0, 1.0, nullptr, nullptr,
+                                                      tm[0]);
+      TMC(w, psi, -1, 1);
+      write_from("out_tmc_op", w, sbytes);
+      geom.free(tinv[0]);
+      geom.free(tinv[1]);
+      geom.free(chi);
+      geom.free(w);
+    }
+
+    // 11. the device copy of the gauge array is kept between calls: repeated
+    // calls, an in-place rewrite announced with invalidateFieldCache(), and an
+    // array released and allocated again
+    {
+      auto *w = geom.allocCBFourSpinor();
+      Dslash<double, 4, 2, true> DC(&geom, -1.0, 1.0, 1.0);
+      DC.dslash(w, psi, F.u[0], 1, 0);
+      DC.dslash(w, psi, F.u[0], 1, 0);
+      write_from("out_cache_1", w, sbytes);
+      read_into("d_u0b", F.u[0], F.gbytes);  // rewritten in place
+      DC.invalidateFieldCache();
+      DC.dslash(w, psi, F.u[0], 1, 0);
+      write_from("out_cache_2", w, sbytes);
+      auto *ua = geom.allocCBGauge();
+      read_into("d_u0", ua, F.gbytes);
+      DC.dslash(w, psi, ua, 1, 0);
+      geom.free(ua);
+      auto *ub = geom.allocCBGauge();  // may reuse ua's address
+      read_into("d_u0b", ub, F.gbytes);
+      DC.dslash(w, psi, ub, 1, 0);
+      write_from("out_cache_3", w, sbytes);
+      geom.free(ub);
+      geom.free(w);
     }
 
     for (int s = 0; s < ns; s++) geom.free(xs[s]);

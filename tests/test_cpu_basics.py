@@ -91,8 +91,9 @@ def test_oracle_hermiticity(oracle):
 
 
 def test_bench_reference_arm_runs_on_cpu():
-    """`bench.py --impl reference` (the CPU path of the same system, timed on
-    host cores) prints the contract's line without a GPU."""
+    """`bench.py --impl reference` (QPhiX's own CPU path solving the same
+    system on the host cores, else the oracle's port) prints the contract's
+    line without a GPU; every step is a full solve to 1e-10."""
     import json
     import sys
     out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
@@ -100,6 +101,11 @@ def test_bench_reference_arm_runs_on_cpu():
     assert out.returncode == 0, out.stderr[-2000:]
     line = json.loads(out.stdout.strip().splitlines()[-1])
     assert line["impl"] == "reference" and line["value"] > 0 and line["unit"] == "solves/s"
-    assert line["cpu_baseline"]["kind"] == "port" and line["cpu_baseline"]["cores"] >= 1
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_dslash
+    built = ref_dslash.available("avx512") or ref_dslash.available("scalar")
+    assert line["cpu_baseline"]["kind"] == ("reference" if built else "port")
+    assert line["cpu_baseline"]["cores"] >= 1
+    assert line["worst_rel_resid"] <= 1e-10
     assert line["e2e"] == {"value": line["value"], "unit": "solves/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}

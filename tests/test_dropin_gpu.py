@@ -5,7 +5,8 @@ padding, and Geometry<float,8,2,true> for the inner solver of
 InvRichardsonMultiPrec) packed from seeded fields, and its outputs -- a
 Dslash, the clover operator, BiCGStab, CG, Richardson and multishift-CG
 solves, the two-flavour twisted-mass Wilson and clover operators and their
-CG solves -- are
+CG solves, the ClovDslash members, InvMR / InvMRSmoother with over-relaxation,
+and the twisted-mass Wilson and twisted-mass clover operators -- are
 checked against the CPU oracle.  An UnprecSolverWrapper solve of the full
 (unpreconditioned) clover system is checked through its full residual."""
 import os
@@ -50,6 +51,13 @@ def test_cpp_dropin(tmp_path, oracle):
     lay.pack_clover(ndc_c).tofile(d / "d_ndc_odiag")
     lay.pack_full_clover(ndc_fu).tofile(d / "d_ndc_fup")
     lay.pack_full_clover(ndc_fd).tofile(d / "d_ndc_fdn")
+    g2 = F.make_gauge(dims, 77, "weak")  # a second gauge field for the cache checks
+    lay.pack_gauge(g2, 0).tofile(d / "d_u0b")
+    mu_tm = 0.07
+    np.array([mu_tm], dtype=np.float64).tofile(d / "tm_mu")
+    tinv = F.twisted_full_inverse(s["clov"][0], mu_tm)
+    lay.pack_full_clover(tinv[0]).tofile(d / "d_tm_finv0")
+    lay.pack_full_clover(tinv[1]).tofile(d / "d_tm_finv1")
     out = subprocess.run([str(exe), str(d)], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr + out.stdout
 
@@ -125,3 +133,28 @@ def test_cpp_dropin(tmp_path, oracle):
     rel = np.sqrt((np.linalg.norm(re) ** 2 + np.linalg.norm(ro) ** 2)
                   / (np.linalg.norm(chi) ** 2 + np.linalg.norm(psi) ** 2))
     assert rel < 2e-10
+    # ClovDslash members (clover_dslash_def.h:33-53), rho = 0.05
+    assert rel_l2(load("out_clov_dslash"), oracle.clov_dslash(L, psi, s["gauge"], s["invclov"][0], 1, 0)) < 1e-13
+    assert rel_l2(load("out_clov_achi"),
+                  oracle.clov_achimbdpsi(L, psi, chi, s["gauge"], s["clov"][1], 0.25, 0.05, -1, 1)) < 1e-13
+    assert rel_l2(load("out_clovmult"), oracle.clover_apply(psi, s["clov"][1])) < 1e-13
+    # InvMR with Omega = 1.1 and InvMRSmoother (5 iterations, Omega = 1.2)
+    xm, im = oracle.mr(O, psi, 1e-10, 2000, 1.1)
+    info = np.fromfile(d / "out_mr_info")
+    assert int(info[0]) == im.n_iters and rel_l2(load("out_mr_x"), xm) < 1e-9
+    xs5, i5 = oracle.mr(O, psi, 0.0, 5, 1.2)
+    info = np.fromfile(d / "out_mrs_info")
+    assert int(info[0]) == 5 and info[1] == -1 and rel_l2(load("out_mrs_x"), xs5) < 1e-12
+    # twisted-mass Wilson operator (twisted_mass.h:62-77) and BiCGStab on it;
+    # twisted-mass clover operator (twisted_mass_clover.h:92-102), isign = -1
+    TW = oracle.OracleOp("tm", L, s["gauge"], mass=s["mass"], twisted_mass=mu_tm)
+    assert rel_l2(load("out_tmw_op"), TW.apply(psi, 1, 1)) < 1e-13
+    xt = load("out_tmw_bicg_x")
+    assert np.linalg.norm(psi - TW.apply(xt, 1)) / np.linalg.norm(psi) < 2e-10
+    TC = oracle.OracleOp("tmclover", L, s["gauge"], clov=s["clov"][1], finv=tinv, rho=mu_tm)
+    assert rel_l2(load("out_tmc_op"), TC.apply(psi, -1, 1)) < 1e-13
+    # the cached device gauge copy: reused, invalidated after an in-place
+    # rewrite, never matched for a reallocated array
+    assert rel_l2(load("out_cache_1"), oracle.dslash(L, psi, s["gauge"], 1, 0)) < 1e-13
+    assert rel_l2(load("out_cache_2"), oracle.dslash(L, psi, g2, 1, 0)) < 1e-13
+    assert rel_l2(load("out_cache_3"), oracle.dslash(L, psi, g2, 1, 0)) < 1e-13

@@ -120,16 +120,36 @@ def test_bicgstab(api, oracle, setup, kind):
     assert rel_l2(x, xo) < 1e-8
 
 
-def test_mr(api, oracle, setup):
+@pytest.mark.parametrize("omega", [1.0, 1.1, 0.8])
+def test_mr(api, oracle, setup, omega):
+    """InvMR (invmr.h:62-210) with over-relaxation: iteration count and
+    solution equal the oracle's for Omega != 1 too."""
     lat, M, O = build_ops(api, oracle, setup, "clover")
     b = F.gaussian_spinor(setup["dims"], 43)
     gx, gb = lat.spinor(), lat.spinor().upload(b)
-    info = api.InvMR(M, 2000, 1.0)(gx, gb, 1e-10)[0]
-    xo, io = oracle.mr(O, b, 1e-10, 2000, 1.0)
+    info = api.InvMR(M, 2000, omega)(gx, gb, 1e-10)[0]
+    xo, io = oracle.mr(O, b, 1e-10, 2000, omega)
     x = gx.download()
     r = b - O.apply(x, 1)
     assert np.linalg.norm(r) / np.linalg.norm(b) < 2e-10
     assert info["n_iters"] == io.n_iters
+    assert rel_l2(x, xo) < 1e-9
+
+
+@pytest.mark.parametrize("omega", [1.0, 1.2])
+def test_mr_smoother(api, oracle, setup, omega):
+    """InvMRSmoother (invmr.h:294-354): exactly n MR iterations, no residual
+    test, rsd_sq_final = -1; the same iterates as the oracle's MR run to an
+    unreachable target for n iterations."""
+    lat, M, O = build_ops(api, oracle, setup, "tmclover")
+    b = F.gaussian_spinor(setup["dims"], 44)
+    for n in (1, 7):
+        gx, gb = lat.spinor(), lat.spinor().upload(b)
+        info = api.InvMRSmoother(M, n, omega)(gx, gb)[0]
+        xo, io = oracle.mr(O, b, 0.0, n, omega)
+        assert io.n_iters == n and info["n_iters"] == n
+        assert info["rsd_sq_final"] == -1
+        assert rel_l2(gx.download(), xo) < 1e-12, n
 
 
 @pytest.mark.parametrize("inner_prec", ["f32", "f16", "bf16", "q16"])
