@@ -25,6 +25,11 @@ cpu_baseline: QPhiX's own CPU path (its code-generated AVX-512 kernels and
          sources) solving one right-hand side of the same system to 1e-10 on
          all host cores; --impl reference times the same solves per step.
 
+At N = 1 the other configurations follow the headline (extra_configs():
+8^4 CG, 24^3x48 24-rhs TM clover, 32^3x64 16-shift multishift, and the
+2000-request serving stream whose latency p50 / p99 is the metric's "p99
+ms"); --no-extra skips them.
+
 N > 1 GPUs: independent replicas (the path does not shard across GPUs here);
 value = all ranks' solves / max-over-ranks time.
 """
@@ -65,6 +70,9 @@ def parse():
     ap.add_argument("--inner-recon", type=int, default=12, choices=[12, 18],
                     help="link storage of the inner operator (12- or 18-real)")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the other configurations (8^4 CG, 24^3x48 24-rhs TM clover, 32^3x64 16-shift "
+                         "multishift, the 2000-request serving stream) measured after the headline at N = 1")
     ap.add_argument("--solver", default="richardson", choices=["ru", "richardson"],
                     help="ru: BiCGStab with reliable updates; richardson: InvRichardsonMultiPrec")
     ap.add_argument("--delta", type=float, default=None,
@@ -278,6 +286,33 @@ def run_reference(args, rank, world):
                              "sample": ref.describe(what)},
             "e2e": {"value": round(v, 4), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def extra_configs():
+    """The benchmark's other configurations, each measured once after the
+    headline (N = 1, rank 0): 8^4 Wilson CG, the 24^3x48 24-rhs batched
+    twisted-mass clover solve, the 32^3x64 16-shift multishift CG
+    (qphix_b200.workloads) and the 2000-request Poisson serving stream at 70 %
+    of measured capacity (qphix_b200.serve_bench), whose latency p50 / p99
+    are the metric's "p99 ms"."""
+    import types
+
+    from qphix_b200 import serve_bench, workloads
+    out = {}
+    for name, fn in (("c1", workloads.c1), ("c3", workloads.c3), ("c4", workloads.c4)):
+        t0 = time.perf_counter()
+        try:
+            out[name] = fn(types.SimpleNamespace(reps=2))
+        except Exception as e:  # pragma: no cover - reported, the headline still prints
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        out[name]["wall_s"] = round(time.perf_counter() - t0, 1)
+    t0 = time.perf_counter()
+    try:
+        out["serve"] = serve_bench.run(["--requests", "2000", "--load", "0.7"])
+    except Exception as e:  # pragma: no cover
+        out["serve"] = {"error": f"{type(e).__name__}: {e}"}
+    out["serve"]["wall_s_total"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 METRIC = "Clover solves/s @1e-10 mixed vs FP64 plain, 1 B200; Dslash HBM GB/s; p99 ms"
@@ -581,11 +616,14 @@ def main():
                 "traffic": (round(traffic2 * vh2) if traffic2 else None)}
 
     cpu = None
+    extra = None
     if rank == 0 and world == 1:
         try:
             cpu = cpu_baseline_leg(inputs, DIMS)
         except Exception as e:  # pragma: no cover
             cpu = {"value": None, "error": str(e)}
+        if not args.no_extra:
+            extra = extra_configs()
 
     if rank == 0:
         p = sorted(step_ms)
@@ -614,6 +652,12 @@ def main():
             "q16_inner_vs_fp64_solves_ratio": (round(q16_line["solves_per_s"] / fp64["solves_per_s"], 3)
                                                if (fp64 and q16_line) else None),
         }
+        if extra:
+            sv = extra.get("serve", {})
+            line["serve_latency_p50_ms"] = sv.get("latency_p50_ms")
+            line["serve_latency_p99_ms"] = sv.get("latency_p99_ms")
+            line["serve_solves_per_s"] = sv.get("solves_per_s")
+            line["configs"] = extra
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

@@ -97,13 +97,29 @@ def random_su3_exp(rng, n, eps):
     det = e^{i eps tr H} = 1.  A final reunitarisation pins det = 1 to the
     last bit for the 12-real form."""
     a = gaussian_complex(rng, (n, 3, 3))
-    h = (a + np.conj(np.swapaxes(a, -1, -2))) / np.sqrt(2.0)
-    tr = np.trace(h, axis1=-2, axis2=-1) / 3.0
-    h = h - tr[:, None, None] * np.eye(3)
-    lam, vec = np.linalg.eigh(h)
-    ph = np.exp(1j * eps * lam)
-    u = np.einsum("nij,nj,nkj->nik", vec, ph, np.conj(vec))
-    return reunitarize(u)
+
+    def expm(lo, hi):
+        b = a[lo:hi]
+        h = (b + np.conj(np.swapaxes(b, -1, -2))) / np.sqrt(2.0)
+        tr = np.trace(h, axis1=-2, axis2=-1) / 3.0
+        h = h - tr[:, None, None] * np.eye(3)
+        lam, vec = np.linalg.eigh(h)
+        ph = np.exp(1j * eps * lam)
+        return reunitarize(np.einsum("nij,nj,nkj->nik", vec, ph, np.conj(vec)))
+
+    # the matrices are independent: chunks in threads (numpy releases the GIL
+    # in eigh / einsum), results identical to one pass
+    chunk = 1 << 18
+    if n <= chunk:
+        return expm(0, n)
+    import concurrent.futures as cf
+    import os
+    out = np.empty((n, 3, 3), dtype=np.complex128)
+    bounds = [(lo, min(n, lo + chunk)) for lo in range(0, n, chunk)]
+    with cf.ThreadPoolExecutor(max_workers=min(len(bounds), os.cpu_count() or 1)) as ex:
+        for (lo, hi), u in zip(bounds, ex.map(lambda b: expm(*b), bounds)):
+            out[lo:hi] = u
+    return out
 
 
 def random_weak_su3(rng, n, factor):

@@ -44,6 +44,12 @@ def make_requests(n, seed, nvol=len(VOLUMES)):
 
 
 def main(argv=None):
+    print(json.dumps(run(argv)), flush=True)
+
+
+def run(argv=None):
+    """Runs the benchmark (arguments as on the command line) and returns its
+    result line as a dict."""
     ap = argparse.ArgumentParser()
     ap.add_argument("--requests", type=int, default=300)
     ap.add_argument("--load", type=float, default=0.7)
@@ -165,7 +171,7 @@ def main(argv=None):
         "data": "synthetic (seeded)",
         "solver": args.solver,
     }
-    print(json.dumps(line), flush=True)
+    return line
 
 
 if __name__ == "__main__":

@@ -8,7 +8,9 @@ lattice workspace and writes to a caller-owned device buffer; the test checks
 that, on two calls in a row, it returns what the regular entry point returns
 and what numpy computes from the downloaded field (relative 1e-13, the FP64
 tolerance of the other parity tests), for several precisions and
-right-hand-side counts, at exactly its largest size with Gaussian data, that
+right-hand-side counts; at exactly its largest size (2.5e7 terms per sum)
+with Gaussian data against numpy within 1e-11, the rounding of two summation
+orders at that length; and that
 it rejects a request larger than its fixed scratch and a host result
 pointer (before launching anything).  This file is collected last so a
 stop-at-first-failure run has already run every other test.
@@ -78,7 +80,9 @@ def test_norm2_noalloc_rejects_oversized_request():
         xs = small.download().reshape(8, -1)
         host = np.einsum("ij,ij->i", xs.conj(), xs).real
         got = out8.cpu().numpy()
-        assert np.all(np.abs(got - host) <= 1e-13 * host), (got, host)
+        # 2.5e7 squares per rhs summed in FP64 in two different orders:
+        # rounding ~ sqrt(n) * 2^-53 ~ 6e-13 relative, bounded at 1e-11
+        assert np.all(np.abs(got - host) <= 1e-11 * host), (got, host)
 
 
 def test_norm2_noalloc_rejects_host_result_pointer():
