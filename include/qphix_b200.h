@@ -140,7 +140,9 @@ int qphix_gpu_launch_count(unsigned long long *out);
  * links, epilogue, lattice, nrhs) is timed over its built shapes (right-hand
  * sides per thread, lattice sites per thread) the first time it runs
  * outside CUDA-graph capture; the fastest shape is kept for the process.
- * Entries are listed in key order. */
+ * Entries are listed in key order.  sites_per_thread = 0 (with rhs_tile = 2)
+ * denotes the shape that keeps two right-hand sides of one site in the
+ * float2 lanes of a thread. */
 int qphix_gpu_tune_enable(int enable);
 int qphix_gpu_tune_entries(int *count);
 int qphix_gpu_tune_entry(int index, char *key, size_t key_len, int *rhs_tile, int *sites_per_thread,

@@ -57,6 +57,77 @@ void launch_blas(int prec, const BlasArgs &a, dim3 grid, cudaStream_t st)
   QPX_PREC_SWITCH(prec, (blas_kernel<P><<<grid, QPX_BLOCK, 0, st>>>(a)));
 }
 
+// Folds the block partials of one reducing launch (reduce_epilogue,
+// qpx_reduce.cuh) into ra.result and runs the solver's finalize step; one
+// block of QPX_FOLD_THREADS threads, launched right after the producing
+// kernel on its stream.  The nres = nrhs x nval values share the 32 warps,
+// a group of G = max(1, 32 / nres) warps per value (further rounds when
+// nres > 32): lane l of warp g of a group adds site blocks 32 g + l,
+// 32 g + l + 32 G, ... in that order, then a shuffle tree per warp and the
+// group's warps in order.  A solver state that is already done makes it
+// return at once, as the producing kernel did.
+__global__ void __launch_bounds__(QPX_FOLD_THREADS) fold_kernel(const ReduceArg ra, SolverState *st, int nrhs,
+                                                                int nparts)
+{
+  if (st && st->done) return;
+  __shared__ double gsum[QPX_FOLD_THREADS / 32];
+  __shared__ double res[QPX_MAX_RHS * QPX_MAX_RED];
+  __shared__ SolverState sst;
+  constexpr int kStateWords = sizeof(SolverState) / sizeof(int);
+  static_assert(sizeof(SolverState) % sizeof(int) == 0, "SolverState is copied as 32-bit words");
+  const int nres = nrhs * ra.nval;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  // the solver state is read and written by the finalize step on thread 0
+  // below: a shared copy turns its chain of dependent global accesses into
+  // shared-memory ones
+  if (st)
+    for (int i = threadIdx.x; i < kStateWords; i += blockDim.x)
+      reinterpret_cast<int *>(&sst)[i] = reinterpret_cast<const int *>(st)[i];
+  const int G = nres >= 32 ? 1 : 32 / nres;
+  const int vpr = 32 / G;  // values per round
+  for (int v0 = 0; v0 < nres; v0 += vpr) {
+    const int slot = wid / G, g = wid % G;
+    const int v = v0 + slot;
+    double acc = 0.0;
+    if (slot < vpr && v < nres) {
+      const double *p = ra.partials + v;
+#pragma unroll 8
+      for (int b = 32 * g + lane; b < nparts; b += 32 * G) acc += __ldcg(p + (long long)b * nres);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) gsum[wid] = acc;
+    __syncthreads();
+    if ((int)threadIdx.x < vpr && v0 + (int)threadIdx.x < nres) {
+      double t = 0.0;
+      for (int k = 0; k < G; k++) t += gsum[threadIdx.x * G + k];
+      res[v0 + threadIdx.x] = t;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    // two-flavour systems: each flavour pair's reductions are one sum (the
+    // reference's num_flav = 2 BLAS), so both get the same solver scalars
+    if (st && sst.coupled)
+      for (int r = 0; r + 1 < nrhs; r += 2)
+        for (int k = 0; k < ra.nval; k++) {
+          const double t = res[r * ra.nval + k] + res[(r + 1) * ra.nval + k];
+          res[r * ra.nval + k] = t;
+          res[(r + 1) * ra.nval + k] = t;
+        }
+    if (ra.fin != FIN_NONE && st) finalize(ra.fin, &sst, res, nrhs, ra.nval);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < nres; i += blockDim.x) ra.result[i] = res[i];
+  if (st)
+    for (int i = threadIdx.x; i < kStateWords; i += blockDim.x)
+      reinterpret_cast<int *>(st)[i] = reinterpret_cast<const int *>(&sst)[i];
+}
+
+void launch_fold(const ReduceArg &ra, SolverState *state, int nrhs, int nparts, cudaStream_t st)
+{
+  fold_kernel<<<1, QPX_FOLD_THREADS, 0, st>>>(ra, state, nrhs, nparts);
+}
+
 template <typename P>
 static void conv_from(int pdst, int vh, SpinorArg src, SpinorArg dst, Coef scale, SolverState *state, int acc,
                       dim3 grid, cudaStream_t st)

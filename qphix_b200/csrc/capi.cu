@@ -153,8 +153,6 @@ static void create_lattice(const int latt[4], cudaMemPool_t pool, qphix_gpu_latt
       // Richardson per-rhs scale factors
       L->partials_len = (size_t)nblocks_for(L->vh) * QPX_MAX_RHS * QPX_MAX_RED + 2 * QPX_MAX_RHS;
       QPX_CUDA(cudaMalloc(&L->partials, L->partials_len * sizeof(double)));
-      QPX_CUDA(cudaMalloc(&L->ticket, 64 * sizeof(unsigned int)));
-      QPX_CUDA(cudaMemset(L->ticket, 0, 64 * sizeof(unsigned int)));
       QPX_CUDA(cudaMalloc(&L->result, QPX_MAX_RHS * QPX_MAX_RED * sizeof(double)));
       QPX_CUDA(cudaMallocHost(&L->h_result, QPX_MAX_RHS * QPX_MAX_RED * sizeof(double)));
       QPX_CUDA(cudaMalloc(&L->state, sizeof(SolverState)));
@@ -179,7 +177,6 @@ static void lattice_release(qphix_gpu_lattice_s *L)
   if (L->staging) dev_free(L, L->mempool != nullptr, L->staging);
   if (L->stream) cudaStreamSynchronize(L->stream);
   cudaFree(L->partials);
-  cudaFree(L->ticket);
   cudaFree(L->result);
   cudaFreeHost(L->h_result);
   cudaFree(L->state);
@@ -608,14 +605,15 @@ bool tune_enabled()
 
 dim3 dslash_grid(const qphix_gpu_lattice_s *lat, const DslashShape &sh, int nrhs)
 {
-  long long per = (long long)QPX_BLOCK * sh.SP;
+  long long per = (long long)QPX_BLOCK * (sh.rl ? 1 : sh.SP);
   long long nsb = (lat->vh + per - 1) / per;
-  return dim3((unsigned)(nsb * (nrhs / sh.R)));
+  return dim3((unsigned)(nsb * (nrhs / (sh.rl ? 2 : sh.R))));
 }
 
 bool shape_built(int prec, int recon, int epi, int achi, const DslashShape &sh, int nrhs)
 {
   if (nrhs % sh.R) return false;
+  if (sh.rl && nrhs % 2) return false;
   return launch_dslash(prec, recon, epi, achi, sh, nullptr, dim3(1), nullptr);
 }
 
@@ -654,9 +652,16 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
     return sh;
   }
   if (gen) return default_shape(prec, true);
-  // forced shapes (experiments)
+  // forced shapes (experiments and tests): QPHIX_GPU_RHS_LANES=1 selects two
+  // right-hand sides in the float2 lanes of one site
   const char *fr = getenv("QPHIX_GPU_RHS_TILE"), *fs = getenv("QPHIX_GPU_SITES_PER_THREAD");
-  if (fr || fs) {
+  const char *fl = getenv("QPHIX_GPU_RHS_LANES");
+  if (fl && atoi(fl) == 1) {
+    DslashShape sh;
+    sh.SP = 2;
+    sh.rl = true;
+    if (shape_built(prec, recon, epi, achi, sh, a.nrhs)) return sh;
+  } else if (fr || fs) {
     DslashShape sh = default_shape(prec, false);
     if (fr) sh.R = atoi(fr);
     if (fs) sh.SP = atoi(fs);
@@ -671,6 +676,12 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
       sh.SP = sp;
       if (shape_built(prec, recon, epi, achi, sh, a.nrhs)) cands.push_back(sh);
     }
+  {
+    DslashShape sh;
+    sh.SP = 2;
+    sh.rl = true;
+    if (shape_built(prec, recon, epi, achi, sh, a.nrhs)) cands.push_back(sh);
+  }
   if (cands.size() <= 1) return cands.empty() ? default_shape(prec, false) : cands[0];
   const int red = tuned_reductions(a);
   const std::string key = tune_key(lat, prec, recon, epi, achi, a.nrhs, red);
@@ -695,7 +706,6 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
   t.red.nval = red_nval(red);
   t.red.fin = FIN_NONE;
   t.red.partials = lat->partials;
-  t.red.ticket = lat->ticket;
   t.red.result = lat->result;
   cudaEvent_t e0, e1;
   QPX_CUDA(cudaEventCreate(&e0));
@@ -752,8 +762,9 @@ extern "C" int qphix_gpu_tune_entry(int index, char *key, size_t key_len, int *r
     auto it = g_tune.begin();
     std::advance(it, index);
     if (key && key_len) snprintf(key, key_len, "%s", it->first.c_str());
-    if (rhs_tile) *rhs_tile = it->second.sh.R;
-    if (sites_per_thread) *sites_per_thread = it->second.sh.SP;
+    // the rhs-lanes shape reads as two right-hand sides on 0 sites per thread
+    if (rhs_tile) *rhs_tile = it->second.sh.rl ? 2 : it->second.sh.R;
+    if (sites_per_thread) *sites_per_thread = it->second.sh.rl ? 0 : it->second.sh.SP;
     if (launch_us) *launch_us = it->second.us;
   });
 }
@@ -764,7 +775,6 @@ static void set_reduce(DslashArgs &a, qphix_gpu_lattice_s *lat, int mask, int fi
   a.red.nval = red_nval(mask);
   a.red.fin = fin;
   a.red.partials = lat->partials;
-  a.red.ticket = lat->ticket;
   a.red.result = lat->result;
   a.state = st;
 }
@@ -774,13 +784,18 @@ static void dslash_launch(qphix_gpu_lattice_s *lat, int prec, int recon, int epi
   DslashShape sh = choose_shape(lat, prec, recon, epi, achi, a);
   if (a.red.mask) {
     a.red.partials = lat->partials;
-    a.red.ticket = lat->ticket;
     a.red.result = lat->result;
     a.red.nval = red_nval(a.red.mask);
   }
-  if (!launch_dslash(prec, recon, epi, achi, sh, &a, dslash_grid(lat, sh, a.nrhs), lat->stream))
+  const dim3 grid = dslash_grid(lat, sh, a.nrhs);
+  if (!launch_dslash(prec, recon, epi, achi, sh, &a, grid, lat->stream))
     throw Error(QPHIX_GPU_EINVAL, "no Dslash kernel built for this precision / link / shape combination");
   check_launch();
+  if (a.red.mask) {  // the blocks' partials: one per (site block, rhs, value)
+    const int ntiles = a.nrhs / (sh.rl ? 2 : sh.R);
+    launch_fold(a.red, a.state, a.nrhs, (int)(grid.x / ntiles), lat->stream);
+    check_launch();
+  }
 }
 
 static void require_spinor(const qphix_gpu_field_s *f, const char *what)
@@ -1484,11 +1499,14 @@ static void blas_launch(qphix_gpu_lattice_s *lat, int prec, int nrhs, const Blas
     a.red.nval = __builtin_popcount(c.slots);
     a.red.fin = c.fin;
     a.red.partials = lat->partials;
-    a.red.ticket = lat->ticket;
     a.red.result = lat->result;
   }
   launch_blas(prec, a, dim3(nblocks_for(lat->vh), nrhs), lat->stream);
   check_launch();
+  if (c.slots) {
+    launch_fold(a.red, c.state, nrhs, (int)nblocks_for(lat->vh), lat->stream);
+    check_launch();
+  }
 }
 
 // fetch the last reduction result (nrhs x nval) to the host

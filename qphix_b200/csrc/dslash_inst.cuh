@@ -9,22 +9,22 @@
 
 namespace qpx {
 
-template <typename P, int RECON, int R, int S, int SP, bool GEN>
+template <typename P, int RECON, int R, int S, int SP, bool GEN, bool RL = false>
 void launch_dslash_k(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStream_t st)
 {
   dim3 block(QPX_BLOCK);
   if (achi == ACHI_NONE) {
     switch (epi) {
-    case EPI_NONE: dslash_kernel<P, RECON, EPI_NONE, ACHI_NONE, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
-    case EPI_CLOV: dslash_kernel<P, RECON, EPI_CLOV, ACHI_NONE, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
-    case EPI_TMINV: dslash_kernel<P, RECON, EPI_TMINV, ACHI_NONE, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
-    case EPI_FCLOV: dslash_kernel<P, RECON, EPI_FCLOV, ACHI_NONE, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
+    case EPI_NONE: dslash_kernel<P, RECON, EPI_NONE, ACHI_NONE, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
+    case EPI_CLOV: dslash_kernel<P, RECON, EPI_CLOV, ACHI_NONE, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
+    case EPI_TMINV: dslash_kernel<P, RECON, EPI_TMINV, ACHI_NONE, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
+    case EPI_FCLOV: dslash_kernel<P, RECON, EPI_FCLOV, ACHI_NONE, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
     }
   } else if (epi == EPI_NONE) {
     switch (achi) {
-    case ACHI_ALPHA: dslash_kernel<P, RECON, EPI_NONE, ACHI_ALPHA, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
-    case ACHI_CLOV: dslash_kernel<P, RECON, EPI_NONE, ACHI_CLOV, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
-    case ACHI_TM: dslash_kernel<P, RECON, EPI_NONE, ACHI_TM, R, S, SP, GEN><<<grid, block, 0, st>>>(a); return;
+    case ACHI_ALPHA: dslash_kernel<P, RECON, EPI_NONE, ACHI_ALPHA, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
+    case ACHI_CLOV: dslash_kernel<P, RECON, EPI_NONE, ACHI_CLOV, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
+    case ACHI_TM: dslash_kernel<P, RECON, EPI_NONE, ACHI_TM, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
     }
   }
   throw Error(QPHIX_GPU_EINVAL, "unsupported dslash epilogue combination");
@@ -48,21 +48,22 @@ void launch_dslash_nd(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStr
 }
 
 // isign is a template parameter: the projector signs become adds / subtracts
-template <typename P, int RECON, int R, int SP, bool GEN>
+template <typename P, int RECON, int R, int SP, bool GEN, bool RL = false>
 void launch_dslash_s(int epi, int achi, const DslashArgs *a, dim3 grid, cudaStream_t st)
 {
   if (!a) return;  // shape query
   if (a->isign == 1)
-    launch_dslash_k<P, RECON, R, 1, SP, GEN>(epi, achi, *a, grid, st);
+    launch_dslash_k<P, RECON, R, 1, SP, GEN, RL>(epi, achi, *a, grid, st);
   else
-    launch_dslash_k<P, RECON, R, -1, SP, GEN>(epi, achi, *a, grid, st);
+    launch_dslash_k<P, RECON, R, -1, SP, GEN, RL>(epi, achi, *a, grid, st);
 }
 
 // The shapes built for storage P.  a == nullptr: only report whether the
 // shape exists.  Returns false for a shape that is not built.
 //   general path (dir mask, twisted phases): R = 1, SP = 1
 //   fast path: R = 1 SP = 1 for every precision; for FP32 arithmetic also
-//   SP = 2 (both link kinds) and R = 2 (12-real links)
+//   SP = 2 (both link kinds), R = 2 (12-real links) and two right-hand sides
+//   in the float2 lanes (rl, 12-real links, even nrhs)
 template <typename P>
 bool launch_dslash_p(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
                      cudaStream_t st)
@@ -78,6 +79,15 @@ bool launch_dslash_p(int recon, int epi, int achi, const DslashShape &sh, const 
     else
       plus ? launch_dslash_nd<P, 18, 1>(epi, achi, *a, grid, st) : launch_dslash_nd<P, 18, -1>(epi, achi, *a, grid, st);
     return true;
+  }
+  if (sh.rl) {
+    if constexpr (fp32) {
+      if (sh.R != 1 || sh.SP != 2 || sh.gen || recon != 12) return false;
+      if (a && a->nrhs % 2) return false;
+      launch_dslash_s<P, 12, 1, 2, false, true>(epi, achi, a, grid, st);
+      return true;
+    }
+    return false;
   }
   if (sh.gen) {
     if (sh.R != 1 || sh.SP != 1) return false;

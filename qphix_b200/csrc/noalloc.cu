@@ -12,17 +12,17 @@
 // library's own device memory (below) and writes the result to a device
 // buffer the caller owns.
 //
-// Scratch: g_noalloc_scratch, 256 bytes of ticket / padding followed by
-// QPX_NOALLOC_PARTIALS doubles (512 KiB in all), held by every GPU that loads
-// the library until the process exits.  Under CUDA's lazy module loading
+// Scratch: g_noalloc_scratch, QPX_NOALLOC_PARTIALS doubles (512 KiB), held
+// by every GPU that loads the library until the process exits.  Under CUDA's lazy module loading
 // (the default since CUDA 12.2) a device reserves the array at the first
 // call made on it (the symbol lookup loads this file's module), so that
 // first call belongs before the caller's allocator reserves the free HBM;
 // CUDA_MODULE_LOADING=EAGER reserves it when the library is loaded.  A call needs
 // ceil(volcb / 128) x nrhs partials; larger requests are rejected.
-// Every call shares the array: the ticket is cleared at the start of each
-// call, and calls whose kernels overlap on the GPU (different streams, or
-// different host threads without ordering) race on it.
+// Every call shares the array: each call's first kernel writes every partial
+// its second kernel (the fold) reads, so nothing carries over from one call
+// to the next, but calls whose kernels overlap on the GPU (different streams,
+// or different host threads without ordering) race on it.
 #include <mutex>
 
 #include "qpx_finalize.cuh"
@@ -33,10 +33,9 @@ using namespace qpx;
 namespace {
 
 constexpr int QPX_NOALLOC_PARTIALS = 65536;
-constexpr int QPX_NOALLOC_HEAD = 32;  // doubles before the partials: the ticket, 256-byte aligned
 constexpr int QPX_MAX_DEVICES = 64;
 
-static __device__ __align__(256) double g_noalloc_scratch[QPX_NOALLOC_HEAD + QPX_NOALLOC_PARTIALS];
+static __device__ __align__(256) double g_noalloc_scratch[QPX_NOALLOC_PARTIALS];
 
 std::mutex g_mu;
 double *g_scratch_addr[QPX_MAX_DEVICES] = {};
@@ -89,9 +88,6 @@ extern "C" int qphix_gpu_blas_norm2_noalloc(qphix_gpu_field x, double *out_dev)
     }
     scratch = g_scratch_addr[dev];
   }
-  // the ticket must start at zero
-  if (cudaMemsetAsync(scratch, 0, QPX_NOALLOC_HEAD * sizeof(double), lat->stream) != cudaSuccess)
-    return qpx_set_last_error("clearing the scratch ticket failed", QPHIX_GPU_ECUDA);
   BlasArgs a;
   memset(&a, 0, sizeof(a));
   a.op = B_NORM2;
@@ -101,12 +97,12 @@ extern "C" int qphix_gpu_blas_norm2_noalloc(qphix_gpu_field x, double *out_dev)
   a.red.mask = 0x1;
   a.red.nval = 1;
   a.red.fin = FIN_NONE;
-  a.red.partials = scratch + QPX_NOALLOC_HEAD;
-  a.red.ticket = reinterpret_cast<unsigned int *>(scratch);
+  a.red.partials = scratch;
   a.red.result = out_dev;
   a.state = nullptr;
   try {
     launch_blas(x->prec, a, dim3((unsigned)nblocks, x->nrhs), lat->stream);
+    launch_fold(a.red, nullptr, x->nrhs, (int)nblocks, lat->stream);
   } catch (const Error &err) {
     return qpx_set_last_error(err.what(), err.code);
   }

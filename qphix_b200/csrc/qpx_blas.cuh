@@ -61,6 +61,46 @@ __device__ __forceinline__ void caxpy_(T *y, double ar, double ai, const T *x)
   }
 }
 
+// Reduction terms of one site: FP64 fields keep their element loops (pairs
+// of reals where the reference's functors pair them); FP32-arithmetic fields
+// sum in FP32 per thread and convert once (red_norm / red_dot).
+template <bool PAIRS, typename T>
+__device__ __forceinline__ double blas_norm(const T *x)
+{
+  if constexpr (std::is_same<T, double>::value) {
+    double n = 0;
+    if (PAIRS) {
+#pragma unroll
+      for (int k = 0; k < 24; k += 2) n += (double)x[k] * x[k] + (double)x[k + 1] * x[k + 1];
+    } else {
+#pragma unroll
+      for (int k = 0; k < 24; k++) n += (double)x[k] * x[k];
+    }
+    return n;
+  } else {
+    const bool one[1] = {true};
+    return red_norm(x, one);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void blas_dot(const T *x, const T *y, double &re, double &im)
+{
+  if constexpr (std::is_same<T, double>::value) {
+    double dr = 0, di = 0;
+#pragma unroll
+    for (int k = 0; k < 24; k += 2) {
+      dr += (double)x[k] * y[k] + (double)x[k + 1] * y[k + 1];
+      di += (double)x[k] * y[k + 1] - (double)x[k + 1] * y[k];
+    }
+    re = dr;
+    im = di;
+  } else {
+    const bool one[1] = {true};
+    red_dot(x, y, one, re, im);
+  }
+}
+
 template <typename P>
 __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
 {
@@ -77,26 +117,15 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
     switch (a.op) {
     case B_NORM2: {
       IO::load(a.x, rhs, s, x);
-      double n = 0;
-#pragma unroll
-      for (int k = 0; k < 24; k++) n += (double)x[k] * x[k];
-      red[0][0] = n;
+      red[0][0] = blas_norm<false>(x);
       break;
     }
     case B_DOT:
     case B_DOTNORM: {
       IO::load(a.x, rhs, s, x);
       IO::load(a.y, rhs, s, y);
-      double re = 0, im = 0, n = 0;
-#pragma unroll
-      for (int k = 0; k < 24; k += 2) {
-        re += (double)x[k] * y[k] + (double)x[k + 1] * y[k + 1];
-        im += (double)x[k] * y[k + 1] - (double)x[k + 1] * y[k];
-        n += (double)x[k] * x[k] + (double)x[k + 1] * x[k + 1];
-      }
-      red[0][0] = re;
-      red[0][1] = im;
-      red[0][2] = n;
+      blas_dot(x, y, red[0][0], red[0][1]);
+      if (a.op == B_DOTNORM) red[0][2] = blas_norm<true>(x);
       break;
     }
     case B_COPY:
@@ -113,30 +142,24 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
       IO::load(a.x, rhs, s, x);
       IO::load(a.y, rhs, s, y);
       const T ar = (T)a.a.r(rhs), ai = (T)a.a.i(rhs), br = (T)a.b.r(rhs), bi = (T)a.b.i(rhs);
-      double n = 0;
 #pragma unroll
       for (int k = 0; k < 24; k += 2) {
         T yr = ar * x[k] - ai * x[k + 1] + br * y[k] - bi * y[k + 1];
         T yi = ar * x[k + 1] + ai * x[k] + br * y[k + 1] + bi * y[k];
         y[k] = yr;
         y[k + 1] = yi;
-        n += (double)yr * yr + (double)yi * yi;
       }
       IO::store(a.y, rhs, s, y);
-      red[0][0] = n;
+      if (a.op == B_CAXPBY_NORM) red[0][0] = blas_norm<true>(y);
       break;
     }
     case B_XMY_NORM: {
       IO::load(a.x, rhs, s, x);
       IO::load(a.y, rhs, s, y);
-      double n = 0;
 #pragma unroll
-      for (int k = 0; k < 24; k++) {
-        x[k] -= y[k];
-        n += (double)x[k] * x[k];
-      }
+      for (int k = 0; k < 24; k++) x[k] -= y[k];
       IO::store(a.z, rhs, s, x);
-      red[0][0] = n;
+      red[0][0] = blas_norm<false>(x);
       break;
     }
     case B_BICG_P: {  // x = r, y = p, z = v ; a = beta, b = omega
@@ -176,16 +199,8 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
       IO::store(a.y, rhs, s, y);
       T w[24];
       IO::load(a.w, rhs, s, w);
-      double n = 0, re = 0, im = 0;
-#pragma unroll
-      for (int k = 0; k < 24; k += 2) {
-        n += (double)y[k] * y[k] + (double)y[k + 1] * y[k + 1];
-        re += (double)w[k] * y[k] + (double)w[k + 1] * y[k + 1];
-        im += (double)w[k] * y[k + 1] - (double)w[k + 1] * y[k];
-      }
-      red[0][0] = n;
-      red[0][1] = re;
-      red[0][2] = im;
+      red[0][0] = blas_norm<true>(y);
+      blas_dot(w, y, red[0][1], red[0][2]);
       break;
     }
     case B_CG_P: {  // x = r, y = p ; a = b
@@ -207,10 +222,7 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
       caxpy_(y, -ar, -ai, mr);
       IO::store(a.x, rhs, s, x);
       IO::store(a.y, rhs, s, y);
-      double n = 0;
-#pragma unroll
-      for (int k = 0; k < 24; k++) n += (double)y[k] * y[k];
-      red[0][0] = n;
+      red[0][0] = blas_norm<false>(y);
       break;
     }
     case B_RICH_RX: {  // x = x, y = r, z = dx, w = t
@@ -219,16 +231,14 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
       IO::load(a.y, rhs, s, y);
       IO::load(a.z, rhs, s, dx);
       IO::load(a.w, rhs, s, t);
-      double n = 0;
 #pragma unroll
       for (int k = 0; k < 24; k++) {
         x[k] += dx[k];
         y[k] -= t[k];
-        n += (double)y[k] * y[k];
       }
       IO::store(a.x, rhs, s, x);
       IO::store(a.y, rhs, s, y);
-      red[0][0] = n;
+      red[0][0] = blas_norm<false>(y);
       break;
     }
     case B_G5: {
@@ -242,7 +252,7 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
       break;
     }
   }
-  if (a.red.mask) reduce_epilogue<1>(a.red, a.state, a.nrhs, rhs, a.red.mask, red);
+  if (a.red.mask) reduce_epilogue<1>(a.red, a.nrhs, rhs, a.red.mask, red);
 }
 
 // Multishift CG vector update (include/qphix/minvcg.h:279-384), fused across

@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+
 namespace qpx {
 
 enum Prec : int { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2, PREC_BF16 = 3, PREC_Q16 = 4, PREC_Q16F32 = 5 };
@@ -82,6 +84,63 @@ __device__ __forceinline__ f2 splat<f2>(double v) { return make_float2((float)v,
 __device__ __forceinline__ double lane(double v, int) { return v; }
 __device__ __forceinline__ float lane(float v, int) { return v; }
 __device__ __forceinline__ float lane(f2 v, int l) { return l ? v.y : v.x; }
+
+// ---- per-thread terms of the fused reductions ------------------------------
+// A thread sums the products of its own spinor elements in its arithmetic
+// type -- FP32 (float or float2 lanes) for 16-bit and FP32 storage, FP64 for
+// FP64 storage -- and converts each value to FP64 once; everything after
+// that (warps, blocks, the fold over blocks) adds in FP64.  Converting every
+// element instead costs two float -> double conversions per product on the
+// slow conversion pipe.  The FP64 forms are the plain element loops.
+// `act` masks the lanes of a two-site thread whose second site is past the
+// end of the lattice.
+__device__ __forceinline__ double red_total(float v, const bool *) { return (double)v; }
+__device__ __forceinline__ double red_total(f2 v, const bool *act)
+{
+  return (act[0] ? (double)v.x : 0.0) + (act[1] ? (double)v.y : 0.0);
+}
+
+// sum |x_k|^2 over the 24 reals of a thread's site(s)
+template <typename T>
+__device__ __forceinline__ double red_norm(const T *x, const bool *act)
+{
+  if constexpr (std::is_same<T, double>::value) {
+    double n = 0;
+#pragma unroll
+    for (int k = 0; k < 24; k++) n += x[k] * x[k];
+    return n;
+  } else {
+    T n = splat<T>(0.0);
+#pragma unroll
+    for (int k = 0; k < 24; k++) n = mad(x[k], x[k], n);
+    return red_total(n, act);
+  }
+}
+
+// <x, y> = sum conj(x) y over the 12 complex elements of a thread's site(s)
+template <typename T>
+__device__ __forceinline__ void red_dot(const T *x, const T *y, const bool *act, double &re, double &im)
+{
+  if constexpr (std::is_same<T, double>::value) {
+    double dre = 0, dim = 0;
+#pragma unroll
+    for (int k = 0; k < 24; k += 2) {
+      dre += x[k] * y[k] + x[k + 1] * y[k + 1];
+      dim += x[k] * y[k + 1] - x[k + 1] * y[k];
+    }
+    re = dre;
+    im = dim;
+  } else {
+    T dre = splat<T>(0.0), dim = splat<T>(0.0);
+#pragma unroll
+    for (int k = 0; k < 24; k += 2) {
+      dre = mad(x[k], y[k], mad(x[k + 1], y[k + 1], dre));
+      dim = mad(x[k], y[k + 1], mad(-x[k + 1], y[k], dim));
+    }
+    re = red_total(dre, act);
+    im = red_total(dim, act);
+  }
+}
 
 // complex products with explicit fused multiply-adds
 // c + a b

@@ -209,6 +209,70 @@ struct HalfProjection<Lanes<F16, 1>> {
   static constexpr bool value = true;
 };
 
+// the same for two right-hand sides in the lanes (RhsLanes<F16>): each rhs is
+// projected on its raw half2 words and the 12 results widened into the lanes
+template <int MU, int SG>
+__device__ __forceinline__ void project_h2_pair(const SpinorArg &f, int rhs, long long s, cx<f2> h[2][3], f2 &nrm)
+{
+  __half2 wa[12], wb[12];
+  float na, nb;
+  load_h2(f, rhs, s, wa, na);
+  load_h2(f, rhs + 1, s, wb, nb);
+  cx<float> ha[2][3], hb[2][3];
+  project_h2<MU, SG>(wa, ha);
+  project_h2<MU, SG>(wb, hb);
+#pragma unroll
+  for (int sp = 0; sp < 2; sp++)
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      h[sp][c] = {make_float2(ha[sp][c].re, hb[sp][c].re), make_float2(ha[sp][c].im, hb[sp][c].im)};
+  nrm = make_float2(na, nb);
+}
+
+template <typename Lane>
+struct RhsHalfProjection {
+  static constexpr bool value = false;
+};
+template <>
+struct RhsHalfProjection<RhsLanes<F16>> {
+  static constexpr bool value = true;
+};
+
+// a per-rhs solver coefficient in the arithmetic type: the lanes of a
+// two-rhs thread take right-hand sides rr and rr + 1
+template <bool RL, typename T>
+__device__ __forceinline__ T rhs_coef(const double *v, int rr)
+{
+  if constexpr (RL)
+    return make_float2((float)v[rr], (float)v[rr + 1]);
+  else
+    return splat<T>(v[rr]);
+}
+
+// the per-lane parts of the fused reductions of a two-rhs thread: lane 0
+// belongs to right-hand side rr, lane 1 to rr + 1
+__device__ __forceinline__ void red_norm_pair(const f2 *x, double &n0, double &n1)
+{
+  f2 n = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 24; k++) n = mad(x[k], x[k], n);
+  n0 = (double)n.x;
+  n1 = (double)n.y;
+}
+__device__ __forceinline__ void red_dot_pair(const f2 *x, const f2 *y, double *re, double *im)
+{
+  f2 dre = make_float2(0.f, 0.f), dim = make_float2(0.f, 0.f);
+#pragma unroll
+  for (int k = 0; k < 24; k += 2) {
+    dre = mad(x[k], y[k], mad(x[k + 1], y[k + 1], dre));
+    dim = mad(x[k], y[k + 1], mad(-x[k + 1], y[k], dim));
+  }
+  re[0] = (double)dre.x;
+  re[1] = (double)dre.y;
+  im[0] = (double)dim.x;
+  im[1] = (double)dim.y;
+}
+
 // --- reconstruct-accumulate of (1 + SG gamma_mu) from chi = U h -------------
 // QPX_ADD(k, v): acc[k] += SG v ; QPX_SUB(k, v): acc[k] -= SG v (signs
 // resolved at compile time)
@@ -446,23 +510,33 @@ __device__ __forceinline__ void lanes_set(f2 &d, const double *v) { d = make_flo
 // GEN    honour a.dir_mask and twisted boundary phases.  Without GEN every
 //        hop is taken and no phase applied: the hops are then straight-line
 //        code and the compiler can schedule every load early.
+// RL     (with SP = 2, R = 1, fast path) the float2 lanes hold two
+//        right-hand sides of one site instead of two sites: links and
+//        clover terms are loaded once for both (RhsLanes).
 // Blocks cover (site block, rhs tile) pairs with the rhs tile varying
 // fastest, so the blocks that share a site block (and its links) run
 // together and the links of the later right-hand sides come from L2.
-template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN, int SP, bool GEN>
+template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN, int SP, bool GEN, bool RL = false>
 __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
 {
-  using L = Lanes<P, SP>;
+  using L = typename std::conditional<RL, RhsLanes<P>, Lanes<P, SP>>::type;
   using T = typename L::T;
   static_assert(SP == 1 || R == 1, "two sites per thread take one right-hand side");
+  static_assert(!RL || (SP == 2 && R == 1 && !GEN), "right-hand-side lanes: SP = 2, R = 1, fast path");
+  constexpr int RT = RL ? 2 : R;  // right-hand sides per thread
   if (a.state && a.state->done) return;
-  const int ntiles = a.nrhs / R;
+  const int ntiles = a.nrhs / RT;
   const int tile = blockIdx.x % ntiles;
   const int sblock = blockIdx.x / ntiles;
-  const int rhs0 = tile * R;
+  const int rhs0 = tile * RT;
   int s[SP];
   bool act[SP];
-  if (SP == 1) {
+  if (RL) {
+    s[0] = sblock * QPX_BLOCK + threadIdx.x;
+    act[0] = s[0] < a.geom.vh;
+    s[SP - 1] = s[0];
+    act[SP - 1] = act[0];
+  } else if (SP == 1) {
     s[0] = sblock * QPX_BLOCK + threadIdx.x;
     act[0] = s[0] < a.geom.vh;
   } else {
@@ -474,9 +548,9 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
     act[SP - 1] = base + 32 < a.geom.vh;
     s[SP - 1] = act[SP - 1] ? base + 32 : base;
   }
-  double red[R][QPX_MAX_RED];
+  double red[RT][QPX_MAX_RED];
 #pragma unroll
-  for (int r = 0; r < R; r++)
+  for (int r = 0; r < RT; r++)
 #pragma unroll
     for (int k = 0; k < QPX_MAX_RED; k++) red[r][k] = 0.0;
 
@@ -488,7 +562,7 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
     int nb[4][2][SP];  // [mu][0 back, 1 forward][lane]
     bool tlast[SP], tfirst[SP];
 #pragma unroll
-    for (int l = 0; l < SP; l++) {
+    for (int l = 0; l < (RL ? 1 : SP); l++) {
       int xh, y, z, t, par;
       const int sl = s[l];
       site_coords(g, sl, a.cb, xh, y, z, t, par);
@@ -504,6 +578,14 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
       nb[3][0][l] = sl + ((t == 0) ? (g.nt - 1) * sxyzt : -sxyzt);
       tlast[l] = (t + 1 == g.nt);
       tfirst[l] = (t == 0);
+    }
+    if (RL) {  // both lanes are the same site
+#pragma unroll
+      for (int mu = 0; mu < 4; mu++)
+#pragma unroll
+        for (int d = 0; d < 2; d++) nb[mu][d][SP - 1] = nb[mu][d][0];
+      tlast[SP - 1] = tlast[0];
+      tfirst[SP - 1] = tfirst[0];
     }
     const T zero = splat<T>(0.0);
     T acc[R][24];
@@ -540,6 +622,8 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
           __half2 w[12];                                                                  \
           load_h2(ghf ? a.ghost_fwd : a.in, rhs0 + r, ixf[0], w, nrm);                    \
           project_h2<MU, -ISIGN>(w, h);                                                   \
+        } else if constexpr (RhsHalfProjection<L>::value) {                               \
+          project_h2_pair<MU, -ISIGN>(a.in, rhs0 + r, ixf[0], h, nrm);                    \
         } else {                                                                          \
           T psi[24];                                                                      \
           L::load_raw(ghf ? a.ghost_fwd : a.in, rhs0 + r, ixf, psi, nrm);                 \
@@ -582,6 +666,8 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
           __half2 w[12];                                                                  \
           load_h2(ghb ? a.ghost_bwd : a.in, rhs0 + r, ixb[0], w, nrm);                    \
           project_h2<MU, ISIGN>(w, h);                                                    \
+        } else if constexpr (RhsHalfProjection<L>::value) {                               \
+          project_h2_pair<MU, ISIGN>(a.in, rhs0 + r, ixb[0], h, nrm);                     \
         } else {                                                                          \
           T psi[24];                                                                      \
           L::load_raw(ghb ? a.ghost_bwd : a.in, rhs0 + r, ixb, psi, nrm);                 \
@@ -775,22 +861,16 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
       }
       // <out, chi> reduction needs chi
       if (a.red.mask & RED_DOT_OUT_CHI) {
+        if constexpr (RL) {
+          double re[2], im[2];
+          red_dot_pair(res[0], chi[0], re, im);
+          red[0][3] = re[0];
+          red[0][4] = im[0];
+          red[1][3] = re[1];
+          red[1][4] = im[1];
+        } else {
 #pragma unroll
-        for (int r = 0; r < R; r++) {
-          double dre = 0, dim = 0;
-#pragma unroll
-          for (int l = 0; l < SP; l++) {
-            if (!act[l]) continue;
-#pragma unroll
-            for (int k = 0; k < 24; k += 2) {
-              const double xr = lane(res[r][k], l), xi = lane(res[r][k + 1], l);
-              const double cr = lane(chi[r][k], l), ci = lane(chi[r][k + 1], l);
-              dre += xr * cr + xi * ci;
-              dim += xr * ci - xi * cr;
-            }
-          }
-          red[r][3] = dre;
-          red[r][4] = dim;
+          for (int r = 0; r < R; r++) red_dot(res[r], chi[r], act, red[r][3], red[r][4]);
         }
       }
     }
@@ -801,52 +881,40 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
       const int rr = rhs0 + r;
       if (rr >= a.nrhs) continue;
       if (a.red.mask & RED_NORM_OUT) {
-        double n2 = 0;
-#pragma unroll
-        for (int l = 0; l < SP; l++) {
-          if (!act[l]) continue;
-#pragma unroll
-          for (int k = 0; k < 24; k++) n2 += (double)lane(res[r][k], l) * lane(res[r][k], l);
-        }
-        red[r][0] = n2;
+        if constexpr (RL)
+          red_norm_pair(res[0], red[0][0], red[1][0]);
+        else
+          red[r][0] = red_norm(res[r], act);
       }
       if (a.red.mask & RED_DOT_W_OUT) {
         T w[24];
         L::load(a.w, rr, s, w);
-        double dre = 0, dim = 0;
-#pragma unroll
-        for (int l = 0; l < SP; l++) {
-          if (!act[l]) continue;
-#pragma unroll
-          for (int k = 0; k < 24; k += 2) {
-            const double wr = lane(w[k], l), wi = lane(w[k + 1], l);
-            const double xr = lane(res[r][k], l), xi = lane(res[r][k + 1], l);
-            dre += wr * xr + wi * xi;
-            dim += wr * xi - wi * xr;
-          }
+        if constexpr (RL) {
+          double re[2], im[2];
+          red_dot_pair(w, res[0], re, im);
+          red[0][1] = re[0];
+          red[0][2] = im[0];
+          red[1][1] = re[1];
+          red[1][2] = im[1];
+        } else {
+          red_dot(w, res[r], act, red[r][1], red[r][2]);
         }
-        red[r][1] = dre;
-        red[r][2] = dim;
       }
       if (a.post == POST_STORE) {
         L::store(a.out, rr, s, act, res[r]);
       } else if (a.post == POST_RAXPY) {  // r += b mmp ; |r|^2
-        const T cb_ = splat<T>(a.state->v[S_B][rr]);
+        const T cb_ = rhs_coef<RL, T>(a.state->v[S_B], rr);
         T rv[24];
         L::load(a.r, rr, s, rv);
 #pragma unroll
         for (int k = 0; k < 24; k++) rv[k] = mad(cb_, res[r][k], rv[k]);
-        double n2 = 0;
-#pragma unroll
-        for (int l = 0; l < SP; l++) {
-          if (!act[l]) continue;
-#pragma unroll
-          for (int k = 0; k < 24; k++) n2 += (double)lane(rv[k], l) * lane(rv[k], l);
-        }
         L::store(a.r, rr, s, act, rv);
-        red[r][5] = n2;
+        if constexpr (RL)
+          red_norm_pair(rv, red[0][5], red[1][5]);
+        else
+          red[r][5] = red_norm(rv, act);
       } else {  // POST_CG: r -= a mmp ; x += a p ; |r|^2
-        const T ca = splat<T>(a.state->v[S_A][rr]), nca = splat<T>(-a.state->v[S_A][rr]);
+        const T ca = rhs_coef<RL, T>(a.state->v[S_A], rr), nca = -ca;
         T rv[24], xv[24], pv[24];
         L::load(a.r, rr, s, rv);
         L::load(a.x, rr, s, xv);
@@ -856,22 +924,17 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
           rv[k] = mad(nca, res[r][k], rv[k]);
           xv[k] = mad(ca, pv[k], xv[k]);
         }
-        double n2 = 0;
-#pragma unroll
-        for (int l = 0; l < SP; l++) {
-          if (!act[l]) continue;
-#pragma unroll
-          for (int k = 0; k < 24; k++) n2 += (double)lane(rv[k], l) * lane(rv[k], l);
-        }
         L::store(a.r, rr, s, act, rv);
         L::store(a.x, rr, s, act, xv);
-        red[r][5] = n2;
+        if constexpr (RL)
+          red_norm_pair(rv, red[0][5], red[1][5]);
+        else
+          red[r][5] = red_norm(rv, act);
       }
     }
   }
   if (a.red.mask)
-    reduce_epilogue<R>(a.red, a.state, a.nrhs, rhs0, red_slots(a.red.mask), red, sblock,
-                       (int)(gridDim.x / ntiles));
+    reduce_epilogue<RT>(a.red, a.nrhs, rhs0, red_slots(a.red.mask), red, sblock);
 }
 
 }  // namespace qpx

@@ -64,7 +64,6 @@ struct qphix_gpu_lattice_s {
   // reduction workspace (one in-flight reduction per stream at a time)
   double *partials = nullptr;
   size_t partials_len = 0;
-  unsigned int *ticket = nullptr;
   double *result = nullptr;       // device [QPX_MAX_RHS * QPX_MAX_RED]
   double *h_result = nullptr;     // pinned mirror
   qpx::SolverState *state = nullptr;   // device
@@ -159,11 +158,15 @@ void lattice_trim(qphix_gpu_lattice_s *L);
 struct DslashShape {
   int R = 1, SP = 1;
   bool gen = false;
+  bool rl = false;  // with R = 1, SP = 2: two right-hand sides of one site in the float2 lanes
 };
 // a == nullptr: report only whether the shape is built for (prec, recon)
 bool launch_dslash(int prec, int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
                    cudaStream_t st);
 void launch_blas(int prec, const BlasArgs &a, dim3 grid, cudaStream_t st);
+// folds the block partials of the reducing launch just issued on `st` (nparts
+// site blocks) and runs its finalize step (fold_kernel, blas.cu)
+void launch_fold(const ReduceArg &ra, SolverState *state, int nrhs, int nparts, cudaStream_t st);
 void launch_convert(int pdst, int psrc, int vh, SpinorArg src, SpinorArg dst, Coef scale, SolverState *state,
                     dim3 grid, cudaStream_t st, int accumulate = 0);
 void launch_spinor_in(int prec, Geom g, HostLayout L, const void *host, SpinorArg f, int nrhs, dim3 grid,

@@ -246,6 +246,66 @@ struct Lanes<F32, 2> {
   }
 };
 
+// ---- two right-hand sides in the lanes ---------------------------------------
+// RhsLanes<P>: one lattice site per thread and two right-hand sides, rhs and
+// rhs + 1, in the .x / .y lanes of f2, so the paired FP32 instructions do the
+// arithmetic of both while every link and clover element is loaded,
+// converted and (12-real) reconstructed once for the pair and broadcast to
+// both lanes.  Both lanes are active or neither (`act` holds the site's
+// flag twice).  For the FP32-arithmetic precisions only.
+template <typename P>
+struct RhsLanes {
+  using T = f2;
+  __device__ __forceinline__ static void load_raw(const SpinorArg &f, int rhs, const int *s, f2 v[24], f2 &nrm)
+  {
+    float a[24], b[24], na, nb;
+    SpinorIO<P>::load_raw(f, rhs, s[0], a, na);
+    SpinorIO<P>::load_raw(f, rhs + 1, s[0], b, nb);
+#pragma unroll
+    for (int k = 0; k < 24; k++) v[k] = make_float2(a[k], b[k]);
+    nrm = make_float2(na, nb);
+  }
+  __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, const int *s, f2 v[24])
+  {
+    float a[24], b[24];
+    SpinorIO<P>::load(f, rhs, s[0], a);
+    SpinorIO<P>::load(f, rhs + 1, s[0], b);
+#pragma unroll
+    for (int k = 0; k < 24; k++) v[k] = make_float2(a[k], b[k]);
+  }
+  __device__ __forceinline__ static void store(const SpinorArg &f, int rhs, const int *s, const bool *act,
+                                               const f2 v[24])
+  {
+    if (!act[0]) return;
+    float a[24], b[24];
+#pragma unroll
+    for (int k = 0; k < 24; k++) {
+      a[k] = v[k].x;
+      b[k] = v[k].y;
+    }
+    SpinorIO<P>::store(f, rhs, s[0], a);
+    SpinorIO<P>::store(f, rhs + 1, s[0], b);
+  }
+  template <int RECON>
+  __device__ __forceinline__ static void load_link(const GaugeArg &g, int cb, int mu, const int *s, cx<f2> u[3][3])
+  {
+    cx<float> w[3][3];
+    GaugeIO<P, RECON>::load(g, cb, mu, s[0], w);
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) u[i][j] = {make_float2(w[i][j].re, w[i][j].re), make_float2(w[i][j].im, w[i][j].im)};
+  }
+  template <int NR>
+  __device__ __forceinline__ static void load_clover(const CloverArg &c, const int *s, int k0, int n, f2 *v)
+  {
+    float w[144];
+    CloverIO<P, NR>::load(c, s[0], k0, n, w);
+#pragma unroll
+    for (int k = 0; k < n; k++) v[k] = make_float2(w[k], w[k]);
+  }
+};
+
 // Q16 spinors, FP32 links and clover terms
 template <>
 struct Lanes<Q16F32, 2> {

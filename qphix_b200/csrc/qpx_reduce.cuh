@@ -3,12 +3,13 @@
 //
 // Every reducing kernel computes up to QPX_MAX_RED doubles per right-hand
 // side per thread, reduces them over the block (warp shuffles, then a fixed
-// order over warps, one barrier for all values), writes one partial per
-// (block, rhs, value), and the last block to finish (atomic ticket) folds the
-// partials -- four values at a time, thread t adds site blocks t, t + 128,
-// ... in order, then a shuffle tree per warp and the warps in order -- and
-// runs a finalize step on thread 0.  The order of every addition is fixed by the
-// launch shape, so results are bitwise reproducible run to run.
+// order over warps, one barrier for all values) and writes one partial per
+// (block, rhs, value).  fold_kernel (blas.cu), launched next on the
+// same stream, adds the partials of every value in a fixed order -- a group
+// of warps per value, lane l of warp g taking site blocks in a fixed stride,
+// then shuffle trees and the group's warps in order -- and runs a finalize
+// step on thread 0.  The order of every addition is fixed by the launch
+// shape, so results are bitwise reproducible run to run.
 //
 // The finalize step updates a SolverState in device memory (Krylov scalars
 // alpha, beta, omega, rho, residual norms, convergence flags) so that a
@@ -66,7 +67,6 @@ struct ReduceArg {
   int nval;            // number of doubles per rhs
   int fin;             // FinOp
   double *partials;    // [nblocks][nrhs][nval]
-  unsigned int *ticket;
   double *result;      // [nrhs][nval]
 };
 
@@ -84,23 +84,20 @@ __device__ inline void finalize(int fin, SolverState *st, const double *res, int
 // time indices so they stay in registers); `slots` (ReduceArg::mask of the
 // producing kernel, translated by it into a slot bit set) says which slots
 // are live, and they are packed in slot order into nval doubles per rhs.
-// rhs0 = first rhs of the block's tile.  The last block runs the finalize.
-// The block's partials are stored under site-block index `sblock` of
-// `nsblocks` (default: blockIdx.x of gridDim.x; kernels whose blocks cover
-// (site block, rhs tile) pairs in one grid dimension pass their own).
+// rhs0 = first rhs of the block's tile.  Each block writes one partial per
+// (rhs, value) under site-block index `sblock` (default: blockIdx.x;
+// kernels whose blocks cover (site block, rhs tile) pairs in one grid
+// dimension pass their own) and is done: the partials are folded, and the
+// solver's finalize step run, by fold_kernel, launched after the producing
+// kernel on the same stream.  Blocks therefore never wait on one another or
+// on a device-wide fence, and the fold runs with a full block of threads.
 template <int R>
-__device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, SolverState *st, int nrhs, int rhs0,
-                                                int slots, const double val[R][QPX_MAX_RED], int sblock = -1,
-                                                int nsblocks = -1)
+__device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, int nrhs, int rhs0, int slots,
+                                                const double val[R][QPX_MAX_RED], int sblock = -1)
 {
   constexpr int NW = QPX_BLOCK / 32;  // launches of these kernels use QPX_BLOCK threads
   __shared__ double wpart[NW][R * QPX_MAX_RED];
-  __shared__ bool am_last;
-  if (sblock < 0) {
-    sblock = blockIdx.x;
-    nsblocks = gridDim.x;
-  }
-  const long long nblocks = (long long)gridDim.x * gridDim.y;
+  if (sblock < 0) sblock = blockIdx.x;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   // every live value's warp sum, then one barrier and a fixed-order sum over warps
 #pragma unroll
@@ -127,57 +124,8 @@ __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, SolverState
       }
     }
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    unsigned int t = atomicAdd(ra.ticket, 1u);
-    am_last = (t == (unsigned int)(nblocks - 1));
-  }
-  __syncthreads();
-  if (!am_last) return;
-  __threadfence();
-  // last block: fold the partials of every site block.  All threads split
-  // the site blocks, four values at a time, so that many loads are in flight
-  // even when a launch reduces only a few values over thousands of blocks.
-  __shared__ double wsum[NW][4];
-  const int gx = nsblocks, nres = nrhs * ra.nval;
-  const long long row = (long long)nres;
-  for (int v0 = 0; v0 < nres; v0 += 4) {
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 4
-    for (int b = threadIdx.x; b < gx; b += QPX_BLOCK) {
-      const double *p = ra.partials + b * row + v0;
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        if (v0 + j < nres) acc[j] += __ldcg(p + j);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const double s = warp_sum(acc[j]);
-      if (lane == 0) wsum[wid][j] = s;
-    }
-    __syncthreads();
-    if (threadIdx.x < 4 && v0 + (int)threadIdx.x < nres) {
-      double s = 0.0;
-      for (int w = 0; w < NW; w++) s += wsum[w][threadIdx.x];
-      ra.result[v0 + threadIdx.x] = s;
-    }
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    *ra.ticket = 0u;
-    __threadfence();
-    // two-flavour systems: each flavour pair's reductions are one sum (the
-    // reference's num_flav = 2 BLAS), so both get the same solver scalars
-    if (st && st->coupled)
-      for (int r = 0; r + 1 < nrhs; r += 2)
-        for (int k = 0; k < ra.nval; k++) {
-          const double s = ra.result[r * ra.nval + k] + ra.result[(r + 1) * ra.nval + k];
-          ra.result[r * ra.nval + k] = s;
-          ra.result[(r + 1) * ra.nval + k] = s;
-        }
-    if (ra.fin != FIN_NONE && st) finalize(ra.fin, st, ra.result, nrhs, ra.nval);
-  }
 }
+
+constexpr int QPX_FOLD_THREADS = 1024;
 
 }  // namespace qpx

@@ -1,6 +1,7 @@
 """Dslash kernel micro-benchmark: one kernel variant, timed alone.
 
     python -m qphix_b200.dslash_bench --lattice 32 32 32 64 --prec f16 --kind clover --nrhs 1
+    python -m qphix_b200.dslash_bench --lattice 16 16 16 32 --nrhs 8 --achi --norms --shape sp2
 
 Times `--iters` launches of one Dslash variant with CUDA events on the
 lattice's stream, L2 flushed (a 256 MiB write) before every launch, and
@@ -33,6 +34,12 @@ def algorithmic_bytes(prec, recon, kind, nrhs, achi=False):
     return nrhs * (2 * spinor + (spinor if achi else 0)) + links + extra
 
 
+SHAPES = {"auto": {}, "sp1": {"QPHIX_GPU_RHS_TILE": "1", "QPHIX_GPU_SITES_PER_THREAD": "1"},
+          "sp2": {"QPHIX_GPU_RHS_TILE": "1", "QPHIX_GPU_SITES_PER_THREAD": "2"},
+          "r2": {"QPHIX_GPU_RHS_TILE": "2", "QPHIX_GPU_SITES_PER_THREAD": "1"},
+          "rhs_lanes": {"QPHIX_GPU_RHS_LANES": "1"}}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--lattice", type=int, nargs=4, default=[32, 32, 32, 64])
@@ -43,7 +50,16 @@ def main(argv=None):
     ap.add_argument("--nrhs", type=int, default=1)
     ap.add_argument("--iters", type=int, default=20)
     ap.add_argument("--no-flush", action="store_true")
+    ap.add_argument("--shape", default="auto", choices=list(SHAPES),
+                    help="launch shape: auto (the autotuner's), sp1 / sp2 (sites per thread), r2 (two rhs per "
+                         "thread), rhs_lanes (two rhs in the float2 lanes)")
+    ap.add_argument("--norms", action="store_true",
+                    help="with --achi --kind clover: fuse the |res|^2 and <res, chi> reductions (BiCGStab's "
+                         "t = M s launch), folded on the device")
     args = ap.parse_args(argv)
+    import os
+    for k, v in SHAPES[args.shape].items():
+        os.environ[k] = v
 
     import torch
 
@@ -85,8 +101,11 @@ def main(argv=None):
             (lambda: D.dslash(out, psi, u, 1, 0))
     elif args.kind == "clover":
         D = api.ClovDslash(lat, -1.0, 1.0, 1.0)
-        run = (lambda: D.dslashAChiMinusBDPsi(out, psi, chi, u, clov, 0.25, 1, 0)) if args.achi else \
-            (lambda: D.dslash(out, psi, u, inv, 1, 0))
+        if args.achi and args.norms:
+            run = lambda: D.dslashAChiMinusBDPsiNorms(out, psi, chi, u, clov, 0.25, 1, 0, fetch=False)
+        else:
+            run = (lambda: D.dslashAChiMinusBDPsi(out, psi, chi, u, clov, 0.25, 1, 0)) if args.achi else \
+                (lambda: D.dslash(out, psi, u, inv, 1, 0))
     else:
         D = api.TMClovDslash(lat, -1.0, 1.0, 1.0, prec_mass_rho=0.05)
         run = (lambda: D.dslashAChiMinusBDPsi(out, psi, chi, u, clov, 0.25, 1, 0)) if args.achi else \
@@ -109,7 +128,8 @@ def main(argv=None):
     per_site = algorithmic_bytes(args.prec, args.recon, args.kind, args.nrhs, args.achi)
     gbs = per_site * vh / t / 1e9
     print(json.dumps({"lattice": list(dims), "prec": args.prec, "recon": args.recon, "kind": args.kind,
-                      "achi": args.achi, "nrhs": args.nrhs, "sites": vh, "bytes_per_site": per_site,
+                      "achi": args.achi, "norms": args.norms, "shape": args.shape, "nrhs": args.nrhs, "sites": vh,
+                      "bytes_per_site": per_site,
                       "launch_us": round(t * 1e6, 2), "min_us": round(min(times) * 1e6, 2),
                       "GBps": round(gbs, 1), "flops_per_site": args.nrhs * 1320}))
 

@@ -52,20 +52,26 @@ def c2_oracle(oracle, c2):
     return L, oracle.OracleOp("clover", L, c2["gauge"], clov=c2["clov_odd"], invclov=c2["invclov_even"])
 
 
-class forced_shape:
-    """Force the Dslash launch shape (rhs per thread R, sites per thread SP)
-    through the library's QPHIX_GPU_RHS_TILE / QPHIX_GPU_SITES_PER_THREAD."""
+SHAPE_ENV = {"sp1": {"QPHIX_GPU_RHS_TILE": "1", "QPHIX_GPU_SITES_PER_THREAD": "1"},
+             "r2": {"QPHIX_GPU_RHS_TILE": "2", "QPHIX_GPU_SITES_PER_THREAD": "1"},
+             "sp2": {"QPHIX_GPU_RHS_TILE": "1", "QPHIX_GPU_SITES_PER_THREAD": "2"},
+             "rhs_lanes": {"QPHIX_GPU_RHS_LANES": "1"}}
 
-    def __init__(self, R, SP):
-        self.R, self.SP = R, SP
+
+class forced_shape:
+    """Force the Dslash launch shape (rhs per thread, sites per thread, or two
+    rhs in the float2 lanes) through the library's QPHIX_GPU_RHS_TILE /
+    QPHIX_GPU_SITES_PER_THREAD / QPHIX_GPU_RHS_LANES."""
+
+    def __init__(self, name):
+        self.env = SHAPE_ENV[name]
 
     def __enter__(self):
-        os.environ["QPHIX_GPU_RHS_TILE"] = str(self.R)
-        os.environ["QPHIX_GPU_SITES_PER_THREAD"] = str(self.SP)
+        os.environ.update(self.env)
 
     def __exit__(self, *exc):
-        os.environ.pop("QPHIX_GPU_RHS_TILE", None)
-        os.environ.pop("QPHIX_GPU_SITES_PER_THREAD", None)
+        for k in self.env:
+            os.environ.pop(k, None)
 
 
 def test_c2_fp64_operator_8rhs(api, c2, c2_oracle):
@@ -85,8 +91,8 @@ def test_c2_fp64_operator_8rhs(api, c2, c2_oracle):
 
 
 @pytest.mark.parametrize("prec", ["f16", "f32", "f64"])
-@pytest.mark.parametrize("R,SP", [(1, 1), (2, 1), (1, 2)])
-def test_c2_inner_kernels_every_shape(api, oracle, c2, c2_oracle, prec, R, SP):
+@pytest.mark.parametrize("shape", ["sp1", "r2", "sp2", "rhs_lanes"])
+def test_c2_inner_kernels_every_shape(api, oracle, c2, c2_oracle, prec, shape):
     """The inner operator's two clover Dslash launches at 16^3x32 x 8 rhs in
     each built launch shape: A^-1 D psi and A chi - b D psi with the three
     fused reductions, against the oracle and numpy."""
@@ -104,7 +110,7 @@ def test_c2_inner_kernels_every_shape(api, oracle, c2, c2_oracle, prec, R, SP):
     tmp = lat.spinor(prec, 8)
     out = lat.spinor(prec, 8)
     D = api.ClovDslash(lat, -1.0, 1.0, 1.0)
-    with forced_shape(R, SP):
+    with forced_shape(shape):
         D.dslash(tmp, psi, u, Ai, 1, 0)
         norms = D.dslashAChiMinusBDPsiNorms(out, tmp, chi, u, A, 0.25, 1, 1, w=w)
     tol = TOL[prec]

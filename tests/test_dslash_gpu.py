@@ -180,7 +180,8 @@ def test_half_error_is_stated(api, oracle, setup):
 
 SHAPES = [("sp1", {"QPHIX_GPU_SITES_PER_THREAD": "1", "QPHIX_GPU_RHS_TILE": "1"}),
           ("sp2", {"QPHIX_GPU_SITES_PER_THREAD": "2", "QPHIX_GPU_RHS_TILE": "1"}),
-          ("r2", {"QPHIX_GPU_SITES_PER_THREAD": "1", "QPHIX_GPU_RHS_TILE": "2"})]
+          ("r2", {"QPHIX_GPU_SITES_PER_THREAD": "1", "QPHIX_GPU_RHS_TILE": "2"}),
+          ("rhs_lanes", {"QPHIX_GPU_RHS_LANES": "1"})]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda s: s[0])
@@ -188,8 +189,9 @@ SHAPES = [("sp1", {"QPHIX_GPU_SITES_PER_THREAD": "1", "QPHIX_GPU_RHS_TILE": "1"}
 @pytest.mark.parametrize("dims", [(6, 4, 4, 6), (8, 8, 8, 8)], ids=lambda d: "x".join(map(str, d)))
 def test_launch_shapes(api, oracle, monkeypatch, shape, prec, dims):
     """Every built kernel shape (sites per thread, right-hand sides per
-    thread) against the oracle with two right-hand sides; 6x4x4x6 has 288
-    sites per checkerboard, so its last warp is only partly filled."""
+    thread, two right-hand sides in the float2 lanes) against the oracle with
+    two right-hand sides, for every epilogue; 6x4x4x6 has 288 sites per
+    checkerboard, so its last warp is only partly filled."""
     for k, v in shape[1].items():
         monkeypatch.setenv(k, v)
     s = make_setup(dims)
@@ -205,6 +207,7 @@ def test_launch_shapes(api, oracle, monkeypatch, shape, prec, dims):
     D = api.Dslash(lat, -1.0, 1.0, 1.0)
     Cd = api.ClovDslash(lat, -1.0, 1.0, 1.0, prec_mass_rho=0.11)
     T = api.TMClovDslash(lat, -1.0, 1.0, 1.0, prec_mass_rho=s["mu"])
+    Tm = api.TMDslash(lat, -1.0, 1.0, 1.0, s["mass"], s["mu"])
     for cb in (0, 1):
         A = lat.clover(prec).upload(s["clov"][cb])
         Ai = lat.clover(prec).upload(s["invclov"][cb])
@@ -233,6 +236,22 @@ def test_launch_shapes(api, oracle, monkeypatch, shape, prec, dims):
             for i in range(2):
                 ref = oracle.tmclov_dslash(L, psi[i], s["gauge"], f0, f1, isign, cb)
                 assert rel_l2(out[i], ref) < TOL[prec], ("tmclover", cb, isign, i)
+            D.dslashAChiMinusBDPsi(gr, gp, gc, u, 1.3, 0.27, isign, cb)
+            out = gr.download()
+            for i in range(2):
+                ref = oracle.dslash_achimbdpsi(L, psi[i], chi[i], s["gauge"], 1.3, 0.27, isign, cb)
+                assert rel_l2(out[i], ref) < TOL[prec], ("wilson achi", cb, isign, i)
+            Tm.dslash(gr, gp, u, isign, cb)
+            out = gr.download()
+            for i in range(2):
+                ref = oracle.tm_dslash(L, psi[i], s["gauge"], s["mass"], s["mu"], isign, cb)
+                assert rel_l2(out[i], ref) < TOL[prec], ("tm", cb, isign, i)
+            Tm.dslashAChiMinusBDPsi(gr, gp, gc, u, 4.0 + s["mass"], 0.25, isign, cb, -1.0)
+            out = gr.download()
+            for i in range(2):
+                ref = oracle.tm_achimbdpsi(L, psi[i], chi[i], s["gauge"], 4.0 + s["mass"], 0.25, s["mass"], s["mu"],
+                                           isign, cb, -1.0)
+                assert rel_l2(out[i], ref) < TOL[prec], ("tm achi", cb, isign, i)
 
 
 def test_autotuner_records_shapes(api, setup):
@@ -248,4 +267,4 @@ def test_autotuner_records_shapes(api, setup):
     key = "dslash p2 r12 e0 a0 %dx%dx%dx%d n2" % tuple(dims)
     assert key in entries, entries
     R, SP, us = entries[key]
-    assert (R, SP) in [(1, 1), (1, 2), (2, 1)] and us > 0
+    assert (R, SP) in [(1, 1), (1, 2), (2, 1), (2, 0)] and us > 0
