@@ -293,8 +293,9 @@ def extra_configs():
     headline (N = 1, rank 0): 8^4 Wilson CG, the 24^3x48 24-rhs batched
     twisted-mass clover solve, the 32^3x64 16-shift multishift CG
     (qphix_b200.workloads) and the 2000-request Poisson serving stream at 70 %
-    of measured capacity (qphix_b200.serve_bench), whose latency p50 / p99
-    are the metric's "p99 ms"."""
+    of measured capacity (qphix_b200.serve_bench, requests solved with
+    InvRichardsonMultiPrec), whose latency p50 / p99 are the metric's "p99
+    ms"."""
     import types
 
     from qphix_b200 import serve_bench, workloads
@@ -308,7 +309,7 @@ def extra_configs():
         out[name]["wall_s"] = round(time.perf_counter() - t0, 1)
     t0 = time.perf_counter()
     try:
-        out["serve"] = serve_bench.run(["--requests", "2000", "--load", "0.7"])
+        out["serve"] = serve_bench.run(["--requests", "2000", "--load", "0.7", "--solver", "richardson"])
     except Exception as e:  # pragma: no cover
         out["serve"] = {"error": f"{type(e).__name__}: {e}"}
     out["serve"]["wall_s_total"] = round(time.perf_counter() - t0, 1)
@@ -614,6 +615,12 @@ def main():
     roof_big = {"lattice": list(big), "nrhs": 1, "bytes_per_site": ps2, "achieved": round(ps2 * vh2 / t2 / 1e9, 1),
                 "frac": round(ps2 * vh2 / t2 / 1e9 / peak, 4), "launch_us": round(t2 * 1e6, 1),
                 "traffic": (round(traffic2 * vh2) if traffic2 else None)}
+    # the same A^-1 D psi launch with FP32 and FP64 storage (the FP64 outer
+    # operator's and the FP32 configurations' kernel), HBM-bound at this size
+    for wide in ("f32", "f64"):
+        psw, vhw, tw = dslash_roofline(big, wide, 1, n=10)
+        roof_big[wide] = {"bytes_per_site": psw, "achieved": round(psw * vhw / tw / 1e9, 1),
+                          "frac": round(psw * vhw / tw / 1e9 / peak, 4), "launch_us": round(tw * 1e6, 1)}
 
     cpu = None
     extra = None

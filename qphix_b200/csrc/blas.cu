@@ -65,11 +65,10 @@ void launch_blas(int prec, const BlasArgs &a, dim3 grid, cudaStream_t st)
 // nres > 32): lane l of warp g of a group adds site blocks 32 g + l,
 // 32 g + l + 32 G, ... in that order, then a shuffle tree per warp and the
 // group's warps in order.  A solver state that is already done makes it
-// return at once, as the producing kernel did.
+// write nothing, as the producing kernel did.
 __global__ void __launch_bounds__(QPX_FOLD_THREADS) fold_kernel(const ReduceArg ra, SolverState *st, int nrhs,
                                                                 int nparts)
 {
-  if (st && st->done) return;
   __shared__ double gsum[QPX_FOLD_THREADS / 32];
   __shared__ double res[QPX_MAX_RHS * QPX_MAX_RED];
   __shared__ SolverState sst;
@@ -79,7 +78,10 @@ __global__ void __launch_bounds__(QPX_FOLD_THREADS) fold_kernel(const ReduceArg 
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   // the solver state is read and written by the finalize step on thread 0
   // below: a shared copy turns its chain of dependent global accesses into
-  // shared-memory ones
+  // shared-memory ones.  Its loads and the partials' loads are all issued
+  // before anything waits on them (a done solver is recognised afterwards,
+  // from the copy: its producing launch wrote no partials, and nothing is
+  // written back).
   if (st)
     for (int i = threadIdx.x; i < kStateWords; i += blockDim.x)
       reinterpret_cast<int *>(&sst)[i] = reinterpret_cast<const int *>(st)[i];
@@ -104,6 +106,7 @@ __global__ void __launch_bounds__(QPX_FOLD_THREADS) fold_kernel(const ReduceArg 
     }
     __syncthreads();
   }
+  if (st && sst.done) return;  // uniform: every thread reads the same shared flag
   if (threadIdx.x == 0) {
     // two-flavour systems: each flavour pair's reductions are one sum (the
     // reference's num_flav = 2 BLAS), so both get the same solver scalars

@@ -1,5 +1,6 @@
 // Scalar recurrences of the Krylov solvers, executed on the device by the
-// last block of the reduction that produces their inputs (see qpx_reduce.cuh).
+// fold kernel of the reduction that produces their inputs (fold_kernel in
+// blas.cu, on a shared-memory copy of the solver state).
 // Each follows the host-side scalar arithmetic of the reference solver cited
 // beside it; a right-hand side that has converged (or broken down) gets zero
 // update coefficients so that later iterations leave its x and r untouched.
