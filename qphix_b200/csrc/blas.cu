@@ -92,9 +92,9 @@ __global__ void __launch_bounds__(QPX_FOLD_THREADS) fold_kernel(const ReduceArg 
     const int v = v0 + slot;
     double acc = 0.0;
     if (slot < vpr && v < nres) {
-      const double *p = ra.partials + v;
+      const double *p = ra.partials + (long long)v * nparts;  // value-major: coalesced across the lanes
 #pragma unroll 8
-      for (int b = 32 * g + lane; b < nparts; b += 32 * G) acc += __ldcg(p + (long long)b * nres);
+      for (int b = 32 * g + lane; b < nparts; b += 32 * G) acc += __ldcg(p + b);
     }
     acc = warp_sum(acc);
     if (lane == 0) gsum[wid] = acc;

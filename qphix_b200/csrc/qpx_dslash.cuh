@@ -934,7 +934,7 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
     }
   }
   if (a.red.mask)
-    reduce_epilogue<RT>(a.red, a.nrhs, rhs0, red_slots(a.red.mask), red, sblock);
+    reduce_epilogue<RT>(a.red, a.nrhs, rhs0, red_slots(a.red.mask), red, sblock, (int)(gridDim.x / ntiles));
 }
 
 }  // namespace qpx

@@ -66,7 +66,7 @@ struct ReduceArg {
   int mask;            // which values (bit order fixed by the producing kernel)
   int nval;            // number of doubles per rhs
   int fin;             // FinOp
-  double *partials;    // [nblocks][nrhs][nval]
+  double *partials;    // [nrhs][nval][nblocks]
   double *result;      // [nrhs][nval]
 };
 
@@ -85,19 +85,25 @@ __device__ inline void finalize(int fin, SolverState *st, const double *res, int
 // producing kernel, translated by it into a slot bit set) says which slots
 // are live, and they are packed in slot order into nval doubles per rhs.
 // rhs0 = first rhs of the block's tile.  Each block writes one partial per
-// (rhs, value) under site-block index `sblock` (default: blockIdx.x;
-// kernels whose blocks cover (site block, rhs tile) pairs in one grid
-// dimension pass their own) and is done: the partials are folded, and the
-// solver's finalize step run, by fold_kernel, launched after the producing
-// kernel on the same stream.  Blocks therefore never wait on one another or
-// on a device-wide fence, and the fold runs with a full block of threads.
+// (rhs, value) under site-block index `sblock` of `nsblocks` (default:
+// blockIdx.x of gridDim.x; kernels whose blocks cover (site block, rhs tile)
+// pairs in one grid dimension pass their own), value-major so that the fold
+// reads every value's partials contiguously, and is done: the partials are
+// folded, and the solver's finalize step run, by fold_kernel, launched after
+// the producing kernel on the same stream.  Blocks therefore never wait on
+// one another or on a device-wide fence, and the fold runs with a full block
+// of threads.
 template <int R>
 __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, int nrhs, int rhs0, int slots,
-                                                const double val[R][QPX_MAX_RED], int sblock = -1)
+                                                const double val[R][QPX_MAX_RED], int sblock = -1,
+                                                int nsblocks = -1)
 {
   constexpr int NW = QPX_BLOCK / 32;  // launches of these kernels use QPX_BLOCK threads
   __shared__ double wpart[NW][R * QPX_MAX_RED];
-  if (sblock < 0) sblock = blockIdx.x;
+  if (sblock < 0) {
+    sblock = blockIdx.x;
+    nsblocks = gridDim.x;
+  }
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   // every live value's warp sum, then one barrier and a fixed-order sum over warps
 #pragma unroll
@@ -118,7 +124,7 @@ __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, int nrhs, i
         if (slots & (1 << k)) {
           double s = 0.0;
           for (int w = 0; w < NW; w++) s += wpart[w][r * QPX_MAX_RED + k];
-          if (rhs0 + r < nrhs) ra.partials[((long long)sblock * nrhs + rhs0 + r) * ra.nval + o] = s;
+          if (rhs0 + r < nrhs) ra.partials[((long long)(rhs0 + r) * ra.nval + o) * nsblocks + sblock] = s;
           o++;
         }
       }
