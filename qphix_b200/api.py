@@ -745,6 +745,14 @@ def zero(x):
     check(L._lib.qphix_gpu_blas_zero(x.h))
 
 
+def launch_count():
+    """Kernels this library has launched in the process (graph replays count
+    their kernels)."""
+    n = C.c_ulonglong(0)
+    check(L._lib.qphix_gpu_launch_count(C.byref(n)))
+    return n.value
+
+
 # ---------------------------------------------------------------------------
 # Dslash launch-shape autotuner
 # ---------------------------------------------------------------------------

@@ -60,12 +60,15 @@ void launch_blas(int prec, const BlasArgs &a, dim3 grid, cudaStream_t st)
 // Folds the block partials of one reducing launch (reduce_epilogue,
 // qpx_reduce.cuh) into ra.result and runs the solver's finalize step; one
 // block of QPX_FOLD_THREADS threads, launched right after the producing
-// kernel on its stream.  The nres = nrhs x nval values share the 32 warps,
-// a group of G = max(1, 32 / nres) warps per value (further rounds when
-// nres > 32): lane l of warp g of a group adds site blocks 32 g + l,
+// kernel on its stream, instantiated per finalize step (FIN) so that each
+// carries only its own recurrence.  The nres = nrhs x nval values share the
+// 32 warps, a group of G = max(1, 32 / nres) warps per value (further rounds
+// when nres > 32): lane l of warp g of a group adds site blocks 32 g + l,
 // 32 g + l + 32 G, ... in that order, then a shuffle tree per warp and the
-// group's warps in order.  A solver state that is already done makes it
-// write nothing, as the producing kernel did.
+// group's warps in order.  Warp 0 then runs the finalize, a lane per
+// right-hand side.  A solver state that is already done makes it write
+// nothing, as the producing kernel did.
+template <int FIN>
 __global__ void __launch_bounds__(QPX_FOLD_THREADS) fold_kernel(const ReduceArg ra, SolverState *st, int nrhs,
                                                                 int nparts)
 {
@@ -74,17 +77,24 @@ __global__ void __launch_bounds__(QPX_FOLD_THREADS) fold_kernel(const ReduceArg 
   __shared__ SolverState sst;
   constexpr int kStateWords = sizeof(SolverState) / sizeof(int);
   static_assert(sizeof(SolverState) % sizeof(int) == 0, "SolverState is copied as 32-bit words");
+  constexpr bool kFinalize = FIN != FIN_NONE && FIN != FIN_STORE;  // steps that update the state
   const int nres = nrhs * ra.nval;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  // the solver state is read and written by the finalize step on thread 0
-  // below: a shared copy turns its chain of dependent global accesses into
+  // the solver state is read and written by the finalize step below: a
+  // shared copy turns its chains of dependent global accesses into
   // shared-memory ones.  Its loads and the partials' loads are all issued
   // before anything waits on them (a done solver is recognised afterwards,
   // from the copy: its producing launch wrote no partials, and nothing is
   // written back).
-  if (st)
-    for (int i = threadIdx.x; i < kStateWords; i += blockDim.x)
-      reinterpret_cast<int *>(&sst)[i] = reinterpret_cast<const int *>(st)[i];
+  if (st) {
+    if (kFinalize)
+      for (int i = threadIdx.x; i < kStateWords; i += blockDim.x)
+        reinterpret_cast<int *>(&sst)[i] = reinterpret_cast<const int *>(st)[i];
+    else if (threadIdx.x == 0) {
+      sst.done = st->done;
+      sst.coupled = st->coupled;
+    }
+  }
   const int G = nres >= 32 ? 1 : 32 / nres;
   const int vpr = 32 / G;  // values per round
   for (int v0 = 0; v0 < nres; v0 += vpr) {
@@ -106,29 +116,53 @@ __global__ void __launch_bounds__(QPX_FOLD_THREADS) fold_kernel(const ReduceArg 
     }
     __syncthreads();
   }
+  __syncthreads();
   if (st && sst.done) return;  // uniform: every thread reads the same shared flag
-  if (threadIdx.x == 0) {
+  const bool use_state = kFinalize && st;
+  if (wid == 0 && st) {
     // two-flavour systems: each flavour pair's reductions are one sum (the
     // reference's num_flav = 2 BLAS), so both get the same solver scalars
-    if (st && sst.coupled)
-      for (int r = 0; r + 1 < nrhs; r += 2)
-        for (int k = 0; k < ra.nval; k++) {
-          const double t = res[r * ra.nval + k] + res[(r + 1) * ra.nval + k];
-          res[r * ra.nval + k] = t;
-          res[(r + 1) * ra.nval + k] = t;
-        }
-    if (ra.fin != FIN_NONE && st) finalize(ra.fin, &sst, res, nrhs, ra.nval);
+    if (sst.coupled) {
+      const int r = lane & ~1;
+      double t[QPX_MAX_RED];
+#pragma unroll
+      for (int k = 0; k < QPX_MAX_RED; k++)
+        if (k < ra.nval && r + 1 < nrhs) t[k] = res[r * ra.nval + k] + res[(r + 1) * ra.nval + k];
+      __syncwarp();
+#pragma unroll
+      for (int k = 0; k < QPX_MAX_RED; k++)
+        if (k < ra.nval && r + 1 < nrhs && lane < nrhs) res[lane * ra.nval + k] = t[k];
+      __syncwarp();
+    }
+    if (use_state) finalize_warp<FIN>(&sst, res, nrhs, ra.nval, lane);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < nres; i += blockDim.x) ra.result[i] = res[i];
-  if (st)
+  if (use_state)
     for (int i = threadIdx.x; i < kStateWords; i += blockDim.x)
       reinterpret_cast<int *>(st)[i] = reinterpret_cast<const int *>(&sst)[i];
 }
 
 void launch_fold(const ReduceArg &ra, SolverState *state, int nrhs, int nparts, cudaStream_t st)
 {
-  fold_kernel<<<1, QPX_FOLD_THREADS, 0, st>>>(ra, state, nrhs, nparts);
+#define QPX_FOLD_CASE(F) \
+  case F: fold_kernel<F><<<1, QPX_FOLD_THREADS, 0, st>>>(ra, state, nrhs, nparts); break;
+  switch (ra.fin) {
+    QPX_FOLD_CASE(FIN_NONE)
+    QPX_FOLD_CASE(FIN_CG_A)
+    QPX_FOLD_CASE(FIN_CG_R)
+    QPX_FOLD_CASE(FIN_BICG_ALPHA)
+    QPX_FOLD_CASE(FIN_BICG_OMEGA)
+    QPX_FOLD_CASE(FIN_BICG_RX)
+    QPX_FOLD_CASE(FIN_BICG_RU)
+    QPX_FOLD_CASE(FIN_MR_A)
+    QPX_FOLD_CASE(FIN_MR_R)
+    QPX_FOLD_CASE(FIN_STORE)
+    QPX_FOLD_CASE(FIN_MCG_D)
+    QPX_FOLD_CASE(FIN_MCG_R)
+  default: throw Error(QPHIX_GPU_EINVAL, "bad finalize step");
+  }
+#undef QPX_FOLD_CASE
 }
 
 template <typename P>

@@ -661,6 +661,58 @@ struct CloverIO<Q16, NR> : CloverIO16<F16, NR> {};
 template <int NR>
 struct CloverIO<Q16F32, NR> : CloverIO<F32, NR> {};
 
+// Coherent<P>: precision P with its spinor loads taken through L2
+// (ld.global.cg) instead of the read-only non-coherent path, for kernels that
+// read spinors written earlier in the same launch (the persistent solver
+// kernels, across their grid barriers).  Links and clover terms stay
+// read-only for a whole solve and keep P's loads.
+template <typename P>
+struct Coherent : P {};
+template <typename P, int RECON>
+struct GaugeIO<Coherent<P>, RECON> : GaugeIO<P, RECON> {};
+template <typename P, int NR>
+struct CloverIO<Coherent<P>, NR> : CloverIO<P, NR> {};
+
+template <>
+struct SpinorIO<Coherent<F64>> : SpinorIO<F64> {
+  __device__ __forceinline__ static void load_raw(const SpinorArg &f, int rhs, long long s, double v[24], double &nrm)
+  {
+    load(f, rhs, s, v);
+    nrm = 1.0;
+  }
+  __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, long long s, double v[24])
+  {
+    const double2 *p = reinterpret_cast<const double2 *>(f.data) + rhs * f.rhs_stride_chunks + s;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      double2 d = __ldcg(p + k * f.stride);
+      v[2 * k] = d.x;
+      v[2 * k + 1] = d.y;
+    }
+  }
+};
+
+template <>
+struct SpinorIO<Coherent<F32>> : SpinorIO<F32> {
+  __device__ __forceinline__ static void load_raw(const SpinorArg &f, int rhs, long long s, float v[24], float &nrm)
+  {
+    load(f, rhs, s, v);
+    nrm = 1.0f;
+  }
+  __device__ __forceinline__ static void load(const SpinorArg &f, int rhs, long long s, float v[24])
+  {
+    const float4 *p = reinterpret_cast<const float4 *>(f.data) + rhs * f.rhs_stride_chunks + s;
+#pragma unroll
+    for (int k = 0; k < 6; k++) {
+      float4 d = __ldcg(p + k * f.stride);
+      v[4 * k] = d.x;
+      v[4 * k + 1] = d.y;
+      v[4 * k + 2] = d.z;
+      v[4 * k + 3] = d.w;
+    }
+  }
+};
+
 // ---------------------------------------------------------------------------
 // lattice geometry as seen by a kernel
 // ---------------------------------------------------------------------------

@@ -516,18 +516,23 @@ __device__ __forceinline__ void lanes_set(f2 &d, const double *v) { d = make_flo
 // Blocks cover (site block, rhs tile) pairs with the rhs tile varying
 // fastest, so the blocks that share a site block (and its links) run
 // together and the links of the later right-hand sides come from L2.
+//
+// dslash_block is the work of one block: block `vblock` of a launch of
+// `nvblocks` blocks, with POST_CG / POST_RAXPY coefficients read from `st`.
+// dslash_kernel runs it once per CUDA block; the persistent solver kernels
+// (qpx_persist.cuh) run it over all virtual blocks of a phase from a grid
+// that stays resident.
 template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN, int SP, bool GEN, bool RL = false>
-__global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
+__device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverState *st, int vblock, int nvblocks)
 {
   using L = typename std::conditional<RL, RhsLanes<P>, Lanes<P, SP>>::type;
   using T = typename L::T;
   static_assert(SP == 1 || R == 1, "two sites per thread take one right-hand side");
   static_assert(!RL || (SP == 2 && R == 1 && !GEN), "right-hand-side lanes: SP = 2, R = 1, fast path");
   constexpr int RT = RL ? 2 : R;  // right-hand sides per thread
-  if (a.state && a.state->done) return;
   const int ntiles = a.nrhs / RT;
-  const int tile = blockIdx.x % ntiles;
-  const int sblock = blockIdx.x / ntiles;
+  const int tile = vblock % ntiles;
+  const int sblock = vblock / ntiles;
   const int rhs0 = tile * RT;
   int s[SP];
   bool act[SP];
@@ -903,7 +908,7 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
       if (a.post == POST_STORE) {
         L::store(a.out, rr, s, act, res[r]);
       } else if (a.post == POST_RAXPY) {  // r += b mmp ; |r|^2
-        const T cb_ = rhs_coef<RL, T>(a.state->v[S_B], rr);
+        const T cb_ = rhs_coef<RL, T>(st->v[S_B], rr);
         T rv[24];
         L::load(a.r, rr, s, rv);
 #pragma unroll
@@ -914,7 +919,7 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
         else
           red[r][5] = red_norm(rv, act);
       } else {  // POST_CG: r -= a mmp ; x += a p ; |r|^2
-        const T ca = rhs_coef<RL, T>(a.state->v[S_A], rr), nca = -ca;
+        const T ca = rhs_coef<RL, T>(st->v[S_A], rr), nca = -ca;
         T rv[24], xv[24], pv[24];
         L::load(a.r, rr, s, rv);
         L::load(a.x, rr, s, xv);
@@ -934,7 +939,14 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const DslashArgs a)
     }
   }
   if (a.red.mask)
-    reduce_epilogue<RT>(a.red, a.nrhs, rhs0, red_slots(a.red.mask), red, sblock, (int)(gridDim.x / ntiles));
+    reduce_epilogue<RT>(a.red, a.nrhs, rhs0, red_slots(a.red.mask), red, sblock, nvblocks / ntiles);
+}
+
+template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN, int SP, bool GEN, bool RL = false>
+__global__ void QPX_DSLASH_BOUNDS dslash_kernel(const __grid_constant__ DslashArgs a)
+{
+  if (a.state && a.state->done) return;
+  dslash_block<P, RECON, EPI, ACHI, R, ISIGN, SP, GEN, RL>(a, a.state, blockIdx.x, gridDim.x);
 }
 
 }  // namespace qpx

@@ -68,6 +68,7 @@ struct qphix_gpu_lattice_s {
   double *h_result = nullptr;     // pinned mirror
   qpx::SolverState *state = nullptr;   // device
   qpx::SolverState *h_state = nullptr; // pinned mirror
+  void *grid_bar = nullptr;             // device GridBarrier of the persistent solvers (lazy)
   void *staging = nullptr;
   size_t staging_bytes = 0;
   // solver temporaries, reused across solves (they hold no lattice reference)
@@ -189,6 +190,10 @@ void launch_two_flav_clover(int prec, int vh, int npairs, SpinorArg out, SpinorA
                             CloverArg c, cudaStream_t st);
 void launch_clover_convert(int prec_in, int prec_out, Geom geo, const void *in, int vpc_in, void *out, int vpc_out,
                            long long stride, int nr, dim3 grid, cudaStream_t st);
+// persistent CG kernel (qpx_persist.cuh) for (recon, Wilson or clover) with
+// FP64 / FP32 storage and isign = +1; nullptr where none is built
+const void *cg_persistent_kernel_f64(int recon, bool clover);
+const void *cg_persistent_kernel_f32(int recon, bool clover);
 
 
 }  // namespace qpx

@@ -77,8 +77,6 @@ __device__ __forceinline__ double warp_sum(double v)
   return v;
 }
 
-__device__ inline void finalize(int fin, SolverState *st, const double *res, int nrhs, int nval);
-
 // Called by every thread of every block after the block's per-thread values
 // are final.  Values live in fixed slots val[r][k] (k < QPX_MAX_RED, compile-
 // time indices so they stay in registers); `slots` (ReduceArg::mask of the

@@ -62,6 +62,7 @@ def c1(args):
     api.zero(x)
     info = cg(x, b, 1e-10)[0]
     ts = []
+    n0 = api.launch_count()
     for _ in range(args.reps):
         api.zero(x)
         e0, e1 = _events(torch, stream)
@@ -69,11 +70,14 @@ def c1(args):
         e1.record(stream)
         torch.cuda.synchronize()
         ts.append(e0.elapsed_time(e1))
+    launches = (api.launch_count() - n0) / max(1, args.reps)
     ms = float(np.median(ts))
     return {"config": "c1", "workload": "8^4 Wilson EO, Gaussian reunitarised links 18-real, kappa 0.12, "
                                          "CG on M^+M to 1e-10, FP64",
             "solves_per_s": 1e3 / ms, "ms_per_solve": ms, "iters": info["n_iters"], "mv_apps": info["mv_apps"],
-            "true_rel_resid": info["true_rel_resid"], "status": info["status"]}
+            "true_rel_resid": info["true_rel_resid"], "status": info["status"],
+            # a persistent-kernel solve (small lattices, qpx_persist.cuh) is a handful of launches
+            "gpu_launches_per_solve": launches}
 
 
 def c3(args):
