@@ -52,9 +52,14 @@ ChunkSpec clover_spec(int prec, int nreal)
   default: throw Error(QPHIX_GPU_EINVAL, "bad precision");         \
   }
 
+static void check_pdl_launch(cudaError_t e)
+{
+  if (e != cudaSuccess) throw Error(QPHIX_GPU_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
 void launch_blas(int prec, const BlasArgs &a, dim3 grid, cudaStream_t st)
 {
-  QPX_PREC_SWITCH(prec, (blas_kernel<P><<<grid, QPX_BLOCK, 0, st>>>(a)));
+  QPX_PREC_SWITCH(prec, (check_pdl_launch(launch_pdl(blas_kernel<P>, grid, dim3(QPX_BLOCK), st, (long long)grid.x * grid.y, a))));
 }
 
 // Folds the block partials of one reducing launch (reduce_epilogue,
@@ -80,6 +85,8 @@ __global__ void __launch_bounds__(QPX_FOLD_THREADS) fold_kernel(const ReduceArg 
   constexpr bool kFinalize = FIN != FIN_NONE && FIN != FIN_STORE;  // steps that update the state
   const int nres = nrhs * ra.nval;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  pdl_trigger();
+  pdl_wait();
   // the solver state is read and written by the finalize step below: a
   // shared copy turns its chains of dependent global accesses into
   // shared-memory ones.  Its loads and the partials' loads are all issued
@@ -146,7 +153,7 @@ __global__ void __launch_bounds__(QPX_FOLD_THREADS) fold_kernel(const ReduceArg 
 void launch_fold(const ReduceArg &ra, SolverState *state, int nrhs, int nparts, cudaStream_t st)
 {
 #define QPX_FOLD_CASE(F) \
-  case F: fold_kernel<F><<<1, QPX_FOLD_THREADS, 0, st>>>(ra, state, nrhs, nparts); break;
+  case F: check_pdl_launch(launch_pdl(fold_kernel<F>, dim3(1), dim3(QPX_FOLD_THREADS), st, (long long)nparts * nrhs, ra, state, nrhs, nparts)); break;
   switch (ra.fin) {
     QPX_FOLD_CASE(FIN_NONE)
     QPX_FOLD_CASE(FIN_CG_A)

@@ -9,22 +9,27 @@
 
 namespace qpx {
 
+inline void check_pdl(cudaError_t e)
+{
+  if (e != cudaSuccess) throw Error(QPHIX_GPU_ECUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+}
+
 template <typename P, int RECON, int R, int S, int SP, bool GEN, bool RL = false>
 void launch_dslash_k(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStream_t st)
 {
   dim3 block(QPX_BLOCK);
   if (achi == ACHI_NONE) {
     switch (epi) {
-    case EPI_NONE: dslash_kernel<P, RECON, EPI_NONE, ACHI_NONE, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
-    case EPI_CLOV: dslash_kernel<P, RECON, EPI_CLOV, ACHI_NONE, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
-    case EPI_TMINV: dslash_kernel<P, RECON, EPI_TMINV, ACHI_NONE, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
-    case EPI_FCLOV: dslash_kernel<P, RECON, EPI_FCLOV, ACHI_NONE, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
+    case EPI_NONE: check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_NONE, ACHI_NONE, R, S, SP, GEN, RL>, grid, block, st, (long long)grid.x * grid.y, a)); return;
+    case EPI_CLOV: check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_CLOV, ACHI_NONE, R, S, SP, GEN, RL>, grid, block, st, (long long)grid.x * grid.y, a)); return;
+    case EPI_TMINV: check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_TMINV, ACHI_NONE, R, S, SP, GEN, RL>, grid, block, st, (long long)grid.x * grid.y, a)); return;
+    case EPI_FCLOV: check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_FCLOV, ACHI_NONE, R, S, SP, GEN, RL>, grid, block, st, (long long)grid.x * grid.y, a)); return;
     }
   } else if (epi == EPI_NONE) {
     switch (achi) {
-    case ACHI_ALPHA: dslash_kernel<P, RECON, EPI_NONE, ACHI_ALPHA, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
-    case ACHI_CLOV: dslash_kernel<P, RECON, EPI_NONE, ACHI_CLOV, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
-    case ACHI_TM: dslash_kernel<P, RECON, EPI_NONE, ACHI_TM, R, S, SP, GEN, RL><<<grid, block, 0, st>>>(a); return;
+    case ACHI_ALPHA: check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_NONE, ACHI_ALPHA, R, S, SP, GEN, RL>, grid, block, st, (long long)grid.x * grid.y, a)); return;
+    case ACHI_CLOV: check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_NONE, ACHI_CLOV, R, S, SP, GEN, RL>, grid, block, st, (long long)grid.x * grid.y, a)); return;
+    case ACHI_TM: check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_NONE, ACHI_TM, R, S, SP, GEN, RL>, grid, block, st, (long long)grid.x * grid.y, a)); return;
     }
   }
   throw Error(QPHIX_GPU_EINVAL, "unsupported dslash epilogue combination");
@@ -36,13 +41,13 @@ void launch_dslash_nd(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStr
 {
   dim3 block(QPX_BLOCK);
   if (achi == ACHI_NONE && epi == EPI_NDTM)
-    dslash_kernel<P, RECON, EPI_NDTM, ACHI_NONE, 2, S, 1, false><<<grid, block, 0, st>>>(a);
+    check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_NDTM, ACHI_NONE, 2, S, 1, false>, grid, block, st, (long long)grid.x * grid.y, a));
   else if (epi == EPI_NONE && achi == ACHI_NDTM)
-    dslash_kernel<P, RECON, EPI_NONE, ACHI_NDTM, 2, S, 1, false><<<grid, block, 0, st>>>(a);
+    check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_NONE, ACHI_NDTM, 2, S, 1, false>, grid, block, st, (long long)grid.x * grid.y, a));
   else if (achi == ACHI_NONE && epi == EPI_NDFCLOV)
-    dslash_kernel<P, RECON, EPI_NDFCLOV, ACHI_NONE, 2, S, 1, false><<<grid, block, 0, st>>>(a);
+    check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_NDFCLOV, ACHI_NONE, 2, S, 1, false>, grid, block, st, (long long)grid.x * grid.y, a));
   else if (epi == EPI_NONE && achi == ACHI_NDCLOV)
-    dslash_kernel<P, RECON, EPI_NONE, ACHI_NDCLOV, 2, S, 1, false><<<grid, block, 0, st>>>(a);
+    check_pdl(launch_pdl(dslash_kernel<P, RECON, EPI_NONE, ACHI_NDCLOV, 2, S, 1, false>, grid, block, st, (long long)grid.x * grid.y, a));
   else
     throw Error(QPHIX_GPU_EINVAL, "unsupported two-flavour dslash combination");
 }

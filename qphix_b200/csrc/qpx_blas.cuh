@@ -106,6 +106,8 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
 {
   using T = typename P::real;
   using IO = SpinorIO<P>;
+  pdl_wait();
+  pdl_trigger();
   if (a.state && a.state->done) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int rhs = blockIdx.y;

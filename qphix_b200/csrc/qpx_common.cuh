@@ -18,9 +18,56 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cstdlib>
 #include <type_traits>
 
 namespace qpx {
+
+// ---------------------------------------------------------------------------
+// Programmatic dependent launch (sm_90 and later).  The Dslash, BLAS and fold
+// kernels of a solver iteration are launched with the programmatic stream
+// serialisation attribute (launch_pdl): each may be scheduled while its
+// predecessor on the stream is still finishing its last blocks, instead of
+// after it has drained.  pdl_wait() blocks until the predecessor grid has
+// completed and its writes are visible, and comes before the kernel reads
+// anything its predecessors wrote; pdl_trigger() lets the successor start
+// launching.  For a kernel launched without the attribute both are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// The attribute pays off where a launch's predecessor ends in a partial last
+// wave of many blocks (measured on B200: the 16^3x32, 8-rhs solve runs 2 %
+// faster with it); behind small launches (an 8^4 lattice's 16-block grids)
+// the dependent wait costs more than the ordinary launch boundary (8^4 CG
+// 10 % slower), so launches of fewer than kPdlMinBlocks blocks, and folds of
+// fewer partials, go the ordinary way.  QPHIX_GPU_PDL=0 turns it off.
+constexpr int kPdlMinBlocks = 296;
+inline bool pdl_enabled()
+{
+  static const bool on = [] {
+    const char *e = std::getenv("QPHIX_GPU_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+// `size`: the block count that decides whether the attribute is set
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, long long size,
+                       Args &&...args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = (pdl_enabled() && size >= kPdlMinBlocks) ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 enum Prec : int { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2, PREC_BF16 = 3, PREC_Q16 = 4, PREC_Q16F32 = 5 };
 

@@ -945,6 +945,8 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
 template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN, int SP, bool GEN, bool RL = false>
 __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const __grid_constant__ DslashArgs a)
 {
+  pdl_wait();
+  pdl_trigger();
   if (a.state && a.state->done) return;
   dslash_block<P, RECON, EPI, ACHI, R, ISIGN, SP, GEN, RL>(a, a.state, blockIdx.x, gridDim.x);
 }
