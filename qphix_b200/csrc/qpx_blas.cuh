@@ -109,25 +109,30 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
   pdl_wait();
   pdl_trigger();
   if (a.state && a.state->done) return;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
   const int rhs = blockIdx.y;
   double red[1][QPX_MAX_RED];
 #pragma unroll
   for (int k = 0; k < QPX_MAX_RED; k++) red[0][k] = 0;
-  if (s < a.vh) {
+  // grid-stride over the sites: a launch with fewer blocks than Vh / 128
+  // gives each thread several sites (and the fold fewer block partials); a
+  // thread's per-site values are added in site order
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.vh; s += gridDim.x * blockDim.x) {
+    double sr[1][QPX_MAX_RED];
+#pragma unroll
+    for (int k = 0; k < QPX_MAX_RED; k++) sr[0][k] = 0;
     T x[24], y[24];
     switch (a.op) {
     case B_NORM2: {
       IO::load(a.x, rhs, s, x);
-      red[0][0] = blas_norm<false>(x);
+      sr[0][0] = blas_norm<false>(x);
       break;
     }
     case B_DOT:
     case B_DOTNORM: {
       IO::load(a.x, rhs, s, x);
       IO::load(a.y, rhs, s, y);
-      blas_dot(x, y, red[0][0], red[0][1]);
-      if (a.op == B_DOTNORM) red[0][2] = blas_norm<true>(x);
+      blas_dot(x, y, sr[0][0], sr[0][1]);
+      if (a.op == B_DOTNORM) sr[0][2] = blas_norm<true>(x);
       break;
     }
     case B_COPY:
@@ -152,7 +157,7 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
         y[k + 1] = yi;
       }
       IO::store(a.y, rhs, s, y);
-      if (a.op == B_CAXPBY_NORM) red[0][0] = blas_norm<true>(y);
+      if (a.op == B_CAXPBY_NORM) sr[0][0] = blas_norm<true>(y);
       break;
     }
     case B_XMY_NORM: {
@@ -161,7 +166,7 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
 #pragma unroll
       for (int k = 0; k < 24; k++) x[k] -= y[k];
       IO::store(a.z, rhs, s, x);
-      red[0][0] = blas_norm<false>(x);
+      sr[0][0] = blas_norm<false>(x);
       break;
     }
     case B_BICG_P: {  // x = r, y = p, z = v ; a = beta, b = omega
@@ -201,8 +206,8 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
       IO::store(a.y, rhs, s, y);
       T w[24];
       IO::load(a.w, rhs, s, w);
-      red[0][0] = blas_norm<true>(y);
-      blas_dot(w, y, red[0][1], red[0][2]);
+      sr[0][0] = blas_norm<true>(y);
+      blas_dot(w, y, sr[0][1], sr[0][2]);
       break;
     }
     case B_CG_P: {  // x = r, y = p ; a = b
@@ -224,7 +229,7 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
       caxpy_(y, -ar, -ai, mr);
       IO::store(a.x, rhs, s, x);
       IO::store(a.y, rhs, s, y);
-      red[0][0] = blas_norm<false>(y);
+      sr[0][0] = blas_norm<false>(y);
       break;
     }
     case B_RICH_RX: {  // x = x, y = r, z = dx, w = t
@@ -240,7 +245,7 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
       }
       IO::store(a.x, rhs, s, x);
       IO::store(a.y, rhs, s, y);
-      red[0][0] = blas_norm<false>(y);
+      sr[0][0] = blas_norm<false>(y);
       break;
     }
     case B_G5: {
@@ -253,6 +258,8 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
     default:
       break;
     }
+#pragma unroll
+    for (int k = 0; k < QPX_MAX_RED; k++) red[0][k] += sr[0][k];
   }
   if (a.red.mask) reduce_epilogue<1>(a.red, a.nrhs, rhs, a.red.mask, red);
 }
