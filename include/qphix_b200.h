@@ -254,6 +254,45 @@ int qphix_gpu_dslash_achimbdpsi_halo(const qphix_gpu_op_params *p, qphix_gpu_fie
                                      double beta, int isign, int cb, double musign,
                                      const qphix_gpu_halo_faces *faces);
 
+/* ---- halo mode for a lattice cut along any of x, y, z, t ---------------------
+ * (the 4D decomposition of include/qphix/comm.h:372-437 and geometry's
+ * per-direction comms flags).  Each rank's lattice is one block of a
+ * Cartesian grid of blocks; every local extent is even (so local and global
+ * checkerboards agree).  For each cut direction mu the Dslash needs the
+ * source field's first slice along mu from the next block, its last slice
+ * from the previous block, and, once per gauge field, U_mu on the previous
+ * block's last slice; hops along uncut directions wrap inside the block.
+ * A face lists the sites of one checkerboard of a slice, ordered
+ * x: ((t Nz + z) Ny + y) / 2, y: (t Nz + z) Nx/2 + x/2,
+ * z: (t Ny + y) Nx/2 + x/2, t: (z Ny + y) Nx/2 + x/2 (local coordinates).
+ * qphix_gpu_halo_pack_spinor_dir packs the field's slice (side 0 first, 1
+ * last) of checkerboard cb (the checkerboard the field lives on, the
+ * opposite of the Dslash's target); qphix_gpu_halo_pack_links_dir packs U_mu
+ * on the last slice, both checkerboards.  Packs are asynchronous on the
+ * field's lattice stream; dst must hold the *_bytes_dir sizes.  A t cut
+ * applies t_boundary on the blocks that hold the global t edges; without one
+ * the block holds both edges. */
+typedef struct {
+  int cut;                  /* bit mu (0 x, 1 y, 2 z, 3 t): the lattice is cut along mu     */
+  const void *psi_fwd[4];   /* cut mu: the next block's side-0 pack of the hopped field      */
+  const void *psi_bwd[4];   /* cut mu: the previous block's side-1 pack of it                */
+  const void *links_bwd[4]; /* cut mu: the previous block's qphix_gpu_halo_pack_links_dir    */
+  int global_first_t;       /* t cut: this block holds global t = 0                          */
+  int global_last_t;        /* t cut: this block holds global t = Nt - 1                     */
+} qphix_gpu_halo_faces4;
+int qphix_gpu_halo_face_sites(qphix_gpu_lattice lat, int mu, size_t *sites);
+int qphix_gpu_halo_spinor_bytes_dir(qphix_gpu_field psi, int mu, size_t *bytes);
+int qphix_gpu_halo_pack_spinor_dir(qphix_gpu_field psi, int mu, int side, int cb, void *dst);
+int qphix_gpu_halo_link_bytes_dir(qphix_gpu_field gauge, int mu, size_t *bytes);
+int qphix_gpu_halo_pack_links_dir(qphix_gpu_field gauge, int mu, void *dst);
+int qphix_gpu_dslash_halo4(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                           qphix_gpu_field gauge, qphix_gpu_field aux, qphix_gpu_field aux2, int isign, int cb,
+                           const qphix_gpu_halo_faces4 *faces);
+int qphix_gpu_dslash_achimbdpsi_halo4(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                                      qphix_gpu_field chi, qphix_gpu_field gauge, qphix_gpu_field aux,
+                                      double alpha, double beta, int isign, int cb, double musign,
+                                      const qphix_gpu_halo_faces4 *faces);
+
 /* ---- clover term on the device ----------------------------------------------
  * QPhiX takes the clover term and its inverse from its caller (Chroma's
  * QDPCloverTerm); these build them on the GPU from a resident FP64 gauge field:

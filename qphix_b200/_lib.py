@@ -36,6 +36,13 @@ class HaloFaces(C.Structure):
                 ("global_first", C.c_int), ("global_last", C.c_int)]
 
 
+class HaloFaces4(C.Structure):
+    """qphix_gpu_halo_faces4: ghost faces of a block of a lattice cut along
+    any of x, y, z, t (bit mu of `cut`)"""
+    _fields_ = [("cut", C.c_int), ("psi_fwd", C.c_void_p * 4), ("psi_bwd", C.c_void_p * 4),
+                ("links_bwd", C.c_void_p * 4), ("global_first_t", C.c_int), ("global_last_t", C.c_int)]
+
+
 class SolveInfo(C.Structure):
     _fields_ = [("n_iters", C.c_int), ("rsd_sq_final", C.c_double), ("site_flops", C.c_ulong),
                 ("mv_apps", C.c_ulong), ("status", C.c_int), ("true_rel_resid", C.c_double),
@@ -102,6 +109,14 @@ _SIGS = {
     "qphix_gpu_dslash_halo": ([C.POINTER(OpParams), P, P, P, P, P, I_, I_, C.POINTER(HaloFaces)], I_),
     "qphix_gpu_dslash_achimbdpsi_halo": ([C.POINTER(OpParams), P, P, P, P, P, D, D, I_, I_, D,
                                           C.POINTER(HaloFaces)], I_),
+    "qphix_gpu_halo_face_sites": ([P, I_, C.POINTER(C.c_size_t)], I_),
+    "qphix_gpu_halo_spinor_bytes_dir": ([P, I_, C.POINTER(C.c_size_t)], I_),
+    "qphix_gpu_halo_pack_spinor_dir": ([P, I_, I_, I_, P], I_),
+    "qphix_gpu_halo_link_bytes_dir": ([P, I_, C.POINTER(C.c_size_t)], I_),
+    "qphix_gpu_halo_pack_links_dir": ([P, I_, P], I_),
+    "qphix_gpu_dslash_halo4": ([C.POINTER(OpParams), P, P, P, P, P, I_, I_, C.POINTER(HaloFaces4)], I_),
+    "qphix_gpu_dslash_achimbdpsi_halo4": ([C.POINTER(OpParams), P, P, P, P, P, D, D, I_, I_, D,
+                                           C.POINTER(HaloFaces4)], I_),
     "qphix_gpu_dslash_two_flav_clover": ([C.POINTER(OpParams), P, P, P, P, P, P, I_, I_], I_),
     "qphix_gpu_clover_apply": ([P, P, P], I_),
     "qphix_gpu_clover_build": ([P, P, I_, D, D, D], I_),

@@ -848,50 +848,181 @@ static void tm_derived(const qphix_gpu_op_params &p, double &dmu, double &dmu_in
 }
 
 // res = EPI(D psi) on checkerboard cb
-// ---- halo mode (t slabs) ----------------------------------------------------
+// ---- halo mode ---------------------------------------------------------------
+// t slabs (qphix_gpu_halo_faces) are the cut {t} of the general mode.
+struct HaloSpec {
+  int cut = 0;
+  const void *psi_fwd[4] = {}, *psi_bwd[4] = {}, *links_bwd[4] = {};
+  int global_first_t = 0, global_last_t = 0;
+};
+
 static size_t face_sites(const qphix_gpu_lattice_s *lat) { return (size_t)lat->nxh * lat->dims[1] * lat->dims[2]; }
 
-static size_t halo_spinor_bytes(const qphix_gpu_field_s *f)
+// sites of one checkerboard of a slice along mu
+static size_t face_sites_dir(const qphix_gpu_lattice_s *lat, int mu)
 {
-  const size_t face = face_sites(f->lat);
+  const size_t nxh = lat->nxh, ny = lat->dims[1], nz = lat->dims[2], nt = lat->dims[3];
+  switch (mu) {
+  case 0: return ny * nz * nt / 2;
+  case 1: return nxh * nz * nt;
+  case 2: return nxh * ny * nt;
+  default: return nxh * ny * nz;
+  }
+}
+
+static size_t halo_spinor_bytes(const qphix_gpu_field_s *f, int mu = 3)
+{
+  const size_t face = face_sites_dir(f->lat, mu);
   return (size_t)f->nrhs * face * ((size_t)f->spec.nchunk * f->spec.chunk_bytes + (f->norm ? sizeof(float) : 0));
 }
 
-static size_t halo_link_bytes(const qphix_gpu_field_s *g)
+static size_t halo_link_bytes(const qphix_gpu_field_s *g, int mu = 3)
 {
-  return 2 * face_sites(g->lat) * (size_t)g->spec.nchunk * g->spec.chunk_bytes;
+  return 2 * face_sites_dir(g->lat, mu) * (size_t)g->spec.nchunk * g->spec.chunk_bytes;
+}
+
+// a cut along mu needs an even local extent along mu (block offsets even, so
+// local and global checkerboards agree) and, for x, an even Ny (x faces take
+// every other y)
+static void require_face_extents(const qphix_gpu_lattice_s *lat, int mu)
+{
+  QPX_REQUIRE(lat->dims[mu] % 2 == 0, "halo mode needs an even local extent along every cut direction");
+  QPX_REQUIRE(mu != 0 || lat->dims[1] % 2 == 0, "a cut along x needs an even local Ny");
 }
 
 // the ghost-face arguments of a halo-mode launch hopping field psi with links gauge
 static void set_halo(DslashArgs &a, const qphix_gpu_op_params &p, const qphix_gpu_field_s *psi,
-                     const qphix_gpu_field_s *gauge, int cb, const qphix_gpu_halo_faces *faces)
+                     const qphix_gpu_field_s *gauge, int cb, const HaloSpec &h)
 {
-  QPX_REQUIRE(faces->psi_fwd && faces->psi_bwd && faces->links_bwd, "halo faces: null buffer");
+  QPX_REQUIRE(h.cut > 0 && h.cut < 16, "halo: the cut mask takes bits 0-3 (x, y, z, t)");
   QPX_REQUIRE(a.tbc_mask == 0, "halo mode takes no twisted boundary phases");
   const auto *lat = psi->lat;
-  const long long face = (long long)face_sites(lat);
-  QPX_REQUIRE(face % 4 == 0, "halo mode needs (Nx/2) Ny Nz divisible by 4");
-  auto ghost = [&](const void *buf) {
-    SpinorArg g;
-    g.data = const_cast<void *>(buf);
-    g.stride = face;
-    g.rhs_stride_chunks = (long long)psi->spec.nchunk * face;
-    g.norm = psi->norm ? reinterpret_cast<float *>(static_cast<char *>(g.data) +
-                                                   (size_t)psi->nrhs * face * psi->spec.nchunk *
-                                                       psi->spec.chunk_bytes)
-                       : nullptr;
-    return g;
-  };
-  a.halo = 1;
-  a.ghost_fwd = ghost(faces->psi_fwd);
-  a.ghost_bwd = ghost(faces->psi_bwd);
-  // the backward hop onto checkerboard cb reads U_t of the other checkerboard
-  a.ghost_link.data = static_cast<const char *>(faces->links_bwd) +
-                      (size_t)(1 - cb) * face * gauge->spec.nchunk * gauge->spec.chunk_bytes;
-  a.ghost_link.stride = face;
-  a.ghost_link.mu_stride = (long long)gauge->spec.nchunk * face;
-  a.coeff_t_edge = p.aniso_t * (faces->global_last ? p.t_boundary : 1.0);
-  a.coeff_t_bwd_edge = p.aniso_t * (faces->global_first ? p.t_boundary : 1.0);
+  for (int mu = 0; mu < 4; mu++) {
+    if (!((h.cut >> mu) & 1)) continue;
+    require_face_extents(lat, mu);
+    QPX_REQUIRE(h.psi_fwd[mu] && h.psi_bwd[mu] && h.links_bwd[mu], "halo faces: null buffer");
+    const long long face = (long long)face_sites_dir(lat, mu);
+    QPX_REQUIRE(face % 4 == 0, "halo mode needs every face size divisible by 4");
+    auto ghost = [&](const void *buf) {
+      SpinorArg g;
+      g.data = const_cast<void *>(buf);
+      g.stride = face;
+      g.rhs_stride_chunks = (long long)psi->spec.nchunk * face;
+      g.norm = psi->norm ? reinterpret_cast<float *>(static_cast<char *>(g.data) +
+                                                     (size_t)psi->nrhs * face * psi->spec.nchunk *
+                                                         psi->spec.chunk_bytes)
+                         : nullptr;
+      return g;
+    };
+    a.ghost_fwd[mu] = ghost(h.psi_fwd[mu]);
+    a.ghost_bwd[mu] = ghost(h.psi_bwd[mu]);
+    // the backward hop onto checkerboard cb reads U_mu of the other checkerboard
+    a.ghost_link[mu].data = static_cast<const char *>(h.links_bwd[mu]) +
+                            (size_t)(1 - cb) * face * gauge->spec.nchunk * gauge->spec.chunk_bytes;
+    a.ghost_link[mu].stride = face;
+    a.ghost_link[mu].mu_stride = (long long)gauge->spec.nchunk * face;
+  }
+  a.halo = h.cut;
+  // without a t cut the block holds both global t edges
+  const bool tcut = (h.cut >> 3) & 1;
+  a.coeff_t_edge = p.aniso_t * ((!tcut || h.global_last_t) ? p.t_boundary : 1.0);
+  a.coeff_t_bwd_edge = p.aniso_t * ((!tcut || h.global_first_t) ? p.t_boundary : 1.0);
+}
+
+static HaloSpec halo_of(const qphix_gpu_halo_faces &f)
+{
+  HaloSpec h;
+  h.cut = 8;
+  h.psi_fwd[3] = f.psi_fwd;
+  h.psi_bwd[3] = f.psi_bwd;
+  h.links_bwd[3] = f.links_bwd;
+  h.global_first_t = f.global_first;
+  h.global_last_t = f.global_last;
+  return h;
+}
+
+static HaloSpec halo_of(const qphix_gpu_halo_faces4 &f)
+{
+  HaloSpec h;
+  h.cut = f.cut;
+  for (int mu = 0; mu < 4; mu++) {
+    h.psi_fwd[mu] = f.psi_fwd[mu];
+    h.psi_bwd[mu] = f.psi_bwd[mu];
+    h.links_bwd[mu] = f.links_bwd[mu];
+  }
+  h.global_first_t = f.global_first_t;
+  h.global_last_t = f.global_last_t;
+  return h;
+}
+
+extern "C" int qphix_gpu_halo_face_sites(qphix_gpu_lattice lat, int mu, size_t *sites)
+{
+  return guard([&] {
+    QPX_REQUIRE(lat && sites, "null argument");
+    QPX_REQUIRE(mu >= 0 && mu < 4, "mu must be in [0, 4)");
+    *sites = face_sites_dir(lat, mu);
+  });
+}
+
+extern "C" int qphix_gpu_halo_spinor_bytes_dir(qphix_gpu_field psi, int mu, size_t *bytes)
+{
+  return guard([&] {
+    QPX_REQUIRE(psi && bytes, "null argument");
+    require_spinor(psi, "psi");
+    QPX_REQUIRE(mu >= 0 && mu < 4, "mu must be in [0, 4)");
+    *bytes = halo_spinor_bytes(psi, mu);
+  });
+}
+
+extern "C" int qphix_gpu_halo_link_bytes_dir(qphix_gpu_field gauge, int mu, size_t *bytes)
+{
+  return guard([&] {
+    QPX_REQUIRE(gauge && bytes && gauge->kind == QPHIX_GPU_GAUGE, "gauge must be a gauge field");
+    QPX_REQUIRE(mu >= 0 && mu < 4, "mu must be in [0, 4)");
+    *bytes = halo_link_bytes(gauge, mu);
+  });
+}
+
+// [rhs][chunk][face] rows, then [rhs][face] norms
+extern "C" int qphix_gpu_halo_pack_spinor_dir(qphix_gpu_field psi, int mu, int side, int cb, void *dst)
+{
+  return guard([&] {
+    QPX_REQUIRE(psi && dst, "null argument");
+    require_spinor(psi, "psi");
+    QPX_REQUIRE(mu >= 0 && mu < 4, "mu must be in [0, 4)");
+    QPX_REQUIRE(side == 0 || side == 1, "side must be 0 (first slice) or 1 (last slice)");
+    QPX_REQUIRE(cb == 0 || cb == 1, "cb must be 0 or 1");
+    auto *lat = psi->lat;
+    require_face_extents(lat, mu);
+    const long long face = (long long)face_sites_dir(lat, mu);
+    const int rows = psi->nrhs * psi->spec.nchunk;
+    float *ndst = psi->norm ? reinterpret_cast<float *>(static_cast<char *>(dst) +
+                                                        (size_t)rows * face * psi->spec.chunk_bytes)
+                            : nullptr;
+    launch_face_pack(lat->geom(), mu, side ? lat->dims[mu] - 1 : 0, cb, psi->data, lat->stride, rows,
+                     psi->spec.chunk_bytes, face, dst, psi->norm, ndst, psi->nrhs, lat->stream);
+    check_launch();
+  });
+}
+
+// U_mu on the last slice along mu, checkerboard 0 then 1, [chunk][face] rows each
+extern "C" int qphix_gpu_halo_pack_links_dir(qphix_gpu_field gauge, int mu, void *dst)
+{
+  return guard([&] {
+    QPX_REQUIRE(gauge && dst && gauge->kind == QPHIX_GPU_GAUGE, "gauge must be a gauge field");
+    QPX_REQUIRE(mu >= 0 && mu < 4, "mu must be in [0, 4)");
+    auto *lat = gauge->lat;
+    require_face_extents(lat, mu);
+    const long long face = (long long)face_sites_dir(lat, mu);
+    const size_t cbytes = gauge->spec.chunk_bytes, nch = gauge->spec.nchunk;
+    const size_t mu_stride = nch * lat->stride;
+    for (int c = 0; c < 2; c++)
+      launch_face_pack(lat->geom(), mu, lat->dims[mu] - 1, c,
+                       static_cast<const char *>(gauge->data) + (c * 4 + mu) * mu_stride * cbytes, lat->stride,
+                       (int)nch, (int)cbytes, face, static_cast<char *>(dst) + c * nch * face * cbytes, nullptr,
+                       nullptr, 0, lat->stream);
+    check_launch();
+  });
 }
 
 extern "C" int qphix_gpu_halo_spinor_bytes(qphix_gpu_field psi, size_t *bytes)
@@ -951,7 +1082,7 @@ extern "C" int qphix_gpu_halo_pack_links(qphix_gpu_field gauge, void *dst)
 static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphix_gpu_field_s *psi,
                         qphix_gpu_field_s *gauge, qphix_gpu_field_s *aux, qphix_gpu_field_s *aux2, int isign,
                         int cb, unsigned dir_mask = 0xFFu, qphix_gpu_field_s *aux3 = nullptr,
-                        const qphix_gpu_halo_faces *faces = nullptr)
+                        const HaloSpec *faces = nullptr)
 {
   require_spinor(res, "res");
   require_spinor(psi, "psi");
@@ -1020,7 +1151,7 @@ static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qp
   }
   if (faces) {
     QPX_REQUIRE(!is_two_flavour(epi, ACHI_NONE), "halo mode is not provided for the two-flavour operators");
-    set_halo(a, p, psi, gauge, cb, faces);
+    set_halo(a, p, psi, gauge, cb, *faces);
   }
   dslash_launch(lat, res->prec, gauge->recon, epi, ACHI_NONE, a);
 }
@@ -1039,7 +1170,7 @@ struct ApplyOpts {
 static void achi_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphix_gpu_field_s *psi,
                       qphix_gpu_field_s *chi, qphix_gpu_field_s *gauge, qphix_gpu_field_s *aux, double alpha,
                       double beta, int isign, int cb, double musign, const ApplyOpts &o,
-                      const qphix_gpu_halo_faces *faces = nullptr)
+                      const HaloSpec *faces = nullptr)
 {
   require_spinor(res, "res");
   require_spinor(psi, "psi");
@@ -1100,7 +1231,7 @@ static void achi_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphi
   if (faces) {
     QPX_REQUIRE(!is_two_flavour(EPI_NONE, achi), "halo mode is not provided for the two-flavour operators");
     QPX_REQUIRE(!o.red_mask && o.post == POST_STORE, "halo launches take no fused solver updates");
-    set_halo(a, p, psi, gauge, cb, faces);
+    set_halo(a, p, psi, gauge, cb, *faces);
   }
   a.post = o.post;
   if (o.w) a.w = o.w->sarg();
@@ -1183,7 +1314,19 @@ extern "C" int qphix_gpu_dslash_halo(const qphix_gpu_op_params *p, qphix_gpu_fie
 {
   return guard([&] {
     QPX_REQUIRE(p && faces, "null argument");
-    dslash_core(*p, res, psi, gauge, aux, aux2, isign, cb, 0xFFu, nullptr, faces);
+    const HaloSpec h = halo_of(*faces);
+    dslash_core(*p, res, psi, gauge, aux, aux2, isign, cb, 0xFFu, nullptr, &h);
+  });
+}
+
+extern "C" int qphix_gpu_dslash_halo4(const qphix_gpu_op_params *p, qphix_gpu_field res, qphix_gpu_field psi,
+                                      qphix_gpu_field gauge, qphix_gpu_field aux, qphix_gpu_field aux2, int isign,
+                                      int cb, const qphix_gpu_halo_faces4 *faces)
+{
+  return guard([&] {
+    QPX_REQUIRE(p && faces, "null argument");
+    const HaloSpec h = halo_of(*faces);
+    dslash_core(*p, res, psi, gauge, aux, aux2, isign, cb, 0xFFu, nullptr, &h);
   });
 }
 
@@ -1194,7 +1337,20 @@ extern "C" int qphix_gpu_dslash_achimbdpsi_halo(const qphix_gpu_op_params *p, qp
 {
   return guard([&] {
     QPX_REQUIRE(p && faces, "null argument");
-    achi_core(*p, res, psi, chi, gauge, aux, alpha, beta, isign, cb, musign, ApplyOpts(), faces);
+    const HaloSpec h = halo_of(*faces);
+    achi_core(*p, res, psi, chi, gauge, aux, alpha, beta, isign, cb, musign, ApplyOpts(), &h);
+  });
+}
+
+extern "C" int qphix_gpu_dslash_achimbdpsi_halo4(const qphix_gpu_op_params *p, qphix_gpu_field res,
+                                                 qphix_gpu_field psi, qphix_gpu_field chi, qphix_gpu_field gauge,
+                                                 qphix_gpu_field aux, double alpha, double beta, int isign, int cb,
+                                                 double musign, const qphix_gpu_halo_faces4 *faces)
+{
+  return guard([&] {
+    QPX_REQUIRE(p && faces, "null argument");
+    const HaloSpec h = halo_of(*faces);
+    achi_core(*p, res, psi, chi, gauge, aux, alpha, beta, isign, cb, musign, ApplyOpts(), &h);
   });
 }
 

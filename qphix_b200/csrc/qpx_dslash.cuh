@@ -111,16 +111,19 @@ struct DslashArgs {
   double rho;           // i rho gamma_5 term
   double eps;           // flavour splitting of the two-flavour twisted mass
   int post;
-  // halo mode (general path only): the lattice is one slab of a lattice cut
-  // along t; hops across the slab's t edges read ghost faces instead of
-  // wrapping.  ghost_fwd = psi on the next slab's first time slice,
-  // ghost_bwd = psi on the previous slab's last slice, ghost_link = U_t on
-  // that slice (the backward hop's link), each indexed by the face site
-  // (z ny + y) nx/2 + x/2.  The forward edge takes coeff_t_edge, the backward
-  // edge coeff_t_bwd_edge (aniso_t, times t_boundary on the global edges).
+  // halo mode (general path only): the lattice is one block of a lattice cut
+  // along the directions whose bit is set in `halo`; a hop that leaves the
+  // block along such a direction reads a ghost face instead of wrapping.
+  // ghost_fwd[mu] = psi on the next block's first slice along mu,
+  // ghost_bwd[mu] = psi on the previous block's last slice, ghost_link[mu] =
+  // U_mu on that slice (the backward hop's link), indexed by the face site
+  // (halo_face): x: ((t nz + z) ny + y) / 2, y: (t nz + z) nx/2 + x/2,
+  // z: (t ny + y) nx/2 + x/2, t: (z ny + y) nx/2 + x/2.  The forward t edge
+  // takes coeff_t_edge, the backward one coeff_t_bwd_edge (aniso_t, times
+  // t_boundary where the edge is the global one).
   int halo;
-  SpinorArg ghost_fwd, ghost_bwd;
-  GaugeArg ghost_link;
+  SpinorArg ghost_fwd[4], ghost_bwd[4];
+  GaugeArg ghost_link[4];
   double coeff_t_bwd_edge;
   SpinorArg r, x, p, w; // extra vectors for POST_CG and RED_DOT_W_OUT
   ReduceArg red;
@@ -566,11 +569,30 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
     const int sxyzt = sxyz * g.nz;
     int nb[4][2][SP];  // [mu][0 back, 1 forward][lane]
     bool tlast[SP], tfirst[SP];
+    // halo mode (general path, one site per thread): per direction, whether
+    // the forward / backward hop leaves the block, and the neighbour's face site
+    bool hlast[4] = {false, false, false, false}, hfirst[4] = {false, false, false, false};
+    int hface[4] = {0, 0, 0, 0};
 #pragma unroll
     for (int l = 0; l < (RL ? 1 : SP); l++) {
       int xh, y, z, t, par;
       const int sl = s[l];
       site_coords(g, sl, a.cb, xh, y, z, t, par);
+      if (GEN && l == 0 && a.halo) {
+        const int x = 2 * xh + par;
+        hlast[0] = x + 1 == g.nx;
+        hfirst[0] = x == 0;
+        hlast[1] = y + 1 == g.ny;
+        hfirst[1] = y == 0;
+        hlast[2] = z + 1 == g.nz;
+        hfirst[2] = z == 0;
+        hlast[3] = t + 1 == g.nt;
+        hfirst[3] = t == 0;
+        hface[0] = ((t * g.nz + z) * g.ny + y) >> 1;
+        hface[1] = (t * g.nz + z) * g.nxh + xh;
+        hface[2] = (t * g.ny + y) * g.nxh + xh;
+        hface[3] = (z * g.ny + y) * g.nxh + xh;
+      }
       const int xf = (par == 0) ? xh : ((xh + 1 == g.nxh) ? 0 : xh + 1);
       const int xb = (par == 1) ? xh : ((xh == 0) ? g.nxh - 1 : xh - 1);
       nb[0][1][l] = sl - xh + xf;
@@ -613,11 +635,10 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
             (MU < 3) ? a.coeff_s : (tlast[l] ? a.coeff_t_edge : a.coeff_t);               \
         lanes_set(cf, c);                                                                 \
       }                                                                                   \
-      /* halo: the next slab's first slice (general path, one site per thread) */         \
-      const bool ghf = GEN && MU == 3 && a.halo && tlast[0];                              \
+      /* halo: the next block's first slice along MU (general path, one site per thread) */ \
+      const bool ghf = GEN && ((a.halo >> MU) & 1) && hlast[MU];                          \
       int ixf[SP];                                                                        \
-      _Pragma("unroll") for (int l = 0; l < SP; l++) ixf[l] =                             \
-          ghf ? s[l] - (a.geom.nt - 1) * sxyzt : nb[MU][1][l];                            \
+      _Pragma("unroll") for (int l = 0; l < SP; l++) ixf[l] = ghf ? hface[MU] : nb[MU][1][l]; \
       const cx<T> ph = {splat<T>(a.tbc[MU][0]), splat<T>(a.tbc[MU][1])};                  \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
@@ -625,13 +646,13 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
         cx<T> h[2][3], ch[2][3];                                                          \
         if constexpr (HalfProjection<L>::value) {                                         \
           __half2 w[12];                                                                  \
-          load_h2(ghf ? a.ghost_fwd : a.in, rhs0 + r, ixf[0], w, nrm);                    \
+          load_h2(ghf ? a.ghost_fwd[MU] : a.in, rhs0 + r, ixf[0], w, nrm);                    \
           project_h2<MU, -ISIGN>(w, h);                                                   \
         } else if constexpr (RhsHalfProjection<L>::value) {                               \
           project_h2_pair<MU, -ISIGN>(a.in, rhs0 + r, ixf[0], h, nrm);                    \
         } else {                                                                          \
           T psi[24];                                                                      \
-          L::load_raw(ghf ? a.ghost_fwd : a.in, rhs0 + r, ixf, psi, nrm);                 \
+          L::load_raw(ghf ? a.ghost_fwd[MU] : a.in, rhs0 + r, ixf, psi, nrm);                 \
           project<MU, -ISIGN>(psi, h);                                                    \
         }                                                                                 \
         if (tw || SP == 2) { /* SP = 2: the folded form costs registers (spills) */       \
@@ -646,12 +667,12 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
     }                                                                                     \
     /* backward hop: U_mu(x - mu)^+ (1 + isign g) psi(x - mu) */                          \
     if (!GEN || (a.dir_mask & (1u << (2 * MU)))) {                                        \
-      /* halo: the previous slab's last slice and its U_t (general path) */               \
-      const bool ghb = GEN && MU == 3 && a.halo && tfirst[0];                             \
+      /* halo: the previous block's last slice along MU and its U_MU (general path) */    \
+      const bool ghb = GEN && ((a.halo >> MU) & 1) && hfirst[MU];                         \
       int ixb[SP];                                                                        \
-      _Pragma("unroll") for (int l = 0; l < SP; l++) ixb[l] = ghb ? s[l] : nb[MU][0][l];  \
+      _Pragma("unroll") for (int l = 0; l < SP; l++) ixb[l] = ghb ? hface[MU] : nb[MU][0][l]; \
       cx<T> u[3][3];                                                                      \
-      L::template load_link<RECON>(ghb ? a.ghost_link : a.gauge, ghb ? 0 : 1 - a.cb,      \
+      L::template load_link<RECON>(ghb ? a.ghost_link[MU] : a.gauge, ghb ? 0 : 1 - a.cb,  \
                                    ghb ? 0 : MU, ixb, u);                                 \
       T cf;                                                                               \
       {                                                                                   \
@@ -669,13 +690,13 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
         cx<T> h[2][3], ch[2][3];                                                          \
         if constexpr (HalfProjection<L>::value) {                                         \
           __half2 w[12];                                                                  \
-          load_h2(ghb ? a.ghost_bwd : a.in, rhs0 + r, ixb[0], w, nrm);                    \
+          load_h2(ghb ? a.ghost_bwd[MU] : a.in, rhs0 + r, ixb[0], w, nrm);                    \
           project_h2<MU, ISIGN>(w, h);                                                    \
         } else if constexpr (RhsHalfProjection<L>::value) {                               \
           project_h2_pair<MU, ISIGN>(a.in, rhs0 + r, ixb[0], h, nrm);                     \
         } else {                                                                          \
           T psi[24];                                                                      \
-          L::load_raw(ghb ? a.ghost_bwd : a.in, rhs0 + r, ixb, psi, nrm);                 \
+          L::load_raw(ghb ? a.ghost_bwd[MU] : a.in, rhs0 + r, ixb, psi, nrm);                 \
           project<MU, ISIGN>(psi, h);                                                     \
         }                                                                                 \
         if (tw || SP == 2) { /* SP = 2: the folded form costs registers (spills) */       \

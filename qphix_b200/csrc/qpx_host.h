@@ -190,6 +190,13 @@ void launch_two_flav_clover(int prec, int vh, int npairs, SpinorArg out, SpinorA
                             CloverArg c, cudaStream_t st);
 void launch_clover_convert(int prec_in, int prec_out, Geom geo, const void *in, int vpc_in, void *out, int vpc_out,
                            long long stride, int nr, dim3 grid, cudaStream_t st);
+// halo mode: copy the sites of one checkerboard of the slice `slice` along
+// mu (face order of DslashArgs::halo) from `rows` chunk rows of src (row r at
+// src + r * src_stride chunks) to dst ([row][face]); with nsrc, also nrows
+// per-site norm rows to ndst ([row][face]); halo.cu
+void launch_face_pack(const Geom &g, int mu, int slice, int cb, const void *src, long long src_stride, int rows,
+                      int chunk_bytes, long long face, void *dst, const float *nsrc, float *ndst, int nrows,
+                      cudaStream_t st);
 // persistent CG kernel (qpx_persist.cuh) for (recon, Wilson or clover) with
 // FP64 / FP32 storage and isign = +1; nullptr where none is built
 const void *cg_persistent_kernel_f64(int recon, bool clover);

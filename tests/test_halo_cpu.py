@@ -1,7 +1,9 @@
 """Host side of the multi-GPU halo mode (qphix_b200/halo.py) on CPU: the
-t-slab index arithmetic, and the face exchange schedule run as gloo
-processes (world size 2 and 3): every rank must receive its next slab's
-first slice and its previous slab's last slice."""
+t-slab and block index arithmetic, the face order the Dslash kernel reads
+against the sites the face packer writes (every ghost entry is the lattice
+neighbour), and the face exchange schedule run as gloo processes (world size
+2 and 3): every rank must receive its next slab's first slice and its
+previous slab's last slice."""
 import os
 import socket
 
@@ -66,3 +68,106 @@ def test_exchange_faces_gloo(world):
     for r in range(world):
         nxt, prv = (r + 1) % world, (r - 1) % world
         assert got[r] == (10.0 * nxt + 1, 10.0 * prv + 2), (r, got)
+
+
+GRIDS = [(2, 1, 1, 1), (1, 2, 1, 1), (1, 1, 2, 1), (1, 1, 1, 2), (1, 2, 2, 1), (2, 2, 2, 2)]
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_block_cut_covers_the_lattice(grid):
+    dims = (8, 4, 4, 8)
+    n = int(np.prod(grid))
+    blocks = [halo.Block(dims, grid, r) for r in range(n)]
+    idx = np.concatenate([b.index() for b in blocks])
+    assert np.array_equal(np.sort(idx), np.arange(dims[0] * dims[1] * dims[2] * dims[3] // 2))
+    psi = F.gaussian_spinor(dims, 3)
+    whole = np.zeros_like(psi)
+    for b in blocks:
+        b.glue_spinor(whole, b.cut_spinor(psi))
+        for mu in range(4):
+            assert blocks[b.next[mu]].prev[mu] == b.rank
+    assert np.array_equal(whole, psi)
+    if grid[:3] == (1, 1, 1):  # a t cut is the t-slab decomposition
+        for b in blocks:
+            assert np.array_equal(b.cut_spinor(psi), halo.TSlab(dims, grid[3], b.rank).cut_spinor(psi))
+
+
+def _coords(dims, s, cb):
+    """local coordinates of checkerboard site s (the layout's site order)"""
+    nx, ny, nz, nt = dims
+    nxh = nx // 2
+    xh, r = s % nxh, s // nxh
+    y, r = r % ny, r // ny
+    z, t = r % nz, r // nz
+    return 2 * xh + ((y + z + t + cb) & 1), y, z, t
+
+
+def _face_index(dims, mu, x, y, z, t):
+    """the face order of the Dslash kernel's ghost reads (DslashArgs::halo)"""
+    nx, ny, nz, nt = dims
+    nxh = nx // 2
+    return [((t * nz + z) * ny + y) >> 1, (t * nz + z) * nxh + x // 2, (t * ny + y) * nxh + x // 2,
+            (z * ny + y) * nxh + x // 2][mu]
+
+
+def _face_site(dims, mu, k, cb, j):
+    """the packer's face site j of slice k along mu, checkerboard cb (halo.cu face_site)"""
+    nx, ny, nz, nt = dims
+    nxh = nx // 2
+    if mu == 3:
+        t, xh, r = k, j % nxh, j // nxh
+        y, z = r % ny, r // ny
+    elif mu == 2:
+        z, xh, r = k, j % nxh, j // nxh
+        y, t = r % ny, r // ny
+    elif mu == 1:
+        y, xh, r = k, j % nxh, j // nxh
+        z, t = r % nz, r // nz
+    else:
+        nyh = ny // 2
+        jy, r = j % nyh, j // nyh
+        z, t = r % nz, r // nz
+        y = 2 * jy + ((cb + k + z + t) & 1)
+        xh = k >> 1
+    return ((t * nz + z) * ny + y) * nxh + xh
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_block_faces_reach_the_neighbour(grid):
+    """For every site on a block's last (first) slice along a cut direction,
+    the ghost face entry the kernel reads is the packed site of the next
+    (previous) block that is its lattice neighbour."""
+    dims = (8, 4, 4, 8)
+    n = int(np.prod(grid))
+    blocks = [halo.Block(dims, grid, r) for r in range(n)]
+    ld = blocks[0].dims
+    nloc = ld[0] * ld[1] * ld[2] * ld[3] // 2
+    gdims = np.array(dims)
+    for b in blocks:
+        for mu in range(4):
+            if grid[mu] == 1:
+                continue
+            for cb in range(2):
+                for s in range(nloc):
+                    x, y, z, t = _coords(ld, s, cb)
+                    c = [x, y, z, t]
+                    for step, edge, nbr in ((+1, ld[mu] - 1, b.next[mu]), (-1, 0, b.prev[mu])):
+                        if c[mu] != edge:
+                            continue
+                        j = _face_index(ld, mu, x, y, z, t)
+                        # the neighbour block packs its first (last) slice of the other checkerboard
+                        k = 0 if step > 0 else ld[mu] - 1
+                        sn = _face_site(ld, mu, k, 1 - cb, j)
+                        xn, yn, zn, tn = _coords(ld, sn, 1 - cb)
+                        got = (np.array([xn, yn, zn, tn]) + np.array(blocks[nbr].origin)) % gdims
+                        want = np.array(c) + np.array(b.origin)
+                        want[mu] += step
+                        assert np.array_equal(got, want % gdims), (b.rank, mu, cb, s, step)
+                        assert 0 <= sn < nloc
+
+
+def test_block_rejects_odd_extents():
+    with pytest.raises(ValueError):
+        halo.Block((8, 4, 4, 6), (1, 1, 1, 2), 0)  # local t extent 3
+    with pytest.raises(ValueError):
+        halo.Block((8, 3, 4, 8), (2, 1, 1, 1), 0)  # an x cut with an odd local Ny
