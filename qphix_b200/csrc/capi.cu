@@ -716,6 +716,10 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
   TuneEntry best;
   best.us = 1e30f;
   best.candidates = (int)cands.size();
+  struct PdlOff {
+    PdlOff() { pdl_suspended() = true; }
+    ~PdlOff() { pdl_suspended() = false; }
+  } pdl_off;
   for (const auto &sh : cands) {
     dim3 grid = dslash_grid(lat, sh, a.nrhs);
     launch_dslash(prec, recon, epi, achi, sh, &t, grid, lat->stream);

@@ -50,6 +50,13 @@ inline bool pdl_enabled()
   }();
   return on;
 }
+// set while the autotuner times launch shapes: its back-to-back timed
+// launches must not overlap one another
+inline bool &pdl_suspended()
+{
+  static thread_local bool off = false;
+  return off;
+}
 
 // `size`: the block count that decides whether the attribute is set
 template <typename... KArgs, typename... Args>
@@ -65,7 +72,7 @@ cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStre
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = (pdl_enabled() && size >= kPdlMinBlocks) ? 1 : 0;
+  cfg.numAttrs = (pdl_enabled() && !pdl_suspended() && size >= kPdlMinBlocks) ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 

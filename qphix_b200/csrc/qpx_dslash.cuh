@@ -24,11 +24,17 @@
 // Register budget of the Dslash kernels, as the minimum resident 128-thread
 // blocks per SM the compiler must allow for (registers per thread capped at
 // 65536 / (128 x that)).  Measured on B200 (FP16 clover, 32^3x64 and
-// 16^3x32 x 8 rhs): one site per thread runs best with the compiler free to
-// use ~125 registers (1); two sites or two right-hand sides per thread with
-// at most 168 (3).
+// 16^3x32 x 8 rhs): one site per thread with 16-bit storage runs best at 4
+// blocks (at most 128 registers, which it fits without spilling; left free
+// it takes 135 and drops to 3 blocks, 13 % slower at 32^3x64); FP32 / FP64
+// storage, which sits at the HBM roofline with ~170-255 registers, keeps the
+// compiler free (1); two sites or two right-hand sides per thread with at
+// most 168 (3).
 #ifndef QPX_MINB1
 #define QPX_MINB1 1
+#endif
+#ifndef QPX_MINB1_16
+#define QPX_MINB1_16 4
 #endif
 #ifndef QPX_MINB2
 #define QPX_MINB2 3
@@ -36,7 +42,8 @@
 #ifndef QPX_MINBR
 #define QPX_MINBR 3
 #endif
-#define QPX_DSLASH_BOUNDS __launch_bounds__(QPX_BLOCK, (SP == 2 ? QPX_MINB2 : (R == 2 ? QPX_MINBR : QPX_MINB1)))
+#define QPX_DSLASH_BOUNDS \
+  __launch_bounds__(QPX_BLOCK, (SP == 2 ? QPX_MINB2 : (R == 2 ? QPX_MINBR : (P::has_norm ? QPX_MINB1_16 : QPX_MINB1))))
 
 namespace qpx {
 
