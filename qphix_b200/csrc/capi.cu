@@ -2071,8 +2071,8 @@ void pair_sum(std::vector<double> &v)
 // phases) and Vh x nrhs stays within kPersistentSites; unset or 0, solves
 // replay the captured iteration graph.  It is not the default: on B200 a
 // grid barrier costs about as much as a kernel boundary of the graph
-// (~2 us), and at 8^4 the graph replay measured faster (0.98 against 1.17
-// ms per FP64 Wilson CG solve).
+// (~2 us), and at 8^4 the graph replay measured slightly faster (0.98
+// against 1.01 ms per FP64 Wilson CG solve).
 constexpr long long kPersistentSites = 32768;
 
 static bool persistent_cg_wanted(qphix_gpu_eo_op_s *op, qphix_gpu_lattice_s *lat, int prec, int nrhs, int isign,
@@ -2112,6 +2112,12 @@ static bool run_cg_persistent(qphix_gpu_lattice_s *lat, const std::vector<Captur
   CgPersistArgs pa;
   memset(&pa, 0, sizeof(pa));
   for (int i = 0; i < 4; i++) pa.d[i] = cap[i].a;
+  // phases 1 and 3 leave g5 M x: with it phases 2 and 3 apply M^+ = g5 M g5
+  // through the isign = +1 kernel bodies (qpx_persist.cuh)
+  pa.d[1].g5_out = 1;
+  pa.d[3].g5_out = 1;
+  QPX_REQUIRE(!(pa.d[1].red.mask & RED_DOT_OUT_CHI) && !(pa.d[3].red.mask & RED_DOT_OUT_CHI),
+              "persistent CG: unexpected <out, chi> reduction");
   pa.r = r->sarg();
   pa.p = p->sarg();
   pa.state = lat->state;

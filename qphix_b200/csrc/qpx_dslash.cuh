@@ -118,6 +118,7 @@ struct DslashArgs {
   double rho;           // i rho gamma_5 term
   double eps;           // flavour splitting of the two-flavour twisted mass
   int post;
+  int g5_out;           // 1: the result times gamma_5 (see the post section of dslash_block)
   // halo mode (general path only): the lattice is one block of a lattice cut
   // along the directions whose bit is set in `halo`; a hop that leaves the
   // block along such a direction reads a ghost face instead of wrapping.
@@ -906,6 +907,18 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
           for (int r = 0; r < R; r++) red_dot(res[r], chi[r], act, red[r][3], red[r][4]);
         }
       }
+    }
+
+    // g5_out: the result times gamma_5 = diag(1, 1, -1, -1) (spins 2 and 3
+    // negated, exactly) before the post operation and the norm reductions;
+    // the <out, chi> value above is taken before it, so the host never
+    // combines the two.  The persistent CG applies M^+ = gamma_5 M gamma_5
+    // this way with the isign = +1 kernels.
+    if (a.g5_out) {
+#pragma unroll
+      for (int r = 0; r < R; r++)
+#pragma unroll
+        for (int k = 12; k < 24; k++) res[r][k] = -res[r][k];
     }
 
     // ---------------- post op + reductions ----------------

@@ -8,12 +8,19 @@
 //
 // One iteration (the graph-captured iteration of solve_cg, as phases):
 //   0  tmp = D p                      (first kernel of M, other checkerboard)
-//   1  mp = M p, partials of |mp|^2   (second kernel of M)
+//   1  mp = g5 M p, partials of |mp|^2  (second kernel of M, result times g5)
 //      barrier; every block: fold |mp|^2, FIN_CG_A -> a
-//   2  tmp = D^+ mp
-//   3  mmp = M^+ mp; r -= a mmp; x += a p; partials of |r|^2   (POST_CG)
+//   2  tmp = D mp
+//   3  mmp = g5 M mp = M^+ M p; r -= a mmp; x += a p; partials of |r|^2
 //      barrier; every block: fold |r|^2, FIN_CG_R -> b, convergence
 //   4  p = r + b p
+// M^+ = g5 M g5 (gamma_5-hermiticity of the Wilson and clover even-odd
+// operators; g5 = diag(1, 1, -1, -1) commutes with the clover term and turns
+// D(+1) into D(-1)), so phases 2 and 3 run the same two kernel bodies as
+// phases 0 and 1 with isign = +1: half the code, which matters because the
+// kernel's phases otherwise evict one another from the instruction cache.
+// The sign flips are exact, so the iterates are bit for bit those of the
+// graph path's D(-1) launches.
 // Phases 0-3 run the Dslash kernel's own per-block code (dslash_block) over
 // all virtual blocks of a launch of the regular kernel's shape (one site and
 // one right-hand side per thread); the folds add the partials in the order
@@ -41,7 +48,7 @@ struct GridBarrier {
 };
 
 struct CgPersistArgs {
-  DslashArgs d[4];  // phases 0-3, as captured from the regular solver's launches
+  DslashArgs d[4];  // phases 0-3, as captured from the regular solver's launches (d[1], d[3]: g5_out)
   SpinorArg r, p;   // phase 4
   SolverState *state;
   GridBarrier *bar;
@@ -130,33 +137,39 @@ __global__ void __launch_bounds__(QPX_BLOCK) cg_persistent_kernel(const __grid_c
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   unsigned int target = 0;  // this block's grid-barrier count
   while (!sst.done) {
-    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
-      dslash_block<PC, RECON, EPI, ACHI_NONE, 1, ISIGN, 1, false>(a.d[0], &sst, vb, nvb);
+    // the two halves of an iteration (M p, then M^+ on its result) run the
+    // same code: one call site per kernel body, the half's arguments
+    // selected at run time
+    bool ok = true;
+#pragma unroll 1
+    for (int half = 0; half < 2 && ok; half++) {
+      const DslashArgs &da = a.d[2 * half], &db = a.d[2 * half + 1];
+      for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+        dslash_block<PC, RECON, EPI, ACHI_NONE, 1, ISIGN, 1, false>(da, &sst, vb, nvb);
+        __syncthreads();
+      }
+      if (!grid_barrier(a.bar, target, 2 * half)) {
+        ok = false;
+        break;
+      }
+      for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+        dslash_block<PC, RECON, EPI_NONE, ACHI, 1, ISIGN, 1, false>(db, &sst, vb, nvb);
+        __syncthreads();
+      }
+      if (!grid_barrier(a.bar, target, 2 * half + 1)) {
+        ok = false;
+        break;
+      }
+      fold_in_block(db.red, a.nrhs, a.nsb, res);
+      if (wid == 0) {
+        if (half == 0)
+          finalize_warp<FIN_CG_A>(&sst, res, a.nrhs, db.red.nval, lane);
+        else
+          finalize_warp<FIN_CG_R>(&sst, res, a.nrhs, db.red.nval, lane);
+      }
       __syncthreads();
     }
-    if (!grid_barrier(a.bar, target, 0)) break;
-    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
-      dslash_block<PC, RECON, EPI_NONE, ACHI, 1, ISIGN, 1, false>(a.d[1], &sst, vb, nvb);
-      __syncthreads();
-    }
-    if (!grid_barrier(a.bar, target, 1)) break;
-    fold_in_block(a.d[1].red, a.nrhs, a.nsb, res);
-    if (wid == 0) finalize_warp<FIN_CG_A>(&sst, res, a.nrhs, a.d[1].red.nval, lane);
-    __syncthreads();
-    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
-      dslash_block<PC, RECON, EPI, ACHI_NONE, 1, -ISIGN, 1, false>(a.d[2], &sst, vb, nvb);
-      __syncthreads();
-    }
-    if (!grid_barrier(a.bar, target, 2)) break;
-    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
-      dslash_block<PC, RECON, EPI_NONE, ACHI, 1, -ISIGN, 1, false>(a.d[3], &sst, vb, nvb);
-      __syncthreads();
-    }
-    if (!grid_barrier(a.bar, target, 3)) break;
-    fold_in_block(a.d[3].red, a.nrhs, a.nsb, res);
-    if (wid == 0) finalize_warp<FIN_CG_R>(&sst, res, a.nrhs, a.d[3].red.nval, lane);
-    __syncthreads();
-    if (sst.done) break;
+    if (!ok || sst.done) break;
     // p = r + b p, the arithmetic of blas_kernel's B_CG_P
     const long long n = (long long)a.vh * a.nrhs;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
