@@ -294,8 +294,9 @@ def extra_configs():
     twisted-mass clover solve, the 32^3x64 16-shift multishift CG
     (qphix_b200.workloads) and the 2000-request Poisson serving stream at 70 %
     of measured capacity (qphix_b200.serve_bench, requests solved with
-    InvRichardsonMultiPrec), whose latency p50 / p99 are the metric's "p99
-    ms"."""
+    reliable-update BiCGStab: on the four-volume mix it gave the lower p99
+    latency; InvRichardsonMultiPrec the higher capacity, with a longer
+    tail), whose latency p50 / p99 are the metric's "p99 ms"."""
     import types
 
     from qphix_b200 import serve_bench, workloads
@@ -309,7 +310,7 @@ def extra_configs():
         out[name]["wall_s"] = round(time.perf_counter() - t0, 1)
     t0 = time.perf_counter()
     try:
-        out["serve"] = serve_bench.run(["--requests", "2000", "--load", "0.7", "--solver", "richardson"])
+        out["serve"] = serve_bench.run(["--requests", "2000", "--load", "0.7", "--solver", "ru"])
     except Exception as e:  # pragma: no cover
         out["serve"] = {"error": f"{type(e).__name__}: {e}"}
     out["serve"]["wall_s_total"] = round(time.perf_counter() - t0, 1)
