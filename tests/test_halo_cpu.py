@@ -171,3 +171,48 @@ def test_block_rejects_odd_extents():
         halo.Block((8, 4, 4, 6), (1, 1, 1, 2), 0)  # local t extent 3
     with pytest.raises(ValueError):
         halo.Block((8, 3, 4, 8), (2, 1, 1, 1), 0)  # an x cut with an odd local Ny
+
+
+def _block_rank_main(rank, world, port, grid, out):
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        b = halo.Block((8, 4, 8, 8), grid, rank)
+        got = {}
+        for mu in range(4):  # every rank walks the cut directions in the same order
+            if grid[mu] == 1:
+                continue
+            first = torch.full((4,), 100.0 * rank + 10 * mu + 1)
+            last = torch.full((4,), 100.0 * rank + 10 * mu + 2)
+            fwd, bwd = halo.exchange_faces_dir(first, last, b, mu)
+            got[mu] = (float(fwd[0]), float(bwd[0]))
+        out[rank] = got
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("grid", [(2, 1, 2, 1), (1, 2, 1, 2)])
+def test_exchange_faces_dir_gloo(grid):
+    """exchange_faces_dir on a 2 x 2 grid of blocks as four gloo processes:
+    along each cut direction a rank receives its next block's first slice
+    and its previous block's last slice."""
+    import torch.multiprocessing as mp
+    world = int(np.prod(grid))
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.start_processes(_block_rank_main, args=(world, port, grid, out), nprocs=world, join=True,
+                           start_method="spawn")
+        got = dict(out)
+    for r in range(world):
+        b = halo.Block((8, 4, 8, 8), grid, r)
+        for mu in range(4):
+            if grid[mu] == 1:
+                continue
+            assert got[r][mu] == (100.0 * b.next[mu] + 10 * mu + 1, 100.0 * b.prev[mu] + 10 * mu + 2), (r, mu, got)
