@@ -608,7 +608,6 @@ bool tune_enabled()
 
 dim3 dslash_grid(const qphix_gpu_lattice_s *lat, const DslashShape &sh, int nrhs)
 {
-  if (sh.rls) return dim3((unsigned)((lat->vh + kRlsSites - 1) / kRlsSites));
   long long per = (long long)QPX_BLOCK * (sh.rl ? 1 : sh.SP);
   long long nsb = (lat->vh + per - 1) / per;
   return dim3((unsigned)(nsb * (nrhs / (sh.rl ? 2 : sh.R))));
@@ -618,9 +617,6 @@ bool shape_built(int prec, int recon, int epi, int achi, const DslashShape &sh, 
 {
   if (nrhs % sh.R) return false;
   if (sh.rl && nrhs % 2) return false;
-  // rls: ceil(Vh / 32) partials per (rhs, value) must fit the lattice's
-  // partials buffer, sized for ceil(Vh / 128) blocks x QPX_MAX_RHS rhs
-  if (sh.rls && nrhs > QPX_MAX_RHS * kRlsSites / QPX_BLOCK) return false;
   return launch_dslash(prec, recon, epi, achi, sh, nullptr, dim3(1), nullptr);
 }
 
@@ -660,15 +656,13 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
   }
   if (gen) return default_shape(prec, true);
   // forced shapes (experiments and tests): QPHIX_GPU_RHS_LANES=1 selects two
-  // right-hand sides in the float2 lanes of one site, =2 the same over links
-  // staged in shared memory (rls)
+  // right-hand sides in the float2 lanes of one site
   const char *fr = getenv("QPHIX_GPU_RHS_TILE"), *fs = getenv("QPHIX_GPU_SITES_PER_THREAD");
   const char *fl = getenv("QPHIX_GPU_RHS_LANES");
-  if (fl && (atoi(fl) == 1 || atoi(fl) == 2)) {
+  if (fl && atoi(fl) == 1) {
     DslashShape sh;
     sh.SP = 2;
     sh.rl = true;
-    sh.rls = atoi(fl) == 2;
     if (shape_built(prec, recon, epi, achi, sh, a.nrhs)) return sh;
   } else if (fr || fs) {
     DslashShape sh = default_shape(prec, false);
@@ -685,11 +679,10 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
       sh.SP = sp;
       if (shape_built(prec, recon, epi, achi, sh, a.nrhs)) cands.push_back(sh);
     }
-  for (int shared = 0; shared <= 1; shared++) {
+  {
     DslashShape sh;
     sh.SP = 2;
     sh.rl = true;
-    sh.rls = shared == 1;
     if (shape_built(prec, recon, epi, achi, sh, a.nrhs)) cands.push_back(sh);
   }
   if (cands.size() <= 1) return cands.empty() ? default_shape(prec, false) : cands[0];
@@ -729,14 +722,12 @@ static DslashShape choose_shape(qphix_gpu_lattice_s *lat, int prec, int recon, i
   } pdl_off;
   for (const auto &sh : cands) {
     dim3 grid = dslash_grid(lat, sh, a.nrhs);
-    // a reducing launch is timed with the fold of its partials, whose number
-    // depends on the shape
-    const int nparts = sh.rls ? (int)grid.x : (int)(grid.x / (a.nrhs / (sh.rl ? 2 : sh.R)));
+    // a reducing launch is timed with the fold of its partials
     auto once = [&] {
       launch_dslash(prec, recon, epi, achi, sh, &t, grid, lat->stream);
       check_launch();
       if (red) {
-        launch_fold(t.red, nullptr, a.nrhs, nparts, lat->stream);
+        launch_fold(t.red, nullptr, a.nrhs, (int)(grid.x / (a.nrhs / (sh.rl ? 2 : sh.R))), lat->stream);
         check_launch();
       }
     };
@@ -783,11 +774,9 @@ extern "C" int qphix_gpu_tune_entry(int index, char *key, size_t key_len, int *r
     auto it = g_tune.begin();
     std::advance(it, index);
     if (key && key_len) snprintf(key, key_len, "%s", it->first.c_str());
-    // the rhs-lanes shape reads as two right-hand sides on 0 sites per
-    // thread, the rls shape (rhs lanes over shared links) on -1
-    const DslashShape &sh = it->second.sh;
-    if (rhs_tile) *rhs_tile = sh.rl ? 2 : sh.R;
-    if (sites_per_thread) *sites_per_thread = sh.rls ? -1 : (sh.rl ? 0 : sh.SP);
+    // the rhs-lanes shape reads as two right-hand sides on 0 sites per thread
+    if (rhs_tile) *rhs_tile = it->second.sh.rl ? 2 : it->second.sh.R;
+    if (sites_per_thread) *sites_per_thread = it->second.sh.rl ? 0 : it->second.sh.SP;
     if (launch_us) *launch_us = it->second.us;
   });
 }
@@ -834,7 +823,7 @@ static void dslash_launch(qphix_gpu_lattice_s *lat, int prec, int recon, int epi
   check_launch();
   if (a.red.mask) {  // the blocks' partials: one per (site block, rhs, value)
     const int ntiles = a.nrhs / (sh.rl ? 2 : sh.R);
-    launch_fold(a.red, a.state, a.nrhs, (int)(sh.rls ? grid.x : grid.x / ntiles), lat->stream);
+    launch_fold(a.red, a.state, a.nrhs, (int)(grid.x / ntiles), lat->stream);
     check_launch();
   }
 }

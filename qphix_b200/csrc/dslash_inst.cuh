@@ -2,7 +2,6 @@
 // precision lives in its own translation unit so they compile in parallel.
 #pragma once
 
-#include <atomic>
 #include <type_traits>
 
 #include "qpx_finalize.cuh"
@@ -53,44 +52,6 @@ void launch_dslash_nd(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStr
     throw Error(QPHIX_GPU_EINVAL, "unsupported two-flavour dslash combination");
 }
 
-// the rls shape (dslash_rls_kernel): dynamic shared memory beyond the
-// default 48 KB is granted per kernel and device once
-template <typename P, int RECON, int EPI, int ACHI, int S>
-void launch_rls_one(const DslashArgs &a, dim3 grid, cudaStream_t st)
-{
-  constexpr int smem = rls_smem_bytes(EPI == EPI_CLOV || ACHI == ACHI_CLOV);
-  static std::atomic<unsigned> granted{0};
-  int dev = 0;
-  check_pdl(cudaGetDevice(&dev));
-  const unsigned bit = 1u << (dev & 31);
-  if (!(granted.load() & bit)) {
-    check_pdl(cudaFuncSetAttribute(dslash_rls_kernel<P, RECON, EPI, ACHI, S>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    granted.fetch_or(bit);
-  }
-  check_pdl(launch_pdl_smem(dslash_rls_kernel<P, RECON, EPI, ACHI, S>, grid, dim3(QPX_BLOCK), smem, st,
-                            (long long)grid.x, a));
-}
-
-template <typename P, int RECON, int S>
-void launch_dslash_rls(int epi, int achi, const DslashArgs &a, dim3 grid, cudaStream_t st)
-{
-  if (achi == ACHI_NONE) {
-    switch (epi) {
-    case EPI_NONE: launch_rls_one<P, RECON, EPI_NONE, ACHI_NONE, S>(a, grid, st); return;
-    case EPI_CLOV: launch_rls_one<P, RECON, EPI_CLOV, ACHI_NONE, S>(a, grid, st); return;
-    case EPI_TMINV: launch_rls_one<P, RECON, EPI_TMINV, ACHI_NONE, S>(a, grid, st); return;
-    }
-  } else if (epi == EPI_NONE) {
-    switch (achi) {
-    case ACHI_ALPHA: launch_rls_one<P, RECON, EPI_NONE, ACHI_ALPHA, S>(a, grid, st); return;
-    case ACHI_CLOV: launch_rls_one<P, RECON, EPI_NONE, ACHI_CLOV, S>(a, grid, st); return;
-    case ACHI_TM: launch_rls_one<P, RECON, EPI_NONE, ACHI_TM, S>(a, grid, st); return;
-    }
-  }
-  throw Error(QPHIX_GPU_EINVAL, "unsupported dslash epilogue combination for the rls shape");
-}
-
 // isign is a template parameter: the projector signs become adds / subtracts
 template <typename P, int RECON, int R, int SP, bool GEN, bool RL = false>
 void launch_dslash_s(int epi, int achi, const DslashArgs *a, dim3 grid, cudaStream_t st)
@@ -107,9 +68,7 @@ void launch_dslash_s(int epi, int achi, const DslashArgs *a, dim3 grid, cudaStre
 //   general path (dir mask, twisted phases): R = 1, SP = 1
 //   fast path: R = 1 SP = 1 for every precision; for FP32 arithmetic also
 //   SP = 2 (both link kinds), R = 2 (12-real links) and two right-hand sides
-//   in the float2 lanes (rl, 12-real links, even nrhs); for 16-bit storage
-//   the rl lanes over shared links (rls: 12-real links, even nrhs, every
-//   epilogue but the full-clover and two-flavour ones)
+//   in the float2 lanes (rl, 12-real links, even nrhs)
 template <typename P>
 bool launch_dslash_p(int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,
                      cudaStream_t st)
@@ -125,21 +84,6 @@ bool launch_dslash_p(int recon, int epi, int achi, const DslashShape &sh, const 
     else
       plus ? launch_dslash_nd<P, 18, 1>(epi, achi, *a, grid, st) : launch_dslash_nd<P, 18, -1>(epi, achi, *a, grid, st);
     return true;
-  }
-  if (sh.rls) {
-    constexpr bool built = std::is_same<P, F16>::value || std::is_same<P, BF16>::value || std::is_same<P, Q16>::value;
-    if constexpr (built) {
-      if (!sh.rl || sh.R != 1 || sh.SP != 2 || sh.gen || recon != 12) return false;
-      if (epi == EPI_FCLOV || (epi != EPI_NONE && achi != ACHI_NONE)) return false;
-      if (a && a->nrhs % 2) return false;
-      if (!a) return true;
-      if (a->isign == 1)
-        launch_dslash_rls<P, 12, 1>(epi, achi, *a, grid, st);
-      else
-        launch_dslash_rls<P, 12, -1>(epi, achi, *a, grid, st);
-      return true;
-    }
-    return false;
   }
   if (sh.rl) {
     if constexpr (fp32) {

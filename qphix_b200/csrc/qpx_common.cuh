@@ -58,16 +58,15 @@ inline bool &pdl_suspended()
   return off;
 }
 
-// `size`: the block count that decides whether the attribute is set;
-// `smem`: dynamic shared memory per block
+// `size`: the block count that decides whether the attribute is set
 template <typename... KArgs, typename... Args>
-cudaError_t launch_pdl_smem(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                            long long size, Args &&...args)
+cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, long long size,
+                       Args &&...args)
 {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
+  cfg.dynamicSmemBytes = 0;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -75,13 +74,6 @@ cudaError_t launch_pdl_smem(void (*kernel)(KArgs...), dim3 grid, dim3 block, siz
   cfg.attrs = at;
   cfg.numAttrs = (pdl_enabled() && !pdl_suspended() && size >= kPdlMinBlocks) ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
-}
-
-template <typename... KArgs, typename... Args>
-cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, long long size,
-                       Args &&...args)
-{
-  return launch_pdl_smem(kernel, grid, block, 0, st, size, std::forward<Args>(args)...);
 }
 
 enum Prec : int { PREC_F64 = 0, PREC_F32 = 1, PREC_F16 = 2, PREC_BF16 = 3, PREC_Q16 = 4, PREC_Q16F32 = 5 };

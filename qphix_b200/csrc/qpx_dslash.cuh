@@ -506,128 +506,6 @@ __device__ __forceinline__ void full6_rows(const T *rows, const T *in, T *out, i
   }
 }
 
-// ---- right-hand-side lanes over shared links (the rls launch shape) ---------
-// One block of QPX_BLOCK = 128 threads covers a group of 32 sites of the
-// target checkerboard and every right-hand side: warp w runs the rhs pairs
-// (tiles) w, w + 4, ... of the group in the float2 lanes, as the rhs-lanes
-// shape does, lane l on site 32 group + l.  The group's eight links per site
-// (U_mu(x) for the forward hops, U_mu(x - mu) for the backward ones) and,
-// with a clover epilogue, its 72 clover reals are loaded, converted and
-// (12-real) reconstructed once per block into shared memory, already
-// broadcast to both lanes, instead of once per rhs pair; the hops of every
-// pair read them back with 128-bit shared loads.
-// Shared layout in float4 units: element e = 3 row + col of link slot
-// k = 2 mu + (1 forward, 0 backward) of group site l at [(32 k + l) 9 + e] as
-// (re, re, im, im); clover reals 2j, 2j + 1 of site l at
-// [kRlsLinkF4 + 37 l + j] as (c_2j, c_2j, c_2j+1, c_2j+1).  Site strides of
-// 9 and 37 float4 (36 and 148 words: 4 x odd) put the eight lanes of each
-// phase of a 128-bit shared access on distinct banks.
-constexpr int kRlsSites = 32;
-constexpr int kRlsLinkF4 = 8 * kRlsSites * 9;  // 36,864 bytes
-constexpr int kRlsClovStride = 37;
-constexpr int kRlsClovF4 = kRlsSites * kRlsClovStride;  // 18,944 bytes
-__host__ __device__ constexpr int rls_smem_bytes(bool clov) { return (kRlsLinkF4 + (clov ? kRlsClovF4 : 0)) * 16; }
-static_assert(QPX_BLOCK == 4 * kRlsSites, "the rls shape stages one link direction per warp");
-
-extern __shared__ float4 qpx_rls_smem[];
-
-__device__ __forceinline__ void rls_link(int slot, cx<f2> u[3][3])
-{
-  const float4 *p = qpx_rls_smem + (slot * kRlsSites + (threadIdx.x & 31)) * 9;
-#pragma unroll
-  for (int e = 0; e < 9; e++) {
-    const float4 q = p[e];
-    u[e / 3][e % 3] = {make_float2(q.x, q.y), make_float2(q.z, q.w)};
-  }
-}
-
-// clover reals [k0, k0 + n), k0 and n even
-__device__ __forceinline__ void rls_clover(int k0, int n, f2 *v)
-{
-  const float4 *p = qpx_rls_smem + kRlsLinkF4 + (threadIdx.x & 31) * kRlsClovStride + k0 / 2;
-#pragma unroll
-  for (int j = 0; j < n / 2; j++) {
-    const float4 q = p[j];
-    v[2 * j] = make_float2(q.x, q.y);
-    v[2 * j + 1] = make_float2(q.z, q.w);
-  }
-}
-
-template <typename P, int K0, int N>
-__device__ __forceinline__ void rls_stage_clover(const CloverArg &c, int s, int lane)
-{
-  float v[N];
-  CloverIO<P, 72>::load(c, s, K0, N, v);
-  float4 *p = qpx_rls_smem + kRlsLinkF4 + lane * kRlsClovStride + K0 / 2;
-#pragma unroll
-  for (int j = 0; j < N / 2; j++) p[j] = make_float4(v[2 * j], v[2 * j], v[2 * j + 1], v[2 * j + 1]);
-}
-
-// The block's staging pass: warp w loads the forward and backward links of
-// direction mu = w for the group's 32 sites and a quarter of their clover
-// reals ([0, 24), [24, 40), [40, 56), [56, 72)).  Lanes past the end of the
-// checkerboard stage nothing; no thread reads their slots.
-template <typename P, int RECON, bool CLOV>
-__device__ __forceinline__ void rls_stage(const DslashArgs &a, int group)
-{
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int s = group * kRlsSites + lane;
-  if (s >= a.geom.vh) return;
-  const Geom &g = a.geom;
-  int xh, y, z, t, par;
-  site_coords(g, s, a.cb, xh, y, z, t, par);
-  int nbb;  // backward neighbour along mu = w (the formulas of dslash_block)
-  if (w == 0) {
-    const int xb = (par == 1) ? xh : ((xh == 0) ? g.nxh - 1 : xh - 1);
-    nbb = s - xh + xb;
-  } else {
-    const int c = (w == 1) ? y : ((w == 2) ? z : t);
-    const int n = (w == 1) ? g.ny : ((w == 2) ? g.nz : g.nt);
-    const int st = (w == 1) ? g.nxh : ((w == 2) ? g.nxh * g.ny : g.nxh * g.ny * g.nz);
-    nbb = s + ((c == 0) ? (n - 1) * st : -st);
-  }
-#pragma unroll
-  for (int fwd = 1; fwd >= 0; fwd--) {
-    cx<float> u[3][3];
-    GaugeIO<P, RECON>::load(a.gauge, fwd ? a.cb : 1 - a.cb, w, fwd ? s : nbb, u);
-    float4 *p = qpx_rls_smem + ((2 * w + fwd) * kRlsSites + lane) * 9;
-#pragma unroll
-    for (int e = 0; e < 9; e++)
-      p[e] = make_float4(u[e / 3][e % 3].re, u[e / 3][e % 3].re, u[e / 3][e % 3].im, u[e / 3][e % 3].im);
-  }
-  if constexpr (CLOV) {
-    if (w == 0)
-      rls_stage_clover<P, 0, 24>(a.clov, s, lane);
-    else if (w == 1)
-      rls_stage_clover<P, 24, 16>(a.clov, s, lane);
-    else if (w == 2)
-      rls_stage_clover<P, 40, 16>(a.clov, s, lane);
-    else
-      rls_stage_clover<P, 56, 16>(a.clov, s, lane);
-  }
-}
-
-// a hop's link: from global memory through the lane policy, or (rls) from
-// the block's staged copy
-template <typename L, int RECON, bool RLS, typename T>
-__device__ __forceinline__ void hop_link(const GaugeArg &g, int cb, int mu, const int *s, int slot, cx<T> u[3][3])
-{
-  if constexpr (RLS)
-    rls_link(slot, u);
-  else
-    L::template load_link<RECON>(g, cb, mu, s, u);
-}
-
-// clover reals [k0, k0 + n) of a 72-real clover field, likewise
-template <typename L, bool RLS, typename T>
-__device__ __forceinline__ void epi_clover(const CloverArg &c, const int *s, int k0, int n, T *v)
-{
-  if constexpr (RLS)
-    rls_clover(k0, n, v);
-  else
-    L::template load_clover<72>(c, s, k0, n, v);
-}
-
 // per-lane values of a lane-generic type from SP doubles
 __device__ __forceinline__ void lanes_set(double &d, const double *v) { d = v[0]; }
 __device__ __forceinline__ void lanes_set(float &d, const double *v) { d = (float)v[0]; }
@@ -646,10 +524,6 @@ __device__ __forceinline__ void lanes_set(f2 &d, const double *v) { d = make_flo
 // RL     (with SP = 2, R = 1, fast path) the float2 lanes hold two
 //        right-hand sides of one site instead of two sites: links and
 //        clover terms are loaded once for both (RhsLanes).
-// RLS    (with RL) the rls shape: the block's 32-site group, links and
-//        clover reals from the block's shared staging (rls_stage), block
-//        `vblock` = (group, tile) with the tile fastest, one partial per
-//        warp (reduce_warp).
 // Blocks cover (site block, rhs tile) pairs with the rhs tile varying
 // fastest, so the blocks that share a site block (and its links) run
 // together and the links of the later right-hand sides come from L2.
@@ -659,15 +533,13 @@ __device__ __forceinline__ void lanes_set(f2 &d, const double *v) { d = make_flo
 // dslash_kernel runs it once per CUDA block; the persistent solver kernels
 // (qpx_persist.cuh) run it over all virtual blocks of a phase from a grid
 // that stays resident.
-template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN, int SP, bool GEN, bool RL = false,
-          bool RLS = false>
+template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN, int SP, bool GEN, bool RL = false>
 __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverState *st, int vblock, int nvblocks)
 {
   using L = typename std::conditional<RL, RhsLanes<P>, Lanes<P, SP>>::type;
   using T = typename L::T;
   static_assert(SP == 1 || R == 1, "two sites per thread take one right-hand side");
   static_assert(!RL || (SP == 2 && R == 1 && !GEN), "right-hand-side lanes: SP = 2, R = 1, fast path");
-  static_assert(!RLS || RL, "the rls shape runs right-hand-side lanes");
   constexpr int RT = RL ? 2 : R;  // right-hand sides per thread
   const int ntiles = a.nrhs / RT;
   const int tile = vblock % ntiles;
@@ -676,7 +548,7 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
   int s[SP];
   bool act[SP];
   if (RL) {
-    s[0] = RLS ? sblock * kRlsSites + (threadIdx.x & 31) : sblock * QPX_BLOCK + threadIdx.x;
+    s[0] = sblock * QPX_BLOCK + threadIdx.x;
     act[0] = s[0] < a.geom.vh;
     s[SP - 1] = s[0];
     act[SP - 1] = act[0];
@@ -763,7 +635,7 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
     /* forward hop: U_mu(x) (1 - isign g) psi(x + mu) */                                  \
     if (!GEN || (a.dir_mask & (1u << (2 * MU + 1)))) {                                    \
       cx<T> u[3][3];                                                                      \
-      hop_link<L, RECON, RLS>(a.gauge, a.cb, MU, s, 2 * MU + 1, u);                       \
+      L::template load_link<RECON>(a.gauge, a.cb, MU, s, u);                              \
       T cf;                                                                               \
       {                                                                                   \
         double c[SP];                                                                     \
@@ -808,8 +680,8 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
       int ixb[SP];                                                                        \
       _Pragma("unroll") for (int l = 0; l < SP; l++) ixb[l] = ghb ? hface[MU] : nb[MU][0][l]; \
       cx<T> u[3][3];                                                                      \
-      hop_link<L, RECON, RLS>(ghb ? a.ghost_link[MU] : a.gauge, ghb ? 0 : 1 - a.cb,       \
-                              ghb ? 0 : MU, ixb, 2 * MU, u);                              \
+      L::template load_link<RECON>(ghb ? a.ghost_link[MU] : a.gauge, ghb ? 0 : 1 - a.cb,  \
+                                   ghb ? 0 : MU, ixb, u);                                 \
       T cf;                                                                               \
       {                                                                                   \
         double c[SP];                                                                     \
@@ -864,7 +736,7 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
 #pragma unroll
         for (int b = 0; b < 2; b++) {
           T blk[36];
-          epi_clover<L, RLS>(a.clov, s, 36 * b, 36, blk);
+          L::template load_clover<72>(a.clov, s, 36 * b, 36, blk);
 #pragma unroll
           for (int r = 0; r < R; r++) herm6_apply(blk, acc[r], res[r], b);
         }
@@ -944,7 +816,7 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
 #pragma unroll
         for (int b = 0; b < 2; b++) {
           T blk[36];
-          epi_clover<L, RLS>(a.clov, s, 36 * b, 36, blk);
+          L::template load_clover<72>(a.clov, s, 36 * b, 36, blk);
 #pragma unroll
           for (int r = 0; r < R; r++) herm6_apply(blk, chi[r], res[r], b);
         }
@@ -1107,12 +979,8 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
       }
     }
   }
-  if (a.red.mask) {
-    if constexpr (RLS)
-      reduce_warp<RT>(a.red, a.nrhs, rhs0, red_slots(a.red.mask), red, sblock, nvblocks / ntiles);
-    else
-      reduce_epilogue<RT>(a.red, a.nrhs, rhs0, red_slots(a.red.mask), red, sblock, nvblocks / ntiles);
-  }
+  if (a.red.mask)
+    reduce_epilogue<RT>(a.red, a.nrhs, rhs0, red_slots(a.red.mask), red, sblock, nvblocks / ntiles);
 }
 
 template <typename P, int RECON, int EPI, int ACHI, int R, int ISIGN, int SP, bool GEN, bool RL = false>
@@ -1122,24 +990,6 @@ __global__ void QPX_DSLASH_BOUNDS dslash_kernel(const __grid_constant__ DslashAr
   pdl_trigger();
   if (a.state && a.state->done) return;
   dslash_block<P, RECON, EPI, ACHI, R, ISIGN, SP, GEN, RL>(a, a.state, blockIdx.x, gridDim.x);
-}
-
-// The rls shape: block = one 32-site group, staged links and clover reals,
-// then warp w runs the group's rhs pairs w, w + 4, ... (grid: ceil(Vh / 32)
-// blocks, launched with rls_smem_bytes(clover) of dynamic shared memory).
-template <typename P, int RECON, int EPI, int ACHI, int ISIGN>
-__global__ void __launch_bounds__(QPX_BLOCK, QPX_MINBR) dslash_rls_kernel(const __grid_constant__ DslashArgs a)
-{
-  pdl_wait();
-  pdl_trigger();
-  if (a.state && a.state->done) return;
-  constexpr bool kClov = EPI == EPI_CLOV || ACHI == ACHI_CLOV;
-  rls_stage<P, RECON, kClov>(a, blockIdx.x);
-  __syncthreads();
-  const int ntiles = a.nrhs / 2;
-  for (int tile = threadIdx.x >> 5; tile < ntiles; tile += QPX_BLOCK / 32)
-    dslash_block<P, RECON, EPI, ACHI, 1, ISIGN, 2, false, true, true>(a, a.state, blockIdx.x * ntiles + tile,
-                                                                     gridDim.x * ntiles);
 }
 
 }  // namespace qpx

@@ -160,10 +160,6 @@ struct DslashShape {
   int R = 1, SP = 1;
   bool gen = false;
   bool rl = false;  // with R = 1, SP = 2: two right-hand sides of one site in the float2 lanes
-  // with rl: a block per 32-site group running every rhs pair over links and
-  // clover reals staged once in shared memory (dslash_rls_kernel); grid
-  // ceil(Vh / 32) blocks, one reduction partial per (block, rhs, value)
-  bool rls = false;
 };
 // a == nullptr: report only whether the shape is built for (prec, recon)
 bool launch_dslash(int prec, int recon, int epi, int achi, const DslashShape &sh, const DslashArgs *a, dim3 grid,

@@ -141,30 +141,6 @@ __device__ __forceinline__ void reduce_epilogue(const ReduceArg &ra, int nrhs, i
   }
 }
 
-// The same for kernels whose warps work on different right-hand sides (the
-// rls Dslash shape): each warp's sums are its block's partial for its rhs,
-// written by lane 0 under site-block index `sblock`; no block barrier, so
-// warps may run different numbers of tiles.  Called by all 32 lanes.
-template <int R>
-__device__ __forceinline__ void reduce_warp(const ReduceArg &ra, int nrhs, int rhs0, int slots,
-                                            const double val[R][QPX_MAX_RED], int sblock, int nsblocks)
-{
-  const int lane = threadIdx.x & 31;
-#pragma unroll
-  for (int r = 0; r < R; r++) {
-    int o = 0;
-#pragma unroll
-    for (int k = 0; k < QPX_MAX_RED; k++) {
-      if (slots & (1 << k)) {
-        const double s = warp_sum(val[r][k]);
-        if (lane == 0 && rhs0 + r < nrhs)
-          store_partial(ra.partials + ((long long)(rhs0 + r) * ra.nval + o) * nsblocks + sblock, s);
-        o++;
-      }
-    }
-  }
-}
-
 constexpr int QPX_FOLD_THREADS = 1024;
 
 }  // namespace qpx

@@ -37,8 +37,7 @@ def algorithmic_bytes(prec, recon, kind, nrhs, achi=False):
 SHAPES = {"auto": {}, "sp1": {"QPHIX_GPU_RHS_TILE": "1", "QPHIX_GPU_SITES_PER_THREAD": "1"},
           "sp2": {"QPHIX_GPU_RHS_TILE": "1", "QPHIX_GPU_SITES_PER_THREAD": "2"},
           "r2": {"QPHIX_GPU_RHS_TILE": "2", "QPHIX_GPU_SITES_PER_THREAD": "1"},
-          "rhs_lanes": {"QPHIX_GPU_RHS_LANES": "1"},
-          "rhs_lanes_shared": {"QPHIX_GPU_RHS_LANES": "2"}}
+          "rhs_lanes": {"QPHIX_GPU_RHS_LANES": "1"}}
 
 
 def main(argv=None):
@@ -53,8 +52,7 @@ def main(argv=None):
     ap.add_argument("--no-flush", action="store_true")
     ap.add_argument("--shape", default="auto", choices=list(SHAPES),
                     help="launch shape: auto (the autotuner's), sp1 / sp2 (sites per thread), r2 (two rhs per "
-                         "thread), rhs_lanes (two rhs in the float2 lanes), rhs_lanes_shared (the same over links "
-                         "and clover terms staged in shared memory once per 32-site group)")
+                         "thread), rhs_lanes (two rhs in the float2 lanes)")
     ap.add_argument("--norms", action="store_true",
                     help="with --achi --kind clover: fuse the |res|^2 and <res, chi> reductions (BiCGStab's "
                          "t = M s launch), folded on the device")

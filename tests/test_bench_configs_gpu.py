@@ -55,8 +55,7 @@ def c2_oracle(oracle, c2):
 SHAPE_ENV = {"sp1": {"QPHIX_GPU_RHS_TILE": "1", "QPHIX_GPU_SITES_PER_THREAD": "1"},
              "r2": {"QPHIX_GPU_RHS_TILE": "2", "QPHIX_GPU_SITES_PER_THREAD": "1"},
              "sp2": {"QPHIX_GPU_RHS_TILE": "1", "QPHIX_GPU_SITES_PER_THREAD": "2"},
-             "rhs_lanes": {"QPHIX_GPU_RHS_LANES": "1"},
-             "rhs_lanes_shared": {"QPHIX_GPU_RHS_LANES": "2"}}
+             "rhs_lanes": {"QPHIX_GPU_RHS_LANES": "1"}}
 
 
 class forced_shape:
@@ -92,7 +91,7 @@ def test_c2_fp64_operator_8rhs(api, c2, c2_oracle):
 
 
 @pytest.mark.parametrize("prec", ["f16", "f32", "f64"])
-@pytest.mark.parametrize("shape", ["sp1", "r2", "sp2", "rhs_lanes", "rhs_lanes_shared"])
+@pytest.mark.parametrize("shape", ["sp1", "r2", "sp2", "rhs_lanes"])
 def test_c2_inner_kernels_every_shape(api, oracle, c2, c2_oracle, prec, shape):
     """The inner operator's two clover Dslash launches at 16^3x32 x 8 rhs in
     each built launch shape: A^-1 D psi and A chi - b D psi with the three
