@@ -42,11 +42,6 @@
 #ifndef QPX_MINBR
 #define QPX_MINBR 3
 #endif
-// 1: FP16 fast-path hops read their neighbour spinors through the cp.async
-// ring (HopRing); 0: straight global loads
-#ifndef QPX_HOP_RING
-#define QPX_HOP_RING 1
-#endif
 #define QPX_DSLASH_BOUNDS \
   __launch_bounds__(QPX_BLOCK, (SP == 2 ? QPX_MINB2 : (R == 2 ? QPX_MINBR : (P::has_norm ? QPX_MINB1_16 : QPX_MINB1))))
 
@@ -253,92 +248,6 @@ template <>
 struct RhsHalfProjection<RhsLanes<F16>> {
   static constexpr bool value = true;
 };
-
-// ---- neighbour spinors through asynchronous copies -----------------------
-// On the fast path with FP16 storage (the half-projection paths above) each
-// thread copies the neighbour spinors of its next kHopDepth hops straight
-// from global into its own slots of a shared-memory ring (cp.async, no
-// registers held while in flight) and reads a hop's words back only when it
-// computes that hop: the eight gathers of a site overlap one another and the
-// arithmetic without the registers that hoisted loads would take.  A thread
-// reads only the slots it filled itself, so the only synchronisation is its
-// own cp.async.wait_group.  Slot layout [slot][rhs][chunk][thread] (16-byte
-// chunks, consecutive threads in consecutive words: conflict-free).
-constexpr int kHopDepth = 2;
-constexpr int kHopSlots = kHopDepth + 1;
-
-template <int NQ>
-struct HopRing {
-  uint4 sp[kHopSlots][NQ][3][QPX_BLOCK];
-  float nrm[kHopSlots][NQ][QPX_BLOCK];
-};
-struct NoHopRing {};
-
-__device__ __forceinline__ void cp_async16(void *dst, const void *src)
-{
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async4(void *dst, const void *src)
-{
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait()
-{
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// start the copies of right-hand sides rhs0 .. rhs0 + NQ - 1 at site ix into `slot`
-template <int NQ>
-__device__ __forceinline__ void hop_fetch(HopRing<NQ> &b, int slot, const SpinorArg &f, int rhs0, long long ix)
-{
-  const int t = threadIdx.x;
-#pragma unroll
-  for (int q = 0; q < NQ; q++) {
-    const uint4 *p = reinterpret_cast<const uint4 *>(f.data) + (rhs0 + q) * f.rhs_stride_chunks + ix;
-#pragma unroll
-    for (int k = 0; k < 3; k++) cp_async16(&b.sp[slot][q][k][t], p + k * f.stride);
-    cp_async4(&b.nrm[slot][q][t], f.norm + (rhs0 + q) * f.stride + ix);
-  }
-}
-
-// the words and norm of right-hand side q of `slot`, as load_h2 returns them
-template <int NQ>
-__device__ __forceinline__ void hop_words(const HopRing<NQ> &b, int slot, int q, __half2 w[12], float &nrm)
-{
-  const int t = threadIdx.x;
-#pragma unroll
-  for (int k = 0; k < 3; k++) {
-    const uint4 d = b.sp[slot][q][k][t];
-    w[4 * k] = *reinterpret_cast<const __half2 *>(&d.x);
-    w[4 * k + 1] = *reinterpret_cast<const __half2 *>(&d.y);
-    w[4 * k + 2] = *reinterpret_cast<const __half2 *>(&d.z);
-    w[4 * k + 3] = *reinterpret_cast<const __half2 *>(&d.w);
-  }
-  nrm = b.nrm[slot][q][t];
-}
-
-// project_h2_pair on ring words: rhs q = 0 in lane .x, q = 1 in lane .y
-template <int MU, int SG>
-__device__ __forceinline__ void project_ring_pair(const HopRing<2> &b, int slot, cx<f2> h[2][3], f2 &nrm)
-{
-  __half2 wa[12], wb[12];
-  float na, nb;
-  hop_words(b, slot, 0, wa, na);
-  hop_words(b, slot, 1, wb, nb);
-  cx<float> ha[2][3], hb[2][3];
-  project_h2<MU, SG>(wa, ha);
-  project_h2<MU, SG>(wb, hb);
-#pragma unroll
-  for (int sp = 0; sp < 2; sp++)
-#pragma unroll
-    for (int c = 0; c < 3; c++)
-      h[sp][c] = {make_float2(ha[sp][c].re, hb[sp][c].re), make_float2(ha[sp][c].im, hb[sp][c].im)};
-  nrm = make_float2(na, nb);
-}
 
 // a per-rhs solver coefficient in the arithmetic type: the lanes of a
 // two-rhs thread take right-hand sides rr and rr + 1
@@ -632,9 +541,6 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
   static_assert(SP == 1 || R == 1, "two sites per thread take one right-hand side");
   static_assert(!RL || (SP == 2 && R == 1 && !GEN), "right-hand-side lanes: SP = 2, R = 1, fast path");
   constexpr int RT = RL ? 2 : R;  // right-hand sides per thread
-  // neighbour spinors through the asynchronous-copy ring (fast path, FP16)
-  constexpr bool RING = !GEN && QPX_HOP_RING && (HalfProjection<L>::value || RhsHalfProjection<L>::value);
-  __shared__ typename std::conditional<RING, HopRing<RT>, NoHopRing>::type ring;
   const int ntiles = a.nrhs / RT;
   const int tile = vblock % ntiles;
   const int sblock = vblock / ntiles;
@@ -722,24 +628,6 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
     for (int r = 0; r < R; r++)
 #pragma unroll
       for (int k = 0; k < 24; k++) acc[r][k] = zero;
-    // hops in the order 0 fwd, 0 bwd, 1 fwd, ...: hop j reads site
-    // nb[j / 2][j odd ? 0 : 1]; the ring holds the next kHopDepth of them
-    if constexpr (RING) {
-#pragma unroll
-      for (int j = 0; j < kHopDepth; j++) {
-        hop_fetch<RT>(ring, j, a.in, rhs0, nb[j / 2][(j % 2) ? 0 : 1][0]);
-        cp_async_commit();
-      }
-    }
-
-// hop J's ring step: start the copies of hop J + kHopDepth, then wait for hop J's
-#define QPX_RING_STEP(J)                                                                  \
-  if constexpr (RING) {                                                                   \
-    constexpr int JN = (J) + kHopDepth;                                                   \
-    if constexpr (JN < 8) hop_fetch<RT>(ring, JN % kHopSlots, a.in, rhs0, nb[JN / 2][(JN % 2) ? 0 : 1][0]); \
-    cp_async_commit();                                                                    \
-    cp_async_wait<kHopDepth>();                                                           \
-  }
 
 #define QPX_HOP(MU)                                                                       \
   {                                                                                       \
@@ -760,18 +648,11 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
       int ixf[SP];                                                                        \
       _Pragma("unroll") for (int l = 0; l < SP; l++) ixf[l] = ghf ? hface[MU] : nb[MU][1][l]; \
       const cx<T> ph = {splat<T>(a.tbc[MU][0]), splat<T>(a.tbc[MU][1])};                  \
-      QPX_RING_STEP(2 * MU)                                                               \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
         T nrm;                                                                            \
         cx<T> h[2][3], ch[2][3];                                                          \
-        if constexpr (RING && RL) {                                                       \
-          project_ring_pair<MU, -ISIGN>(ring, (2 * MU) % kHopSlots, h, nrm);              \
-        } else if constexpr (RING) {                                                      \
-          __half2 w[12];                                                                  \
-          hop_words(ring, (2 * MU) % kHopSlots, r, w, nrm);                               \
-          project_h2<MU, -ISIGN>(w, h);                                                   \
-        } else if constexpr (HalfProjection<L>::value) {                                  \
+        if constexpr (HalfProjection<L>::value) {                                         \
           __half2 w[12];                                                                  \
           load_h2(ghf ? a.ghost_fwd[MU] : a.in, rhs0 + r, ixf[0], w, nrm);                    \
           project_h2<MU, -ISIGN>(w, h);                                                   \
@@ -811,18 +692,11 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
         lanes_set(cf, c);                                                                 \
       }                                                                                   \
       const cx<T> ph = {splat<T>(a.tbc[MU][0]), splat<T>(-a.tbc[MU][1])};                 \
-      QPX_RING_STEP(2 * MU + 1)                                                           \
       _Pragma("unroll") for (int r = 0; r < R; r++)                                       \
       {                                                                                   \
         T nrm;                                                                            \
         cx<T> h[2][3], ch[2][3];                                                          \
-        if constexpr (RING && RL) {                                                       \
-          project_ring_pair<MU, ISIGN>(ring, (2 * MU + 1) % kHopSlots, h, nrm);           \
-        } else if constexpr (RING) {                                                      \
-          __half2 w[12];                                                                  \
-          hop_words(ring, (2 * MU + 1) % kHopSlots, r, w, nrm);                           \
-          project_h2<MU, ISIGN>(w, h);                                                    \
-        } else if constexpr (HalfProjection<L>::value) {                                  \
+        if constexpr (HalfProjection<L>::value) {                                         \
           __half2 w[12];                                                                  \
           load_h2(ghb ? a.ghost_bwd[MU] : a.in, rhs0 + r, ixb[0], w, nrm);                    \
           project_h2<MU, ISIGN>(w, h);                                                    \
@@ -849,7 +723,6 @@ __device__ __forceinline__ void dslash_block(const DslashArgs &a, const SolverSt
     QPX_HOP(2)
     QPX_HOP(3)
 #undef QPX_HOP
-#undef QPX_RING_STEP
 
     // ---------------- epilogue ----------------
     T res[R][24];
