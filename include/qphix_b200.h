@@ -383,6 +383,30 @@ int qphix_gpu_solve_richardson(qphix_gpu_eo_op op_outer, qphix_gpu_eo_op op_inne
                                qphix_gpu_field x, qphix_gpu_field rhs, double rsd_target, double delta,
                                int max_iters, int inner_max_iters, int isign, int cb,
                                qphix_gpu_solve_info *info);
+/* CG on shifted normal equations, one shift per right-hand side: solves
+ * (M^dag M + shifts[i]) x_i = rhs_i (shifts[i] >= 0) for every right-hand
+ * side i of the block at once.  No counterpart in the reference; with all
+ * shifts 0 it is qphix_gpu_solve_cg.  rsd_target[i] is relative, and
+ * info[i].rsd_sq_final / true_rel_resid are the shifted system's true
+ * residual. */
+int qphix_gpu_solve_cg_shifted(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs, const double *shifts,
+                               const double *rsd_target, int max_iters, int isign, int cb,
+                               qphix_gpu_solve_info *info);
+/* Multishift CG with low-precision iterations (no counterpart in the
+ * reference; the systems are MInvCG's, minvcg.h:77): one multishift CG on
+ * op_low (FP32 or 16-bit storage) to rsd_low (nullptr: rsd_target), then
+ * every shift refined side by side in the precision of op and x, by
+ * low-precision shifted CG solves on the normalised true residuals, until
+ * every shift meets rsd_target[i] by its true residual |rhs - (M^dag M +
+ * shifts[i]) x_i| / |rhs|.  x: n_shift one-rhs fields in op's precision.
+ * Outputs: multishift iterations, refinement iterations (summed over the
+ * rounds, the slowest shift's count per round), refinement rounds, each
+ * shift's final true relative residual squared, operator applications. */
+int qphix_gpu_solve_mshift_cg_mixed(qphix_gpu_eo_op op, qphix_gpu_eo_op op_low, qphix_gpu_field *x,
+                                    qphix_gpu_field rhs, int n_shift, const double *shifts,
+                                    const double *rsd_target, const double *rsd_low, int max_iters, int isign,
+                                    int cb, int *n_iters, int *refine_iters, int *corrections,
+                                    double *rel_sq_final, unsigned long *mv_apps);
 
 /* ---- BLAS (include/qphix/blas_new_c.h) --------------------------------------
  * Per right-hand side results are written to out[nrhs] (complex: out[2*nrhs]). */

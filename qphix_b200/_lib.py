@@ -136,6 +136,9 @@ _SIGS = {
                                    C.POINTER(C.c_ulong)], I_),
     "qphix_gpu_solve_bicgstab_mixed": ([P, P, P, P, D, D, I_, I_, I_, C.POINTER(SolveInfo)], I_),
     "qphix_gpu_solve_richardson": ([P, P, I_, P, P, D, D, I_, I_, I_, I_, C.POINTER(SolveInfo)], I_),
+    "qphix_gpu_solve_cg_shifted": ([P, P, P, P, P, I_, I_, I_, C.POINTER(SolveInfo)], I_),
+    "qphix_gpu_solve_mshift_cg_mixed": ([P, P, PP, P, I_, P, P, P, I_, I_, I_, C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_int), P, C.POINTER(C.c_ulong)], I_),
     "qphix_gpu_blas_norm2": ([P, P], I_),
     "qphix_gpu_blas_norm2_noalloc": ([P, P], I_),
     "qphix_gpu_blas_inner_product": ([P, P, P], I_),

@@ -691,6 +691,49 @@ class MInvCG:
         return it.value, fin, mv.value
 
 
+class InvCGShifted(InvCG):
+    """CG on (M^+M + shifts[i]) x_i = rhs_i, one shift per right-hand side of
+    the block (qphix_gpu_solve_cg_shifted; no reference counterpart)."""
+
+    def __call__(self, x, rhs, shifts, rsd_targets, isign=1, cb=1):
+        inf = _infos(x.nrhs)
+        sh = np.ascontiguousarray(np.broadcast_to(shifts, (x.nrhs,)), dtype=np.float64)
+        rs = np.ascontiguousarray(np.broadcast_to(rsd_targets, (x.nrhs,)), dtype=np.float64)
+        _solve_rc(L._lib.qphix_gpu_solve_cg_shifted(self.M.h, x.h, rhs.h, sh.ctypes.data_as(C.c_void_p),
+                                                    rs.ctypes.data_as(C.c_void_p), self.max_iters, isign,
+                                                    cb, inf))
+        return _as_dicts(inf)
+
+
+class MInvCGMixed:
+    """Multishift CG with low-precision iterations and a batched refinement of
+    every shift to its target (qphix_gpu_solve_mshift_cg_mixed; no reference
+    counterpart).  xs: one-rhs fields in M's precision; M_low: the same
+    operator on low-precision fields."""
+
+    def __init__(self, M, M_low, max_iters, max_shifts=32):
+        self.M, self.M_low, self.max_iters, self.max_shifts = M, M_low, max_iters, max_shifts
+
+    def __call__(self, xs, rhs, shifts, rsd_targets, isign=1, cb=1, rsd_low=None):
+        n = len(shifts)
+        if n > self.max_shifts:
+            raise ValueError("too many shifts")
+        xh = (C.c_void_p * n)(*[x.h.value for x in xs])
+        sh = np.ascontiguousarray(shifts, dtype=np.float64)
+        rs = np.ascontiguousarray(rsd_targets, dtype=np.float64)
+        rl = None if rsd_low is None else np.ascontiguousarray(np.broadcast_to(rsd_low, (n,)), dtype=np.float64)
+        fin = np.zeros(n)
+        it, rit, corr = C.c_int(0), C.c_int(0), C.c_int(0)
+        mv = C.c_ulong(0)
+        check(L._lib.qphix_gpu_solve_mshift_cg_mixed(
+            self.M.h, self.M_low.h, C.cast(xh, L.PP), rhs.h, n, sh.ctypes.data_as(C.c_void_p),
+            rs.ctypes.data_as(C.c_void_p), None if rl is None else rl.ctypes.data_as(C.c_void_p),
+            self.max_iters, isign, cb, C.byref(it), C.byref(rit), C.byref(corr),
+            fin.ctypes.data_as(C.c_void_p), C.byref(mv)))
+        return {"n_iters": it.value, "refine_iters": rit.value, "corrections": corr.value,
+                "true_rel_resid": np.sqrt(fin), "mv_apps": mv.value}
+
+
 # ---------------------------------------------------------------------------
 # BLAS
 # ---------------------------------------------------------------------------

@@ -167,6 +167,7 @@ void launch_fold(const ReduceArg &ra, SolverState *state, int nrhs, int nparts, 
     QPX_FOLD_CASE(FIN_STORE)
     QPX_FOLD_CASE(FIN_MCG_D)
     QPX_FOLD_CASE(FIN_MCG_R)
+    QPX_FOLD_CASE(FIN_CG_P)
   default: throw Error(QPHIX_GPU_EINVAL, "bad finalize step");
   }
 #undef QPX_FOLD_CASE

@@ -151,9 +151,10 @@ static void create_lattice(const int latt[4], cudaMemPool_t pool, qphix_gpu_latt
       QPX_CUDA(cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking));
       L->owns_stream = true;
       L->mempool = pool;
-      // per-block partials, plus 2 x QPX_MAX_RHS doubles at the end for the
-      // Richardson per-rhs scale factors
-      L->partials_len = (size_t)nblocks_for(L->vh) * QPX_MAX_RHS * QPX_MAX_RED + 2 * QPX_MAX_RHS;
+      // per-block partials, plus 3 x QPX_MAX_RHS doubles at the end: the
+      // Richardson per-rhs scale factors (last two) and the shifted CG's
+      // per-rhs shifts (shift_coefs)
+      L->partials_len = (size_t)nblocks_for(L->vh) * QPX_MAX_RHS * QPX_MAX_RED + 3 * QPX_MAX_RHS;
       QPX_CUDA(cudaMalloc(&L->partials, L->partials_len * sizeof(double)));
       QPX_CUDA(cudaMalloc(&L->result, QPX_MAX_RHS * QPX_MAX_RED * sizeof(double)));
       QPX_CUDA(cudaMallocHost(&L->h_result, QPX_MAX_RHS * QPX_MAX_RED * sizeof(double)));
@@ -2145,8 +2146,35 @@ static bool run_cg_persistent(qphix_gpu_lattice_s *lat, const std::vector<Captur
   return true;
 }
 
+// the per-rhs shift coefficients of a shifted CG solve (device, QPX_MAX_RHS)
+static double *shift_coefs(qphix_gpu_lattice_s *lat) { return lat->partials + lat->partials_len - 3 * QPX_MAX_RHS; }
+
+// r -= s_i x_i per rhs with |r|^2 on the host: the shift term of a shifted
+// system's residual b - (M^+M + s) x (the per-rhs -s_i already in
+// shift_coefs(lat))
+static std::vector<double> sub_shift_norm(qphix_gpu_lattice_s *lat, int prec, int nr, qphix_gpu_field_s *x,
+                                          qphix_gpu_field_s *r)
+{
+  BlasCall c;
+  c.op = B_CAXPBY_NORM;
+  c.x = x;
+  c.y = r;
+  c.a = Coef{0, 0, shift_coefs(lat), nullptr};
+  c.b = cval(1.0);
+  c.slots = 0x1;
+  blas_launch(lat, prec, nr, c);
+  const double *h = fetch_result(lat, nr, 1);
+  return std::vector<double>(h, h + nr);
+}
+
+// shifts == nullptr: CG on M^+M.  Otherwise CG on M^+M + s_i for right-hand
+// side i (shifted systems solved side by side, e.g. the refinement of a
+// multishift solve); the iteration then stores M^+M p and updates r and x
+// in a BLAS pass (B_CG_RX: r -= a (M^+M p + s p)), and the p update's fold
+// keeps |p|^2 for d = <p, (M^+M + s) p> = |Mp|^2 + s |p|^2.
 void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rhs, const double *rsd,
-              int max_iters, int isign, int cb, qphix_gpu_solve_info *info, bool final_resid = true)
+              int max_iters, int isign, int cb, qphix_gpu_solve_info *info, bool final_resid = true,
+              const double *shifts = nullptr)
 {
   check_solver_fields(op, x, rhs, true);
   auto *lat = x->lat;
@@ -2155,6 +2183,16 @@ void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
   // products sum over both flavours (include/qphix/invcg.h with num_flav = 2)
   const bool coupled = two_flavour_kind(op->p.kind);
   QPX_REQUIRE(!coupled || nr % 2 == 0, "two-flavour fields hold (up, down) pairs");
+  QPX_REQUIRE(!shifts || !coupled, "shifted CG takes single-flavour operators");
+  if (shifts) {
+    std::vector<double> ns(nr);
+    for (int i = 0; i < nr; i++) {
+      QPX_REQUIRE(shifts[i] >= 0.0, "shifts must be non-negative");
+      ns[i] = -shifts[i];
+    }
+    QPX_CUDA(cudaMemcpyAsync(shift_coefs(lat), ns.data(), sizeof(double) * nr, cudaMemcpyHostToDevice,
+                             lat->stream));
+  }
   Timer timer(lat);
   Tmp mp(lat, prec, nr), mmp(lat, prec, nr), r(lat, prec, nr), p(lat, prec, nr);
   std::vector<double> chi = norm2_host(rhs);
@@ -2170,11 +2208,16 @@ void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
   blas_launch(lat, prec, nr, c);
   const double *h = fetch_result(lat, nr, 1);
   std::vector<double> cp(h, h + nr);
+  if (shifts) cp = sub_shift_norm(lat, prec, nr, x, r);
   if (coupled) pair_sum(cp);
   SolverState &S = state_reset(lat, nr, max_iters + 1);
   S.coupled = coupled ? 1 : 0;
   bool all = true;
   for (int i = 0; i < nr; i++) {
+    if (shifts) {
+      S.v[S_AUX3][i] = shifts[i];
+      S.v[S_AUX4][i] = cp[i];  // |p|^2 with p = r
+    }
     S.v[S_RSD][i] = rsd[i] * rsd[i] * chi[i];
     S.v[S_C][i] = cp[i];
     S.v[S_RNORM][i] = cp[i];
@@ -2220,8 +2263,47 @@ void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
       pu.state = ds;
       blas_launch(lat, prec, nr, pu);
     };
+    auto step_shifted = [&] {
+      ApplyOpts o1;
+      o1.red_mask = RED_NORM_OUT;
+      o1.fin = FIN_CG_A;
+      o1.state = ds;
+      eo_apply(op, mp, p, isign, cb, o1);
+      ApplyOpts o2;
+      o2.state = ds;
+      eo_apply(op, mmp, mp, -isign, cb, o2);
+      BlasCall u;
+      u.op = B_CG_RX;
+      u.x = x;
+      u.y = r;
+      u.z = mmp;
+      u.v = p;
+      u.a = cslot(ds, S_A);
+      u.b = cslot(ds, S_AUX3);
+      u.slots = 0x1;
+      u.fin = FIN_CG_R;
+      u.state = ds;
+      blas_launch(lat, prec, nr, u);
+      BlasCall pu;
+      pu.op = B_CG_P;
+      pu.x = r;
+      pu.y = p;
+      pu.a = cslot(ds, S_B);
+      pu.slots = 0x1;
+      pu.fin = FIN_CG_P;
+      pu.state = ds;
+      blas_launch(lat, prec, nr, pu);
+    };
     bool done = false;
-    if (persistent_cg_wanted(op, lat, prec, nr, isign, coupled)) {
+    if (shifts) {
+      ApplyOpts t1;
+      t1.red_mask = RED_NORM_OUT;
+      pretune_op(op, lat, nr, isign, cb, {t1});
+      std::string key = "cgs/" + std::to_string(op->serial) + "/" + fkey(x) + "/" + fkey(mp) + fkey(mmp) +
+                        fkey(r) + fkey(p) + "/" + std::to_string(isign) + std::to_string(cb);
+      run_iterations(lat, step_shifted, max_iters + 1, key);
+      done = true;
+    } else if (persistent_cg_wanted(op, lat, prec, nr, isign, coupled)) {
       std::vector<CapturedDslash> cap;
       g_dslash_capture = &cap;
       try {
@@ -2245,6 +2327,10 @@ void solve_cg(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *x, qphix_gpu_field_s *rh
   std::vector<double> abs2(nr, -1.0), rel(nr, -1.0);
   if (final_resid) {
     true_residual(op, x, rhs, mmp, r, isign, cb, true, chi, abs2, rel);
+    if (shifts) {
+      abs2 = sub_shift_norm(lat, prec, nr, x, r);
+      for (int i = 0; i < nr; i++) rel[i] = chi[i] > 0 ? std::sqrt(abs2[i] / chi[i]) : 0.0;
+    }
     if (coupled) {
       pair_sum(abs2);
       for (int i = 0; i < nr; i++) rel[i] = chi[i] > 0 ? std::sqrt(abs2[i] / chi[i]) : 0.0;
@@ -3023,5 +3109,183 @@ extern "C" int qphix_gpu_solve_mshift_cg(qphix_gpu_eo_op op, qphix_gpu_field *x,
 {
   return guard([&] {
     solve_mshift(op, x, rhs, n_shift, shifts, rsd_target, max_iters, isign, cb, n_iters, rsd_sq_final, mv_apps);
+  });
+}
+
+// ---------------------------------------------------------------------------
+// CG on the shifted normal equations (M^+M + s_i) x_i = b_i, one shift per
+// right-hand side (no reference counterpart: the batched form of the
+// per-shift refinement that follows a multishift solve).
+extern "C" int qphix_gpu_solve_cg_shifted(qphix_gpu_eo_op op, qphix_gpu_field x, qphix_gpu_field rhs,
+                                          const double *shifts, const double *rsd_target, int max_iters, int isign,
+                                          int cb, qphix_gpu_solve_info *info)
+{
+  QPX_SOLVE_ENTRY({
+    QPX_REQUIRE(info && x && shifts && rsd_target, "null argument");
+    solve_cg(op, x, rhs, rsd_target, max_iters, isign, cb, info, true, shifts);
+  })
+}
+
+// one right-hand side of a multi-rhs spinor field as a one-rhs field argument
+static SpinorArg slice_arg(const qphix_gpu_field_s *f, int s)
+{
+  SpinorArg a = f->sarg();
+  a.data = static_cast<char *>(a.data) + (size_t)s * a.rhs_stride_chunks * 16;  // 16-byte spinor chunks
+  if (a.norm) a.norm += (size_t)s * a.stride;
+  return a;
+}
+
+static void convert_slice(int pdst, const SpinorArg &dst, int psrc, const SpinorArg &src, qphix_gpu_lattice_s *lat)
+{
+  launch_convert(pdst, psrc, (int)lat->vh, src, dst, Coef{1.0, 0, nullptr, nullptr}, nullptr,
+                 dim3(nblocks_for(lat->vh), 1), lat->stream, 0);
+  check_launch();
+}
+
+// Multishift CG with low-precision iterations (no reference counterpart;
+// the shifted systems of include/qphix/minvcg.h:77-387): one multishift CG
+// on op_low (FP32 or 16-bit storage) to rsd_low, then every shift's solution
+// in op's precision is refined side by side, a shift per right-hand side:
+// R = b - (M^+M + s) X in op's precision, the low-precision shifted CG on
+// R / |R| (qphix_gpu_solve_cg_shifted's iteration) to the fraction of
+// |R| that is still missing (with a margin), X += |R| D, until every shift
+// meets rsd_target by its true residual.
+static void solve_mshift_mixed(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opl, qphix_gpu_field_s **x,
+                               qphix_gpu_field_s *rhs, int ns, const double *shifts, const double *rsd,
+                               const double *rsd_low, int max_iters, int isign, int cb, int *n_iters,
+                               int *refine_iters, int *corrections, double *rel_sq_final, unsigned long *mv_apps)
+{
+  QPX_REQUIRE(op && opl && x && rhs && shifts && rsd && n_iters && refine_iters && corrections && rel_sq_final &&
+                  mv_apps,
+              "null argument");
+  QPX_REQUIRE(ns >= 1 && ns <= QPX_MAX_RHS, "n_shift must be in [1, 32]");
+  require_spinor(rhs, "rhs");
+  QPX_REQUIRE(rhs->nrhs == 1, "multishift CG takes one right-hand side");
+  for (int s = 0; s < ns; s++) {
+    require_spinor(x[s], "x");
+    require_same(x[s], rhs);
+    QPX_REQUIRE(x[s]->nrhs == 1, "multishift CG solutions hold one right-hand side");
+    QPX_REQUIRE(shifts[s] >= 0.0, "shifts must be non-negative");
+  }
+  require_same(rhs, op->gauge);
+  QPX_REQUIRE(!two_flavour_kind(op->p.kind) && !two_flavour_kind(opl->p.kind),
+              "multishift CG takes single-flavour operators");
+  auto *lat = rhs->lat;
+  QPX_REQUIRE(same_shape(opl->gauge->lat, lat), "the two operators' lattices differ");
+  sync_op_fields(op, lat);
+  sync_op_fields(opl, lat);
+  const int prec = rhs->prec, lp = opl->gauge->prec;
+  const double bn = norm2_host(rhs)[0];
+
+  // 1. the multishift CG in the low precision
+  Tmp bl(lat, lp, 1);
+  convert_field(bl, rhs, cval(1.0), nullptr);
+  std::vector<Tmp *> xl;
+  struct Free {
+    std::vector<Tmp *> &v;
+    ~Free()
+    {
+      for (auto *t : v) delete t;
+    }
+  } free_xl{xl};
+  std::vector<qphix_gpu_field_s *> xlp;
+  for (int s = 0; s < ns; s++) {
+    xl.push_back(new Tmp(lat, lp, 1));
+    xlp.push_back(*xl.back());
+  }
+  std::vector<double> lsq(ns);
+  unsigned long mv = 0;
+  solve_mshift(opl, xlp.data(), bl, ns, shifts, rsd_low ? rsd_low : rsd, max_iters, isign, cb, n_iters, lsq.data(),
+               &mv);
+
+  // 2. every shift as a right-hand side in op's precision
+  Tmp X(lat, prec, ns), B(lat, prec, ns), T1(lat, prec, ns), T2(lat, prec, ns), R(lat, prec, ns);
+  Tmp Rl(lat, lp, ns), Dl(lat, lp, ns);
+  for (int s = 0; s < ns; s++) {
+    convert_slice(prec, slice_arg(X, s), lp, static_cast<qphix_gpu_field_s *>(*xl[s])->sarg(), lat);
+    convert_slice(prec, slice_arg(B, s), prec, rhs->sarg(), lat);
+  }
+  std::vector<double> nsig(ns), t2(ns), rn(ns);
+  for (int s = 0; s < ns; s++) {
+    nsig[s] = -shifts[s];
+    t2[s] = rsd[s] * rsd[s] * bn;
+  }
+  auto residual = [&] {  // R = B - (M^+M + s) X, |R_s|^2
+    eo_apply(op, T1, X, isign, cb, ApplyOpts());
+    eo_apply(op, T2, T1, -isign, cb, ApplyOpts());
+    mv += 2;
+    BlasCall c;
+    c.op = B_XMY_NORM;
+    c.x = B;
+    c.y = T2;
+    c.z = R;
+    c.slots = 0x1;
+    blas_launch(lat, prec, ns, c);
+    QPX_CUDA(cudaMemcpyAsync(shift_coefs(lat), nsig.data(), sizeof(double) * ns, cudaMemcpyHostToDevice,
+                             lat->stream));
+    rn = sub_shift_norm(lat, prec, ns, X, R);
+  };
+
+  // 3. refinement rounds
+  double *d_scales = lat->partials + lat->partials_len - 2 * QPX_MAX_RHS;
+  std::vector<qphix_gpu_solve_info> ii(ns);
+  std::vector<int> done(ns, 0);
+  int corr = 0, rit = 0;
+  const int max_rounds = 10;
+  for (int round = 0;; round++) {
+    residual();
+    bool all = true;
+    for (int s = 0; s < ns; s++) {
+      done[s] = rn[s] <= t2[s] || bn == 0.0;
+      all = all && done[s];
+    }
+    if (all || round == max_rounds) break;
+    std::vector<double> sc(2 * QPX_MAX_RHS, 0.0), inner(ns, 1.0);
+    for (int s = 0; s < ns; s++) {
+      if (done[s]) continue;  // a zero right-hand side: the inner CG leaves it at zero
+      const double rnorm = std::sqrt(rn[s]);
+      sc[s] = 1.0 / rnorm;
+      sc[QPX_MAX_RHS + s] = rnorm;
+      // the reduction still missing, with a margin, within what the low
+      // precision reaches on its own
+      inner[s] = std::min(0.5, std::max(1e-5, 0.3 * std::sqrt(t2[s] / rn[s])));
+    }
+    QPX_CUDA(cudaMemcpyAsync(d_scales, sc.data(), sizeof(double) * 2 * QPX_MAX_RHS, cudaMemcpyHostToDevice,
+                             lat->stream));
+    convert_field(Rl, R, Coef{0, 0, d_scales, nullptr}, nullptr);
+    BlasCall z;
+    z.op = B_ZERO;
+    z.x = Dl;
+    blas_launch(lat, lp, ns, z);
+    solve_cg(opl, Dl, Rl, inner.data(), max_iters, isign, cb, ii.data(), false, shifts);
+    mv += ii[0].mv_apps;
+    int its = 0;
+    for (int s = 0; s < ns; s++) its = std::max(its, ii[s].n_iters);
+    rit += its;
+    convert_field(X, Dl, Coef{0, 0, d_scales + QPX_MAX_RHS, nullptr}, nullptr, 1);
+    corr++;
+  }
+  for (int s = 0; s < ns; s++) convert_slice(prec, x[s]->sarg(), prec, slice_arg(X, s), lat);
+  QPX_CUDA(cudaStreamSynchronize(lat->stream));
+  *refine_iters = rit;
+  *corrections = corr;
+  *mv_apps = mv;
+  bool all = true;
+  for (int s = 0; s < ns; s++) {
+    rel_sq_final[s] = bn > 0 ? rn[s] / bn : 0.0;
+    all = all && done[s];
+  }
+  if (!all) throw Error(QPHIX_GPU_ENOTCONV, "mixed-precision multishift CG did not converge");
+}
+
+extern "C" int qphix_gpu_solve_mshift_cg_mixed(qphix_gpu_eo_op op, qphix_gpu_eo_op op_low, qphix_gpu_field *x,
+                                               qphix_gpu_field rhs, int n_shift, const double *shifts,
+                                               const double *rsd_target, const double *rsd_low, int max_iters,
+                                               int isign, int cb, int *n_iters, int *refine_iters,
+                                               int *corrections, double *rel_sq_final, unsigned long *mv_apps)
+{
+  return guard([&] {
+    solve_mshift_mixed(op, op_low, x, rhs, n_shift, shifts, rsd_target, rsd_low, max_iters, isign, cb, n_iters,
+                       refine_iters, corrections, rel_sq_final, mv_apps);
   });
 }

@@ -35,6 +35,7 @@ enum BlasOp : int {
   B_MR_RX,         // x += a r ; r -= a Mr ; red |r|^2
   B_RICH_RX,       // x += dx ; r -= t ; red |r|^2  (richardson_rxupdateNormR)
   B_G5,            // y = gamma_5 x
+  B_CG_RX,         // x += a p ; r -= a (q + s p) ; red |r|^2   (CG on M^+M + s, s per rhs)
 };
 
 // BLAS reductions use red.mask directly as the slot set: B_NORM2 / the
@@ -210,13 +211,31 @@ __global__ void __launch_bounds__(QPX_BLOCK) blas_kernel(const BlasArgs a)
       blas_dot(w, y, sr[0][1], sr[0][2]);
       break;
     }
-    case B_CG_P: {  // x = r, y = p ; a = b
+    case B_CG_P: {  // x = r, y = p ; a = b ; with a reduction: |p|^2 (shifted CG)
       IO::load(a.x, rhs, s, x);
       IO::load(a.y, rhs, s, y);
       const T b = (T)a.a.r(rhs);
 #pragma unroll
       for (int k = 0; k < 24; k++) y[k] = x[k] + b * y[k];
       IO::store(a.y, rhs, s, y);
+      if (a.red.mask) sr[0][0] = blas_norm<false>(y);
+      break;
+    }
+    case B_CG_RX: {  // x = x, y = r, z = q = M^+M p, v = p ; a = alpha, b = shift
+      T q[24], p[24];
+      IO::load(a.x, rhs, s, x);
+      IO::load(a.y, rhs, s, y);
+      IO::load(a.z, rhs, s, q);
+      IO::load(a.v, rhs, s, p);
+      const T al = (T)a.a.r(rhs), sg = (T)a.b.r(rhs);
+#pragma unroll
+      for (int k = 0; k < 24; k++) {
+        x[k] += al * p[k];
+        y[k] -= al * (q[k] + sg * p[k]);
+      }
+      IO::store(a.x, rhs, s, x);
+      IO::store(a.y, rhs, s, y);
+      sr[0][0] = blas_norm<false>(y);
       break;
     }
     case B_MR_RX: {  // x = x, y = r, z = Mr ; a = a

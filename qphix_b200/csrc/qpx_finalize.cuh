@@ -66,11 +66,17 @@ __device__ void finalize_warp(SolverState *st, const double *res, int nrhs, int 
   const int r = lane;
   const bool live = r < nrhs && !st->rhs_done[r];
   // ---- CG (include/qphix/invcg.h:281-417) --------------------------------
+  // shifted CG (M^+M + s, s = v[S_AUX3], 0 for plain CG): <p, (M^+M + s) p> =
+  // |Mp|^2 + s |p|^2, with |p|^2 from the p update's fold (FIN_CG_P, v[S_AUX4])
   if constexpr (FIN == FIN_CG_A) {
     if (live) {
-      v[S_D][r] = res[r * nval];
+      double d = res[r * nval];
+      if (v[S_AUX3][r] != 0.0) d += v[S_AUX3][r] * v[S_AUX4][r];
+      v[S_D][r] = d;
       v[S_A][r] = v[S_C][r] / v[S_D][r];
     }
+  } else if constexpr (FIN == FIN_CG_P) {
+    if (live) v[S_AUX4][r] = res[r * nval];
   } else if constexpr (FIN == FIN_CG_R) {
     if (live) {
       double cp = res[r * nval];

@@ -60,6 +60,7 @@ enum FinOp : int {
   FIN_MCG_D,       // multishift CG: d = |Mp|^2, b = -cp/d
   FIN_MCG_R,       // multishift CG: c = |r|^2, zeta/beta per shift, convergence
   FIN_BICG_RU,     // BiCGStab with reliable updates: as FIN_BICG_RX, asks for an update
+  FIN_CG_P,        // shifted CG: |p|^2 of the new p, for the next FIN_CG_A
 };
 
 struct ReduceArg {

@@ -325,6 +325,64 @@ def test_multishift_fp32_with_fp64_refinement(api, oracle, setup):
         assert np.linalg.norm(r) / bn < tol, (sh, np.linalg.norm(r) / bn)
 
 
+@pytest.mark.parametrize("kind", KINDS)
+def test_cg_shifted(api, oracle, setup, kind):
+    """CG on (M^+M + s_i) x_i = b_i, one shift per right-hand side
+    (qphix_gpu_solve_cg_shifted): every system meets its target by the
+    oracle's true residual; the s = 0 system takes the oracle CG's
+    iteration count (within one: the shifted iteration sums |r|^2 in a BLAS
+    pass instead of the Dslash epilogue)."""
+    lat, M, O = build_ops(api, oracle, setup, kind)
+    shifts = [0.0, 1e-3, 0.05, 1.0]
+    tol = 1e-10
+    bs = [F.gaussian_spinor(setup["dims"], 140 + i) for i in range(len(shifts))]
+    gb = lat.spinor("f64", len(shifts)).upload(np.stack(bs))
+    gx = lat.spinor("f64", len(shifts))
+    api.zero(gx)
+    infos = api.InvCGShifted(M, 2000)(gx, gb, shifts, tol)
+    xs = gx.download()
+    for i, sh in enumerate(shifts):
+        r = bs[i] - (O.apply(O.apply(xs[i], 1), -1) + sh * xs[i])
+        rel = np.linalg.norm(r) / np.linalg.norm(bs[i])
+        assert rel < tol, (kind, sh, rel)
+        assert infos[i]["status"] == 0
+        assert abs(infos[i]["true_rel_resid"] - rel) <= 1e-3 * rel + 1e-16
+    _, io = oracle.cg(O, bs[0], tol, 2000)
+    assert abs(infos[0]["n_iters"] - io.n_iters) <= 1
+    # larger shifts converge in fewer iterations
+    assert infos[3]["n_iters"] < infos[1]["n_iters"]
+
+
+@pytest.mark.parametrize("kind", ["wilson", "clover"])
+@pytest.mark.parametrize("low,rsd_low", [("f32", None), ("f16", 1e-3)])
+def test_mshift_mixed(api, oracle, setup, kind, low, rsd_low):
+    """Multishift CG in low precision plus the batched refinement of every
+    shift (qphix_gpu_solve_mshift_cg_mixed): each shift meets 1e-9 by the
+    oracle's FP64 true residual of (M^+M + shift), and the solutions agree
+    with the FP64 multishift CG's."""
+    s = setup
+    lat, M64, O = build_ops(api, oracle, s, kind)
+    Ml = _low_op(api, lat, s, kind, low)
+    shifts = [1e-4, 1e-3, 0.01, 0.1, 1.0]
+    tol = 1e-9
+    b = F.gaussian_spinor(s["dims"], 151)
+    gb = lat.spinor("f64").upload(b)
+    xs = [lat.spinor("f64") for _ in shifts]
+    out = api.MInvCGMixed(M64, Ml, 5000)(xs, gb, shifts, [tol] * len(shifts), rsd_low=rsd_low)
+    assert out["corrections"] >= 1 and out["refine_iters"] > 0
+    bn = np.linalg.norm(b)
+    for k, sh in enumerate(shifts):
+        x = xs[k].download()
+        r = b - (O.apply(O.apply(x, 1), -1) + sh * x)
+        rel = np.linalg.norm(r) / bn
+        assert rel < tol, (kind, low, sh, rel)
+        assert abs(out["true_rel_resid"][k] - rel) <= 1e-3 * rel + 1e-16
+    ref = [lat.spinor("f64") for _ in shifts]
+    api.MInvCG(M64, 5000)(ref, gb, shifts, [tol] * len(shifts))
+    for x, xr in zip(xs, ref):
+        assert rel_l2(x.download(), xr.download()) < 1e-7
+
+
 def test_fused_blas_entry_points():
     """qphix_gpu_blas_caxpby_norm2 / _xmy_norm2 / _inner_product_norm
     (axpyNorm2, xmyNorm2Spinor, innerProductNorm of include/qphix/blas_new_c.h)
