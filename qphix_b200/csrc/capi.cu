@@ -1092,7 +1092,7 @@ extern "C" int qphix_gpu_halo_pack_links(qphix_gpu_field gauge, void *dst)
 static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qphix_gpu_field_s *psi,
                         qphix_gpu_field_s *gauge, qphix_gpu_field_s *aux, qphix_gpu_field_s *aux2, int isign,
                         int cb, unsigned dir_mask = 0xFFu, qphix_gpu_field_s *aux3 = nullptr,
-                        const HaloSpec *faces = nullptr)
+                        const HaloSpec *faces = nullptr, SolverState *state = nullptr)
 {
   require_spinor(res, "res");
   require_spinor(psi, "psi");
@@ -1163,6 +1163,9 @@ static void dslash_core(const qphix_gpu_op_params &p, qphix_gpu_field_s *res, qp
     QPX_REQUIRE(!is_two_flavour(epi, ACHI_NONE), "halo mode is not provided for the two-flavour operators");
     set_halo(a, p, psi, gauge, cb, *faces);
   }
+  // inside a solver iteration: a state whose solve is done makes the launch
+  // return at once (graph replays after convergence, before the host sees it)
+  a.state = state;
   dslash_launch(lat, res->prec, gauge->recon, epi, ACHI_NONE, a);
 }
 
@@ -1583,30 +1586,31 @@ static void eo_apply(qphix_gpu_eo_op_s *op, qphix_gpu_field_s *res, qphix_gpu_fi
   switch (p.kind) {
   case QPHIX_GPU_WILSON: {  // include/qphix/wilson.h:49-65
     double alpha = 4.0 + p.mass, beta = 0.25 / alpha;
-    dslash_core(p, tmp, in, op->gauge, nullptr, nullptr, isign, other);
+    dslash_core(p, tmp, in, op->gauge, nullptr, nullptr, isign, other, 0xFFu, nullptr, nullptr, o.state);
     achi_core(p, res, tmp, in, op->gauge, nullptr, alpha, beta, isign, target_cb, 1.0, o);
     break;
   }
   case QPHIX_GPU_CLOVER_OP:  // include/qphix/clover.h:162-172
-    dslash_core(p, tmp, in, op->gauge, op->invclov, nullptr, isign, other);
+    dslash_core(p, tmp, in, op->gauge, op->invclov, nullptr, isign, other, 0xFFu, nullptr, nullptr, o.state);
     achi_core(p, res, tmp, in, op->gauge, op->clov, 0.0, 0.25, isign, target_cb, 1.0, o);
     break;
   case QPHIX_GPU_TM: {  // include/qphix/twisted_mass.h:62-77
     double alpha = 4.0 + p.mass;
-    dslash_core(p, tmp, in, op->gauge, nullptr, nullptr, isign, other);
+    dslash_core(p, tmp, in, op->gauge, nullptr, nullptr, isign, other, 0xFFu, nullptr, nullptr, o.state);
     achi_core(p, res, tmp, in, op->gauge, nullptr, alpha, 0.25, isign, target_cb, 1.0, o);
     break;
   }
   case QPHIX_GPU_NDTM:  // include/qphix/ndtm_reuse_operator.h:68-110
-    dslash_core(p, tmp, in, op->gauge, nullptr, nullptr, isign, other);
+    dslash_core(p, tmp, in, op->gauge, nullptr, nullptr, isign, other, 0xFFu, nullptr, nullptr, o.state);
     achi_core(p, res, tmp, in, op->gauge, nullptr, 4.0 + p.mass, 0.25, isign, target_cb, 1.0, o);
     break;
   case QPHIX_GPU_TMCLOVER:  // include/qphix/twisted_mass_clover.h:92-102
-    dslash_core(p, tmp, in, op->gauge, op->finv0, op->finv1, isign, other);
+    dslash_core(p, tmp, in, op->gauge, op->finv0, op->finv1, isign, other, 0xFFu, nullptr, nullptr, o.state);
     achi_core(p, res, tmp, in, op->gauge, op->clov, 0.0, 0.25, isign, target_cb, 1.0, o);
     break;
   case QPHIX_GPU_NDTMCLOVER:  // include/qphix/ndtm_reuse_operator_clover.h:117-128
-    dslash_core(p, tmp, in, op->gauge, op->finv0, op->finv1, isign, other, 0xFFu, op->invclov);
+    dslash_core(p, tmp, in, op->gauge, op->finv0, op->finv1, isign, other, 0xFFu, op->invclov, nullptr,
+                o.state);
     achi_core(p, res, tmp, in, op->gauge, op->clov, 0.0, 0.25, isign, target_cb, 1.0, o);
     break;
   default:
