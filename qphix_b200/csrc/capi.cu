@@ -3180,6 +3180,19 @@ static void solve_mshift_mixed(qphix_gpu_eo_op_s *op, qphix_gpu_eo_op_s *opl, qp
   sync_op_fields(opl, lat);
   const int prec = rhs->prec, lp = opl->gauge->prec;
   const double bn = norm2_host(rhs)[0];
+  if (bn == 0.0) {  // every solution is zero
+    for (int s = 0; s < ns; s++) {
+      BlasCall z;
+      z.op = B_ZERO;
+      z.x = x[s];
+      blas_launch(lat, prec, 1, z);
+      rel_sq_final[s] = 0.0;
+    }
+    QPX_CUDA(cudaStreamSynchronize(lat->stream));
+    *n_iters = *refine_iters = *corrections = 0;
+    *mv_apps = 0;
+    return;
+  }
 
   // 1. the multishift CG in the low precision
   Tmp bl(lat, lp, 1);

@@ -383,6 +383,20 @@ def test_mshift_mixed(api, oracle, setup, kind, low, rsd_low):
         assert rel_l2(x.download(), xr.download()) < 1e-7
 
 
+def test_mshift_mixed_zero_source(api, oracle, setup):
+    """A zero source gives zero solutions without iterating."""
+    s = setup
+    lat, M64, O = build_ops(api, oracle, s, "wilson")
+    Ml = _low_op(api, lat, s, "wilson", "f32")
+    gb = lat.spinor("f64")
+    api.zero(gb)
+    xs = [lat.spinor("f64").upload(F.gaussian_spinor(s["dims"], 160 + k)) for k in range(3)]
+    out = api.MInvCGMixed(M64, Ml, 100)(xs, gb, [1e-3, 0.1, 1.0], [1e-9] * 3)
+    assert out["n_iters"] == 0 and out["corrections"] == 0 and out["mv_apps"] == 0
+    for x in xs:
+        assert not np.any(x.download())
+
+
 def test_fused_blas_entry_points():
     """qphix_gpu_blas_caxpby_norm2 / _xmy_norm2 / _inner_product_norm
     (axpyNorm2, xmyNorm2Spinor, innerProductNorm of include/qphix/blas_new_c.h)
