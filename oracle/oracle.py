@@ -69,6 +69,7 @@ def _declare(l):
         "or_tmclov_dslash": [C.POINTER(Lattice), P, P, P, P, P, I_, I_],
         "or_eo_apply": [C.POINTER(Operator), P, P, I_, I_],
         "or_cg": [C.POINTER(Operator), P, P, D, I_, I_, I_, C.POINTER(SolveInfo)],
+        "or_cg_shift": [C.POINTER(Operator), P, P, D, D, I_, I_, I_, C.POINTER(SolveInfo)],
         "or_bicgstab": [C.POINTER(Operator), P, P, D, I_, I_, I_, C.POINTER(SolveInfo)],
         "or_mr": [C.POINTER(Operator), P, P, D, I_, D, I_, I_, C.POINTER(SolveInfo)],
         "or_minvcg": [C.POINTER(Operator), P, P, I_, P, P, I_, I_, I_,
@@ -239,6 +240,11 @@ def _solve(fn, op, rhs, x0, *args):
 
 def cg(op, rhs, rsd, max_iters=1000, isign=1, cb=1, x0=None):
     return _solve(lib().or_cg, op, rhs, x0, rsd, max_iters, isign, cb)
+
+
+def cg_shift(op, rhs, shift, rsd, max_iters=1000, isign=1, cb=1, x0=None):
+    """CG on M^+M + shift (qphix_oracle.c or_cg_shift)."""
+    return _solve(lib().or_cg_shift, op, rhs, x0, shift, rsd, max_iters, isign, cb)
 
 
 def bicgstab(op, rhs, rsd, max_iters=1000, isign=1, cb=1, x0=None):

@@ -538,8 +538,12 @@ static inline void cmul(double r[2], const double a[2], const double b[2])
 
 /* ---- solvers ------------------------------------------------------------ */
 
-void or_cg(const or_operator *op, double *x, const double *rhs, double rsd,
-           int max_iters, int isign, int cb, or_solve_info *info)
+/* CG on M^+M + shift (shift = 0: or_cg).  The shifted system is the one
+   MInvCG solves per shift (include/qphix/minvcg.h:77); here it is solved on
+   its own with the CG recurrence of include/qphix/invcg.h:281-417, the
+   operator applications taking + shift * vector, d = |Mp|^2 + shift |p|^2. */
+void or_cg_shift(const or_operator *op, double *x, const double *rhs, double shift, double rsd,
+                 int max_iters, int isign, int cb, or_solve_info *info)
 {
   long n = or_op_len(op);
   double *r = malloc(sizeof(double) * n), *p = malloc(sizeof(double) * n);
@@ -550,6 +554,8 @@ void or_cg(const or_operator *op, double *x, const double *rhs, double rsd,
   or_eo_apply(op, mp, x, isign, cb);
   or_eo_apply(op, mmp, mp, -isign, cb);
   mv += 2;
+  if (shift != 0.0)
+    for (long i = 0; i < n; i++) mmp[i] += shift * x[i];
   for (long i = 0; i < n; i++) r[i] = rhs[i] - mmp[i];
   double cp = or_norm2(n, r);
   info->status = 0;
@@ -566,6 +572,10 @@ void or_cg(const or_operator *op, double *x, const double *rhs, double rsd,
     or_eo_apply(op, mmp, mp, -isign, cb);
     mv += 2;
     double d = or_norm2(n, mp);
+    if (shift != 0.0) {
+      d += shift * or_norm2(n, p);
+      for (long i = 0; i < n; i++) mmp[i] += shift * p[i];
+    }
     double a = c / d;
     cp = 0;
     for (long i = 0; i < n; i++) {
@@ -580,6 +590,8 @@ void or_cg(const or_operator *op, double *x, const double *rhs, double rsd,
          no operator applications for it and leaves rsd_sq_final unset */
       or_eo_apply(op, mp, x, isign, cb);
       or_eo_apply(op, mmp, mp, -isign, cb);
+      if (shift != 0.0)
+        for (long i = 0; i < n; i++) mmp[i] += shift * x[i];
       for (long i = 0; i < n; i++) r[i] = rhs[i] - mmp[i];
       info->rsd_sq_final = or_norm2(n, r);
       info->mv_apps = mv;
@@ -594,6 +606,12 @@ void or_cg(const or_operator *op, double *x, const double *rhs, double rsd,
   info->status = 1;
 done:
   free(r); free(p); free(mp); free(mmp);
+}
+
+void or_cg(const or_operator *op, double *x, const double *rhs, double rsd,
+           int max_iters, int isign, int cb, or_solve_info *info)
+{
+  or_cg_shift(op, x, rhs, 0.0, rsd, max_iters, isign, cb, info);
 }
 
 void or_bicgstab(const or_operator *op, double *x, const double *rhs,

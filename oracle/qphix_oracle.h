@@ -124,6 +124,8 @@ typedef struct {
 /* include/qphix/invcg.h:88-456: CG on M^dag M (isign selects M^dag M/MM^dag) */
 void or_cg(const or_operator *op, double *x, const double *rhs, double rsd,
            int max_iters, int isign, int cb, or_solve_info *info);
+void or_cg_shift(const or_operator *op, double *x, const double *rhs, double shift, double rsd,
+                 int max_iters, int isign, int cb, or_solve_info *info);
 /* include/qphix/invbicgstab.h:80-263 */
 void or_bicgstab(const or_operator *op, double *x, const double *rhs,
                  double rsd, int max_iters, int isign, int cb,

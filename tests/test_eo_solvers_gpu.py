@@ -329,9 +329,9 @@ def test_multishift_fp32_with_fp64_refinement(api, oracle, setup):
 def test_cg_shifted(api, oracle, setup, kind):
     """CG on (M^+M + s_i) x_i = b_i, one shift per right-hand side
     (qphix_gpu_solve_cg_shifted): every system meets its target by the
-    oracle's true residual; the s = 0 system takes the oracle CG's
-    iteration count (within one: the shifted iteration sums |r|^2 in a BLAS
-    pass instead of the Dslash epilogue)."""
+    oracle's true residual, and takes the oracle's shifted CG's iteration
+    count (within one: |r|^2 and |p|^2 are summed in BLAS passes, in another
+    order than the oracle's) to the same solution."""
     lat, M, O = build_ops(api, oracle, setup, kind)
     shifts = [0.0, 1e-3, 0.05, 1.0]
     tol = 1e-10
@@ -347,8 +347,10 @@ def test_cg_shifted(api, oracle, setup, kind):
         assert rel < tol, (kind, sh, rel)
         assert infos[i]["status"] == 0
         assert abs(infos[i]["true_rel_resid"] - rel) <= 1e-3 * rel + 1e-16
-    _, io = oracle.cg(O, bs[0], tol, 2000)
-    assert abs(infos[0]["n_iters"] - io.n_iters) <= 1
+    for i, sh in enumerate(shifts):
+        xo, io = oracle.cg_shift(O, bs[i], sh, tol, 2000)
+        assert abs(infos[i]["n_iters"] - io.n_iters) <= 1, (kind, sh, infos[i]["n_iters"], io.n_iters)
+        assert rel_l2(xs[i], xo) < 1e-8, (kind, sh)
     # larger shifts converge in fewer iterations
     assert infos[3]["n_iters"] < infos[1]["n_iters"]
 

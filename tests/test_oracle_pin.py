@@ -91,6 +91,25 @@ def test_minvcg_against_reference(oracle, gold, inp):
     assert np.allclose(fin, gold["minv_rsd"], rtol=1e-6)
 
 
+def test_shifted_cg_oracle(oracle, gold, inp):
+    """The oracle's CG on M^+M + shift: shift 0 is its CG (pinned to the
+    reference above) bit for bit; with a shift, the solution meets the target
+    by the shifted system's true residual, and the shifted system's solution
+    equals the reference-pinned multishift CG's for that shift."""
+    s, x, y, b = inp
+    op = _clover_op(oracle, s)
+    x0, i0 = oracle.cg(op, b, 1e-10, 1000)
+    xs0, is0 = oracle.cg_shift(op, b, 0.0, 1e-10, 1000)
+    assert i0.n_iters == is0.n_iters and i0.mv_apps == is0.mv_apps
+    assert np.array_equal(x0, xs0)
+    for k, sh in enumerate(SHIFTS):
+        xs, info = oracle.cg_shift(op, b, sh, 1e-10, 1000)
+        r = b - (op.apply(op.apply(xs, 1), -1) + sh * xs)
+        assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-10, sh
+        assert info.status == 0 and info.n_iters <= i0.n_iters
+        assert np.abs(xs - gold["minv_x"][k]).max() < 1e-8 * np.abs(xs).max()
+
+
 def _ref():
     import ref_oracle as R
     if not R.available():
